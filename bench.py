@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""Benchmark: batched U(1) two-site H_eff matvec on B200 (FP64 drop-in vs mixed).
+
+Workload (one step): 64 independent two-site H_eff matvecs
+``abc,apqd,bpse,eqtf,dfg->cstg`` for the width-6 Heisenberg cylinder (U(1)
+MPO, bond dim 26), chi drawn uniformly from {256, 512, 1024, 2048}, 30 U(1)
+sectors per bond with Gaussian sizes (sigma=3, clipped to 4..256), all
+problems in one launch per stage.  Synthetic seeded data; operator images
+are packed once (per-site setup), theta is packed every step.
+
+    python bench.py [--gpus N --steps K --warmup W --precision bf16x3]
+    python bench.py --impl reference      # CPU baseline arm (oracle port)
+
+Prints one JSON line on rank 0.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+os.environ.setdefault("OPENBLAS_NUM_THREADS", str(os.cpu_count()))
+
+import numpy as np  # noqa: E402
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "U(1) H_eff matvec TFLOP/s & DMRG sweep s at χ=2048: mixed vs FP64, |ΔE|≤1e-9"
+WORKLOAD = ("batched grouped-sector contraction: 64 independent two-site H_eff matvecs, width-6 Heisenberg "
+            "cylinder U(1) MPO (Dw=26), chi~U{256,512,1024,2048}, 30 U(1) sectors/bond, Gaussian sizes "
+            "sigma=3 clipped 4..256, one launch per stage")
+CHIS = (256, 512, 1024, 2048)
+N_PROBLEMS = 64
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines: list = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from tenax_b200 import HeffBatch, HeffOperator, _capi
+    from tenax_b200.tensor import embed_in_keys
+    from tenax_b200.workloads import batched_problems
+
+    problems = batched_problems(N_PROBLEMS, CHIS, seed=args.seed + 1000 * rank)
+    chi_counts = {int(c): sum(1 for p in problems if p.chi == c) for c in CHIS}
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def run_precision(prec, with_e2e=False, sampler=None):
+        ops = [HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, prec) for p in problems]
+        sizes = [o.size for o in ops]
+        offs = np.concatenate([[0], np.cumsum(sizes)])
+        x_all = torch.empty(int(offs[-1]), dtype=torch.float64, device=dev)
+        y_all = torch.empty(int(offs[-1]), dtype=torch.float64, device=dev)
+        for i, (p, o) in enumerate(zip(problems, ops)):
+            x_all[offs[i]:offs[i + 1]].copy_(embed_in_keys(p.theta, o.keys).data)
+        xs = [x_all[offs[i]:offs[i + 1]] for i in range(len(ops))]
+        ys = [y_all[offs[i]:offs[i + 1]] for i in range(len(ops))]
+        batch = HeffBatch(ops)
+        flops = batch.flops
+        st = torch.cuda.current_stream()
+        for _ in range(args.warmup):
+            batch.apply(xs, ys)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if sampler:
+            sampler.__enter__()
+        e0.record(st)
+        for _ in range(args.steps):
+            batch.apply(xs, ys)
+        e1.record(st)
+        barrier()
+        if sampler:
+            sampler.__exit__()
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        err = batch.device_error()
+        # per-stage timing (each stage re-run alone, same buffers)
+        stage_ms = []
+        for s in range(4):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            for _ in range(args.steps):
+                _capi.check(_capi.LIB.tnx_heff_batch_apply_stage(batch.handle, s, st.cuda_stream))
+            b.record(st)
+            torch.cuda.synchronize()
+            stage_ms.append(a.elapsed_time(b) / args.steps)
+        import ctypes as C
+
+        sf = np.zeros(3)
+        tot_sf = np.zeros(3)
+        for o in ops:
+            _capi.check(_capi.LIB.tnx_heff_stage_flops(o.handle, sf.ctypes.data))
+            tot_sf += sf
+        res = {"ms": ms, "flops": flops, "stage_ms": stage_ms, "stage_flops": tot_sf.tolist(), "err": err,
+               "per_problem_flops": [o.flops for o in ops], "launches": batch.launches_per_apply}
+        if with_e2e:
+            host_in = torch.empty(int(offs[-1]), dtype=torch.float64, pin_memory=True)
+            host_out = torch.empty(int(offs[-1]), dtype=torch.float64, pin_memory=True)
+            host_in.copy_(x_all.cpu())
+            for _ in range(args.warmup):
+                x_all.copy_(host_in, non_blocking=True)
+                batch.apply(xs, ys)
+                host_out.copy_(y_all, non_blocking=True)
+            barrier()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            for _ in range(args.steps):
+                x_all.copy_(host_in, non_blocking=True)
+                batch.apply(xs, ys)
+                host_out.copy_(y_all, non_blocking=True)
+            b.record(st)
+            barrier()
+            res["e2e_ms"] = max_over_ranks(a.elapsed_time(b) / args.steps)
+            res["e2e_bytes"] = int(offs[-1]) * 8
+        del batch, ops, x_all, y_all, xs, ys
+        torch.cuda.empty_cache()
+        return res
+
+    r64 = run_precision("fp64")
+    sampler = ClockSampler(local)
+    rmx = run_precision(args.precision, with_e2e=True, sampler=sampler)
+    clocks = sampler.summary()
+
+    flops_all = rmx["flops"] * world
+    value = flops_all / (rmx["ms"] * 1e-3) / 1e12
+    fp64_value = r64["flops"] * world / (r64["ms"] * 1e-3) / 1e12
+    peaks, peak_src = _peaks()
+    # dominant GEMM stage of the mixed step
+    st_ms = rmx["stage_ms"]
+    gemm = {1: rmx["stage_flops"][0], 3: rmx["stage_flops"][2]}
+    dom = max((1, 3), key=lambda s: st_ms[s])
+    split = 3.0 if args.precision == "bf16x3" else 1.0
+    peak = peaks["bf16_tflops"] / split if args.precision == "bf16x3" else peaks["bf16_tflops"] / 2.0
+    achieved = gemm[dom] / (st_ms[dom] * 1e-3) / 1e12
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(f"{args.precision}_stage{dom}")
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(rmx["ms"], 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.precision, "data": "synthetic (seeded N(0,1) blocks; no dataset)",
+            "config": {"workload": WORKLOAD, "problems_per_gpu": N_PROBLEMS, "chi_counts": chi_counts,
+                       "flops_per_step_per_gpu": rmx["flops"], "flop_count": "block-sparse 4-stage sector GEMM "
+                       "flops from stored block dims", "l2": "inputs larger than L2 (operators+theta >> 126 MB); "
+                       "no flush", "parallelism": f"replicas x{world} (independent problems per GPU)"},
+            "fp64": {"value": round(fp64_value, 3), "unit": "TFLOP/s", "ms_per_step": round(r64["ms"], 4),
+                     "stage_ms": [round(x, 4) for x in r64["stage_ms"]]},
+            "mixed_over_fp64": round(value / fp64_value, 3),
+            "stage_ms": [round(x, 4) for x in st_ms],
+            "stage_names": ["pack theta", "stage-1 GEMM L.theta", "fused MPO (W_l W_r)", "stage-4 GEMM .R"],
+            "roofline": {"bound": "tensor", "kernel": f"stage{dom} tcgen05 grouped GEMM", "achieved":
+                         round(achieved, 2), "peak": round(peak, 1), "unit": "TFLOP/s",
+                         "frac": round(achieved / peak, 4), "peak_source": f"{peak_src} bf16 burst"
+                         + (" / 3 (three products)" if split == 3 else " / 2 (tf32)"), "traffic": traffic},
+            "e2e": {"value": round(flops_all / (rmx["e2e_ms"] * 1e-3) / 1e12, 3), "unit": "TFLOP/s",
+                    "h2d_bytes_per_step": rmx["e2e_bytes"], "d2h_bytes_per_step": rmx["e2e_bytes"]},
+            "gpu_launches": rmx["launches"] * args.steps,
+            "device_error_flag": rmx["err"],
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(problems, rmx["per_problem_flops"], budget_s=args.cpu_budget)
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _host_problem(p):
+    """Device problem -> oracle tensors on the host."""
+    from oracle.blocksparse import Leg, OTensor
+
+    def h(t):
+        return OTensor(tuple(Leg(i.charges, int(i.flow), i.label) for i in t.indices), t.numpy_blocks())
+
+    return [h(t) for t in (p.L, p.theta, p.Wl, p.Wr, p.R)]
+
+
+def cpu_baseline(problems, flops, budget_s=15.0):
+    """The oracle port of the reference's per-combination H_eff
+    (algorithms/dmrg.py:1048-1151) on the host cores, on a bounded sample:
+    the smallest-chi problems of the batch, in order, until the budget."""
+    from oracle import dmrg as odmrg
+
+    order = sorted(range(len(problems)), key=lambda i: problems[i].chi)
+    done_flops, t_used, sample = 0.0, 0.0, []
+    odmrg.heff_matvec(*_host_problem(problems[order[0]]))  # warm-up (einsum path caches)
+    for i in order:
+        args = _host_problem(problems[i])
+        t0 = time.perf_counter()
+        odmrg.heff_matvec(*args)
+        dt = time.perf_counter() - t0
+        t_used += dt
+        done_flops += flops[i]
+        sample.append(problems[i].chi)
+        if t_used > budget_s:
+            break
+    return {"value": round(done_flops / t_used / 1e12, 6), "unit": "TFLOP/s", "cores": os.cpu_count(),
+            "kind": "port", "sample": f"{len(sample)} matvecs of the batch (chi {sorted(set(sample))}), "
+            f"{t_used:.1f} s, numpy einsum per block combination, BLAS threads={os.cpu_count()}"}
+
+
+def run_reference(args):
+    """CPU arm: the oracle port of the reference's H_eff on the host cores."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    import ctypes as C
+
+    from oracle import dmrg as odmrg
+    from oracle.blocksparse import Leg, OTensor
+    from tenax_b200 import _capi
+    from tenax_b200.auto_mpo import heisenberg_cylinder_sites
+    from tenax_b200.workloads import PHYS, _env_keys, bond_charges
+
+    sites = heisenberg_cylinder_sites(4, 6)
+    wl, wr = sites[7], sites[8]
+    rng = np.random.default_rng(args.seed)
+    chis = rng.choice(np.asarray(CHIS), size=N_PROBLEMS)
+    W = [OTensor(tuple(Leg(c, f, l) for c, f, l in zip(s.charges, s.flows, s.labels)), s.blocks()) for s in (wl, wr)]
+    gen = np.random.default_rng(args.seed + 1)
+
+    def problem(chi):
+        v = bond_charges(int(chi))
+        def blocks(legs, keys):
+            return {k: gen.standard_normal(tuple(int(np.sum(l.charges == q)) for l, q in zip(legs, k))) for k in keys}
+        Lg = (Leg(v, -1, "vl"), Leg(wl.charges[0], -1, "wl"), Leg(v, -1, "vl_c"))
+        Rg = (Leg(v, 1, "vr"), Leg(wr.charges[3], 1, "wr"), Leg(v, 1, "vr_c"))
+        Tg = (Leg(v, 1, "vl"), Leg(PHYS, 1, "p1"), Leg(PHYS, 1, "p2"), Leg(v, -1, "vr"))
+        sv = set(np.unique(v).tolist())
+        tk = sorted((int(a), int(p), int(q), int(a + p + q)) for a in np.unique(v) for p in PHYS for q in PHYS
+                    if int(a + p + q) in sv)
+        L = OTensor(Lg, blocks(Lg, _env_keys(v, wl.charges[0], v)))
+        R = OTensor(Rg, blocks(Rg, _env_keys(v, wr.charges[3], v)))
+        T = OTensor(Tg, blocks(Tg, tk))
+        # algorithmic flop count of this structure (planner, counting only)
+        hold = [_capi.DescHolder([l.charges for l in t.legs], [l.flow for l in t.legs], sorted(t.blocks), None)
+                for t in (L, T, W[0], W[1], R)]
+        h = C.c_void_p()
+        _capi.check(_capi.LIB.tnx_heff_create(*[C.byref(x.desc) for x in hold], C.byref(h)))
+        f = _capi.LIB.tnx_heff_flops(h)
+        _capi.LIB.tnx_heff_destroy(h)
+        return (L, T, W[0], W[1], R), f
+
+    total_flops = 0.0
+    pf = {}
+    for c in CHIS:
+        _, pf[int(c)] = problem(c)
+    total_flops = sum(pf[int(c)] for c in chis)
+    # bounded per-step sample: smallest-chi problems first
+    order = sorted(chis.tolist())
+    samples = [problem(c) for c in order[:max(1, args.ref_problems)]]
+    for _ in range(max(1, args.warmup)):
+        odmrg.heff_matvec(*samples[0][0])
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        fl = 0.0
+        for args_, f in samples:
+            odmrg.heff_matvec(*args_)
+            fl += f
+        times.append((time.perf_counter() - t0, fl))
+    dt = sum(t for t, _ in times)
+    fl = sum(f for _, f in times)
+    value = fl / dt / 1e12
+    ms_step = total_flops / (value * 1e12) * 1e3
+    out = {"metric": METRIC, "value": round(value, 6), "unit": "TFLOP/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 1), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded N(0,1) blocks)",
+           "impl": "reference",
+           "config": {"workload": WORKLOAD, "problems_per_gpu": N_PROBLEMS,
+                      "chi_counts": {int(c): int(np.sum(chis == c)) for c in CHIS}},
+           "cpu_baseline": {"value": round(value, 6), "unit": "TFLOP/s", "cores": os.cpu_count(), "kind": "port",
+                            "sample": f"each step: {len(samples)} smallest-chi matvecs of the batch "
+                            f"(chi {sorted(set(order[:len(samples)]))}); ms_per_step extrapolates the full batch"},
+           "e2e": {"value": round(value, 6), "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "tf32"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-problems", type=int, default=2)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    sys.path.insert(0, ROOT)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,159 @@
+/*
+ * tenax_b200.h -- C ABI of the B200 block-sparse symmetric contraction library.
+ *
+ * The reference (tenax, pure Python/JAX) has no native boundary; these entry
+ * points are the custom calls its Python layer binds (ctypes here, XLA FFI or
+ * a torch extension elsewhere).  Each function names the reference function
+ * whose behaviour it reproduces.  All entry points return an int status
+ * (TNX_OK on success); no C++ exception crosses this boundary.  Device
+ * pointers are caller-owned unless stated; `stream` is a cudaStream_t passed
+ * as void*.  Block buffers hold one tensor's blocks contiguously, row-major,
+ * in the order of the key list given to the planner (the Python layer uses
+ * sorted-key order = tenax's pytree leaf order, core/tensor.py:572-578).
+ */
+#ifndef TENAX_B200_H
+#define TENAX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes; the Python layer maps them to the reference's exceptions */
+enum {
+  TNX_OK = 0,
+  TNX_ERR_VALUE = 1,       /* ValueError   */
+  TNX_ERR_TYPE = 2,        /* TypeError    */
+  TNX_ERR_RUNTIME = 3,     /* RuntimeError */
+  TNX_ERR_CUDA = 4,        /* CUDA API or launch failure */
+  TNX_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+  TNX_ERR_UNSUPPORTED = 6  /* valid input outside what this build implements */
+};
+
+/* arithmetic of the sector GEMMs */
+enum {
+  TNX_PREC_FP64 = 0,   /* DMMA f64 tensor-core GEMM, FP64 accumulate            */
+  TNX_PREC_BF16X3 = 1, /* tcgen05 kind::f16: hi*hi + hi*lo + lo*hi, FP32 accum   */
+  TNX_PREC_TF32 = 2    /* tcgen05 kind::tf32, FP32 accumulate                    */
+};
+
+/* block-matching semantics of a contraction plan */
+enum {
+  TNX_MATCH_FILTERED = 0,   /* _contract_symmetric: contraction/contractor.py:291-484 */
+  TNX_MATCH_UNFILTERED = 1  /* _blockwise_contract: algorithms/dmrg.py:1048-1151      */
+};
+
+/* One operand's structure (no data).  charges: all legs' int32 charge
+ * arrays concatenated (leg_dims[i] entries each); keys: n_blocks x n_legs. */
+typedef struct tnx_tensor_desc {
+  int32_t n_legs;
+  const char* subs;       /* einsum chars, one per leg (may be NULL for H_eff) */
+  const int32_t* flows;   /* +1 IN / -1 OUT                                  */
+  const int32_t* charges;
+  const int64_t* leg_dims;
+  int64_t n_blocks;
+  const int32_t* keys;
+} tnx_tensor_desc;
+
+typedef struct tnx_plan tnx_plan;
+typedef struct tnx_heff tnx_heff;
+typedef struct tnx_heff_batch tnx_heff_batch;
+
+/* Text of the last error on the calling thread. */
+const char* tnx_last_error(void);
+int tnx_version(void);
+
+/* Valid block keys, in the reference's order.  Replaces _compute_valid_blocks
+ * (core/tensor.py:53-165).  modulus = 0 selects U(1), n >= 2 selects Z_n.
+ * Call with keys_out == NULL to get the count in *n_keys. */
+int tnx_valid_blocks(int32_t n_legs, const int32_t* charges, const int64_t* leg_dims, const int32_t* flows,
+                     int32_t modulus, int32_t has_target, int64_t target, int64_t* n_keys, int32_t* keys_out,
+                     int64_t keys_cap);
+
+/* Plan a block-sparse contraction of n_ops operands with subscripts
+ * ops[i].subs -> out_subs.  mode TNX_MATCH_FILTERED reproduces
+ * _contract_symmetric (contractor.py:291-484, output-target inference and
+ * conservation filter; >= 3 operands with differing contracted sets give an
+ * empty result as in the reference); TNX_MATCH_UNFILTERED reproduces
+ * _blockwise_contract (dmrg.py:1048-1151, no output filter).  out_charges /
+ * out_leg_dims / out_flows describe the output legs (used by the filter). */
+int tnx_plan_create(const tnx_tensor_desc* ops, int32_t n_ops, const char* out_subs, int32_t mode,
+                    int32_t modulus, const int32_t* out_charges, const int64_t* out_leg_dims,
+                    const int32_t* out_flows, tnx_plan** plan);
+/* Output structure: blocks in sorted-key order, contiguous. keys may be NULL. */
+int tnx_plan_output(const tnx_plan* plan, int64_t* n_blocks, int32_t* keys, int64_t* total_elems,
+                    int32_t* has_target, int64_t* target);
+int tnx_plan_workspace(const tnx_plan* plan, int32_t precision, size_t* bytes);
+double tnx_plan_flops(const tnx_plan* plan);
+/* Execute on device FP64 data: inputs[i] are the operands' block buffers. */
+int tnx_plan_execute(tnx_plan* plan, const double* const* inputs, double* out, int32_t precision, void* workspace,
+                     size_t workspace_bytes, void* stream);
+void tnx_plan_destroy(tnx_plan* plan);
+
+/* Two-site effective Hamiltonian "abc,apqd,bpse,eqtf,dfg->cstg"
+ * (dmrg.py:1282-1289) over the block structures of L, theta, W_l, W_r, R.
+ * The output uses theta's block layout; tnx_heff_closed() reports whether
+ * every output key is one of theta's keys (the caller extends theta's key
+ * set until it is -- the key-union growth of the reference's Lanczos). */
+int tnx_heff_create(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, const tnx_tensor_desc* Wl,
+                    const tnx_tensor_desc* Wr, const tnx_tensor_desc* R, tnx_heff** h);
+int tnx_heff_closed(const tnx_heff* h, int32_t* closed);
+/* Output keys of H_eff applied to theta's key set (structure only). */
+int tnx_heff_out_keys(const tnx_heff* h, int64_t* n_keys, int32_t* keys);
+/* Keys of theta that H_eff actually writes (others come out zero). */
+double tnx_heff_flops(const tnx_heff* h);
+/* Pack L, W_l, W_r, R (device FP64 block buffers) into GEMM operand images
+ * for the given precision; done once per site, reused by every matvec. */
+int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const double* Wr, const double* R,
+                           int32_t precision, void* stream);
+void tnx_heff_destroy(tnx_heff* h);
+
+/* Many independent H_eff problems applied in one launch per stage
+ * (persistent grouped GEMMs over all sectors of all problems). */
+int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx_heff_batch** b);
+int tnx_heff_batch_apply(tnx_heff_batch* b, const double* const* thetas, double* const* outs, void* stream);
+/* Re-run one stage of the last apply (0 pack theta, 1 stage-1 GEMM, 2 fused
+ * MPO, 3 stage-4 GEMM) with the same buffers -- per-kernel timing. */
+int tnx_heff_batch_apply_stage(tnx_heff_batch* b, int32_t stage, void* stream);
+/* Algorithmic flops of stage 1 (L.theta), stages 2+3 (MPO), stage 4 (.R). */
+int tnx_heff_stage_flops(const tnx_heff* h, double* flops3);
+/* Number of kernel launches one apply issues (launch accounting). */
+int tnx_heff_batch_launches(const tnx_heff_batch* b, int32_t* n_launches);
+/* Device error flag of the tcgen05 GEMM (non-zero: a bounded wait gave up). */
+int tnx_heff_batch_error(tnx_heff_batch* b, int32_t* err);
+/* Optional device int32 flag: when non-zero, every kernel of an apply returns
+ * immediately (Lanczos early exit inside a captured graph). */
+int tnx_heff_batch_set_skip_flag(tnx_heff_batch* b, const int32_t* flag);
+void tnx_heff_batch_destroy(tnx_heff_batch* b);
+
+/* FP64 vector primitives on flat block buffers (inner/norm of the reference's
+ * SymmetricTensor arithmetic, core/tensor.py:296-319, 863-868).  Reductions
+ * are deterministic two-pass sums; `scratch` is a caller-owned device buffer
+ * of tnx_reduce_scratch_len() doubles (calls sharing one scratch must be
+ * stream-ordered).  Results are written to device memory. */
+int64_t tnx_reduce_scratch_len(void);
+int tnx_dot(const double* x, const double* y, int64_t n, double* result, double* scratch, void* stream);
+int tnx_nrm2(const double* x, int64_t n, double* result, double* scratch, void* stream);
+
+/* One Lanczos orthogonalisation step (dmrg.py:1005-1019) on device:
+ *   alpha[k] = <v, w>;  w -= alpha[k] v  (- beta[k] v_prev if k > 0);
+ *   beta[k+1] = ||w||;  if beta[k+1] < tol: *done = 1  else v_next = w / beta[k+1]
+ * alpha/beta live in device memory; nothing is read back to the host.
+ * Every kernel of the step returns immediately once *done is set. */
+int tnx_lanczos_step(double* w, const double* v, const double* v_prev, double* v_next, int64_t n, double* alpha,
+                     double* beta, int32_t k, double tol, int32_t* done, double* scratch, void* stream);
+/* out = sum_k coefs[k] * basis[k], summed left to right as the reference's
+ * eigenvector reconstruction (dmrg.py:1038-1040); device pointer table and
+ * device coefficients. */
+int tnx_combine(const double* const* basis_dev_table, const double* coefs_dev, int32_t n_vec, int64_t n, double* out,
+                void* stream);
+/* out = x * s (mode 0), x / s (mode 1), x / (s + 1e-15) (mode 2); s on device. */
+int tnx_scale(const double* x, double* out, int64_t n, const double* scale_dev, int32_t mode, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TENAX_B200_H */

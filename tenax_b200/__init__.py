@@ -1,0 +1,28 @@
+"""tenax_b200: B200-native block-sparse symmetric contraction for tenax.
+
+Drop-in GPU path for tenax's ``SymmetricTensor`` contraction and the
+two-site DMRG H_eff matvec built on it: the same names and argument
+meanings as ``tenax.contract``, ``SymmetricTensor``/``TensorIndex`` and
+``dmrg()``; arithmetic runs in this package's sm_100a kernels through the C
+ABI in ``include/tenax_b200.h``.
+"""
+
+from tenax_b200 import _capi  # noqa: F401  (loads libtenax_b200.so or raises)
+from tenax_b200.core import (  # noqa: F401
+    BaseSymmetry,
+    FlowDirection,
+    Label,
+    TensorIndex,
+    U1Symmetry,
+    ZnSymmetry,
+)
+from tenax_b200.tensor import SymmetricTensor, compute_valid_blocks, inner  # noqa: F401
+from tenax_b200.contraction import (  # noqa: F401
+    blockwise_contract,
+    contract,
+    contract_with_subscripts,
+)
+from tenax_b200.heff import HeffBatch, HeffOperator  # noqa: F401
+
+EPS = 1e-15
+LOG_EPS = 1e-250

@@ -1,0 +1,996 @@
+// C ABI of the library (declared in include/tenax_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/tenax_b200.h"
+#include "common.cuh"
+#include "kernels.cuh"
+#include "planner.hpp"
+
+using namespace tnx;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+static int set_err(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define TNX_TRY(...)                                                         \
+  try {                                                                      \
+    __VA_ARGS__                                                              \
+  } catch (const PlanError& e) {                                             \
+    return set_err(e.code, e.msg);                                           \
+  } catch (const std::bad_alloc&) {                                          \
+    return set_err(TNX_ERR_RUNTIME, "host allocation failed");               \
+  } catch (const std::exception& e) {                                        \
+    return set_err(TNX_ERR_RUNTIME, e.what());                               \
+  }
+
+#define CUDA_OK(x)                                                                                  \
+  do {                                                                                              \
+    cudaError_t _e = (x);                                                                           \
+    if (_e != cudaSuccess) throw PlanError{TNX_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)}; \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// device memory
+// ---------------------------------------------------------------------------
+namespace {
+struct DevMem {
+  void* p = nullptr;
+  size_t n = 0;
+  DevMem() = default;
+  DevMem(const DevMem&) = delete;
+  DevMem& operator=(const DevMem&) = delete;
+  ~DevMem() {
+    if (p) cudaFree(p);
+  }
+  void alloc(size_t bytes) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = bytes;
+    if (bytes) CUDA_OK(cudaMalloc(&p, bytes));
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+template <class T>
+void upload(DevMem& m, const std::vector<T>& v, cudaStream_t st = nullptr) {
+  m.alloc(v.size() * sizeof(T));
+  if (!v.empty()) CUDA_OK(cudaMemcpyAsync(m.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+constexpr int kMaxSlots = 256;
+struct PtrTab {
+  uint64_t p[kMaxSlots];
+};
+
+TensorStruct parse_desc(const tnx_tensor_desc* d, const char* default_subs) {
+  if (!d) throw PlanError{TNX_ERR_VALUE, "null tensor descriptor"};
+  if (d->n_legs < 0 || d->n_legs > kMaxLegs) throw PlanError{TNX_ERR_UNSUPPORTED, "at most 8 legs per tensor"};
+  TensorStruct t;
+  t.nl = d->n_legs;
+  if (d->subs)
+    t.subs = std::string(d->subs);
+  else if (default_subs)
+    t.subs = default_subs;
+  if (static_cast<int>(t.subs.size()) != t.nl) throw PlanError{TNX_ERR_VALUE, "subscripts do not match leg count"};
+  t.flows.assign(d->flows, d->flows + t.nl);
+  int64_t off = 0;
+  t.charges.resize(t.nl);
+  for (int l = 0; l < t.nl; ++l) {
+    t.charges[l].assign(d->charges + off, d->charges + off + d->leg_dims[l]);
+    off += d->leg_dims[l];
+  }
+  t.finalize_leg_maps();
+  t.keys.resize(d->n_blocks);
+  for (int64_t b = 0; b < d->n_blocks; ++b) t.keys[b].assign(d->keys + b * t.nl, d->keys + (b + 1) * t.nl);
+  t.layout_blocks();
+  return t;
+}
+
+int img_mode_of(int precision) {
+  if (precision == TNX_PREC_FP64) return IMG_F64;
+  if (precision == TNX_PREC_BF16X3) return IMG_BF16;
+  if (precision == TNX_PREC_TF32) return IMG_TF32;
+  throw PlanError{TNX_ERR_VALUE, "unknown precision"};
+}
+
+int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// image geometry of one pair plan for one mode
+struct PairGeom {
+  std::vector<int64_t> a_tile0, b_tile0;  // per group, in tiles
+  std::vector<int32_t> nMt, nNt, nKt;
+  int64_t a_tiles = 0, b_tiles = 0;
+};
+
+PairGeom pair_geom(const PairPlan& P, int mode) {
+  ImgGeom g = img_geom(mode);
+  PairGeom G;
+  for (auto& gs : P.groups) {
+    int32_t mt = static_cast<int32_t>(cdiv(gs.M, g.tm)), nt = static_cast<int32_t>(cdiv(gs.N, g.tm)),
+            kt = static_cast<int32_t>(cdiv(gs.K, g.tk));
+    G.nMt.push_back(mt);
+    G.nNt.push_back(nt);
+    G.nKt.push_back(kt);
+    G.a_tile0.push_back(G.a_tiles);
+    G.b_tile0.push_back(G.b_tiles);
+    G.a_tiles += static_cast<int64_t>(mt) * kt;
+    G.b_tiles += static_cast<int64_t>(nt) * kt;
+  }
+  return G;
+}
+
+void build_pack(const std::vector<PackSeg>& segs, const PairGeom& G, bool a_side, uint64_t img_base,
+                int64_t lo_off, int tile_bytes, int src_slot, std::vector<DevPackSeg>& out,
+                std::vector<DevChunk>& chunks) {
+  for (auto& s : segs) {
+    DevPackSeg d{};
+    d.src_off = s.src_off;
+    int64_t t0 = a_side ? G.a_tile0[s.group] : G.b_tile0[s.group];
+    d.img_addr = img_base + static_cast<uint64_t>(t0) * tile_bytes;
+    d.lo_off = lo_off;
+    d.row0 = s.row0;
+    d.k0 = s.k0;
+    d.nKt = G.nKt[s.group];
+    d.nlegs = s.nlegs;
+    d.src_slot = src_slot;
+    for (int l = 0; l < s.nlegs; ++l) {
+      d.dims[l] = s.dims[l];
+      d.rstr[l] = s.rstr[l];
+      d.kstr[l] = s.kstr[l];
+    }
+    int seg_id = static_cast<int>(out.size());
+    out.push_back(d);
+    for (int64_t st = 0; st < s.count; st += 2048) chunks.push_back({seg_id, 0, st, std::min<int64_t>(2048, s.count - st)});
+  }
+}
+
+void build_tiles(const PairPlan& P, const PairGeom& G, int group_base, std::vector<std::pair<int64_t, DevTile>>& tl) {
+  for (size_t g = 0; g < P.groups.size(); ++g)
+    for (int mt = 0; mt < G.nMt[g]; ++mt)
+      for (int nt = 0; nt < G.nNt[g]; ++nt) tl.push_back({G.nKt[g], DevTile{group_base + static_cast<int>(g), mt, nt, 0}});
+}
+
+std::vector<DevTile> sorted_tiles(std::vector<std::pair<int64_t, DevTile>>& tl) {
+  std::stable_sort(tl.begin(), tl.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  std::vector<DevTile> out;
+  out.reserve(tl.size());
+  for (auto& x : tl) out.push_back(x.second);
+  return out;
+}
+
+void gemm_launch(int mode, const DevMem& groups, const DevMem& tiles, int n_tiles, const DevMem& rowoff,
+                 const PtrTab& out_tab, bool out_f64, int32_t* err, const int32_t* skip, cudaStream_t st,
+                 DevMem& out_tab_dev) {
+  // out_tab travels through a small device array (kernels index it per group)
+  CUDA_OK(cudaMemcpyAsync(out_tab_dev.p, out_tab.p, sizeof(PtrTab), cudaMemcpyHostToDevice, st));
+  if (mode == IMG_F64)
+    launch_gemm_f64(groups.as<DevGroup>(), tiles.as<DevTile>(), n_tiles, rowoff.as<int64_t>(),
+                    out_tab_dev.as<uint64_t>(), skip, st);
+  else
+    launch_gemm_tc(mode, groups.as<DevGroup>(), tiles.as<DevTile>(), n_tiles, rowoff.as<int64_t>(),
+                   out_tab_dev.as<uint64_t>(), out_f64, err, skip, st);
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// generic plans
+// ---------------------------------------------------------------------------
+struct StepDev {
+  int mode = -1;
+  PairGeom G;
+  DevMem a_img, b_img, c_res;  // images and result matrices
+  int64_t a_lo = 0, b_lo = 0;
+  DevMem packA, chunksA, packB, chunksB, groups, tiles, rowoff, scat, chunksS, out_tab;
+  int nA = 0, nB = 0, nT = 0, nS = 0;
+  bool res_f32 = false;
+};
+
+struct tnx_plan {
+  int mode_sem = 0;
+  std::vector<TensorStruct> ins;
+  std::vector<PairPlan> steps;
+  std::vector<int> a_src;  // operand index for step 0, -1 = previous intermediate
+  std::vector<int> b_src;
+  bool empty_result = false;  // filtered >=3 operands with no common signature
+  bool has_scalar = false;    // single-operand plan: B is an internal scalar 1.0
+  TensorStruct out;
+  bool has_target = false;
+  int64_t target = 0;
+  double flops = 0.0;
+  // device state
+  int dev_prec = -1;
+  std::vector<std::unique_ptr<StepDev>> dev;
+  std::vector<std::unique_ptr<DevMem>> inter;  // intermediate block buffers (fp64)
+  DevMem scalar_one;                           // operand for single-tensor plans
+  DevMem err_flag, src_tab;
+};
+
+static void finalize_plan_out(tnx_plan* p) {
+  if (p->empty_result) return;
+  p->out = p->steps.back().out;
+}
+
+extern "C" {
+
+const char* tnx_last_error(void) { return g_last_error.c_str(); }
+int tnx_version(void) { return 1; }
+
+int tnx_valid_blocks(int32_t n_legs, const int32_t* charges, const int64_t* leg_dims, const int32_t* flows,
+                     int32_t modulus, int32_t has_target, int64_t target, int64_t* n_keys, int32_t* keys_out,
+                     int64_t keys_cap) {
+  TNX_TRY({
+    std::vector<std::vector<int32_t>> ch(n_legs);
+    int64_t off = 0;
+    for (int l = 0; l < n_legs; ++l) {
+      ch[l].assign(charges + off, charges + off + leg_dims[l]);
+      off += leg_dims[l];
+    }
+    std::vector<int32_t> fl(flows, flows + n_legs);
+    auto keys = valid_blocks(ch, fl, modulus, has_target != 0, target);
+    *n_keys = static_cast<int64_t>(keys.size());
+    if (keys_out) {
+      if (keys_cap < static_cast<int64_t>(keys.size()) * n_legs)
+        return set_err(TNX_ERR_VALUE, "keys_out capacity too small");
+      for (size_t i = 0; i < keys.size(); ++i)
+        for (int l = 0; l < n_legs; ++l) keys_out[i * n_legs + l] = keys[i][l];
+    }
+    return TNX_OK;
+  })
+}
+
+int tnx_plan_create(const tnx_tensor_desc* ops, int32_t n_ops, const char* out_subs, int32_t mode,
+                    int32_t modulus, const int32_t* out_charges, const int64_t* out_leg_dims,
+                    const int32_t* out_flows, tnx_plan** plan) {
+  TNX_TRY({
+    if (n_ops < 1) return set_err(TNX_ERR_VALUE, "contract() requires at least one tensor");
+    if (!out_subs) return set_err(TNX_ERR_VALUE, "null output subscripts");
+    auto p = std::make_unique<tnx_plan>();
+    p->mode_sem = mode;
+    for (int i = 0; i < n_ops; ++i) p->ins.push_back(parse_desc(&ops[i], nullptr));
+    const std::string osubs(out_subs);
+    std::vector<std::vector<int32_t>> och;
+    std::vector<int32_t> ofl;
+    if (out_charges && out_leg_dims && out_flows) {
+      int64_t off = 0;
+      for (size_t l = 0; l < osubs.size(); ++l) {
+        och.emplace_back(out_charges + off, out_charges + off + out_leg_dims[l]);
+        off += out_leg_dims[l];
+      }
+      ofl.assign(out_flows, out_flows + osubs.size());
+    }
+    // character counts
+    std::map<char, int> cnt;
+    for (auto& t : p->ins)
+      for (char c : t.subs) cnt[c]++;
+    for (auto& kv : cnt)
+      if (kv.second > 2) return set_err(TNX_ERR_VALUE, std::string("subscript '") + kv.first + "' used more than twice");
+    KeyFilter filt;
+    if (mode == TNX_MATCH_FILTERED) {
+      if (och.empty()) return set_err(TNX_ERR_VALUE, "filtered plans need the output leg charges");
+      // output target inference (contractor.py:344-355): plain integer sum
+      int64_t total = 0;
+      for (auto& t : p->ins) {
+        if (t.keys.empty()) continue;
+        std::set<int64_t> tg;
+        for (auto& k : t.keys) {
+          int64_t s = 0;
+          for (int l = 0; l < t.nl; ++l) s += static_cast<int64_t>(t.flows[l]) * k[l];
+          tg.insert(s);
+        }
+        if (tg.size() == 1) total += *tg.begin();
+      }
+      p->has_target = total != 0;
+      p->target = total;
+      auto vk = valid_blocks(och, ofl, modulus, p->has_target, total);
+      filt.active = true;
+      for (auto& k : vk) filt.allowed[k] = 1;
+      if (n_ops >= 3) {
+        // signature intersection (contractor.py:373-403)
+        std::set<char> contracted;
+        for (auto& kv : cnt)
+          if (kv.second >= 2) contracted.insert(kv.first);
+        std::vector<std::set<Key>> sigs;
+        std::vector<size_t> siglen;
+        for (auto& t : p->ins) {
+          std::vector<std::pair<char, int>> pos;
+          for (int l = 0; l < t.nl; ++l)
+            if (contracted.count(t.subs[l])) pos.push_back({t.subs[l], l});
+          std::sort(pos.begin(), pos.end());
+          std::set<Key> s;
+          for (auto& k : t.keys) {
+            Key sg;
+            for (auto& pp : pos) sg.push_back(k[pp.second]);
+            s.insert(sg);
+          }
+          sigs.push_back(s);
+          siglen.push_back(pos.size());
+        }
+        std::set<Key> common = sigs[0];
+        for (size_t i = 1; i < sigs.size(); ++i) {
+          std::set<Key> nx;
+          for (auto& k : common)
+            if (sigs[i].count(k)) nx.insert(k);
+          common.swap(nx);
+        }
+        if (common.empty()) {
+          p->empty_result = true;
+          p->out.nl = static_cast<int>(osubs.size());
+          p->out.subs = osubs;
+          p->out.charges = och;
+          p->out.flows = ofl;
+          p->out.finalize_leg_maps();
+          *plan = p.release();
+          return TNX_OK;
+        }
+        return set_err(TNX_ERR_UNSUPPORTED,
+                       "filtered contraction of >=3 operands with a common contracted signature is not supported; "
+                       "contract pairwise");
+      }
+    }
+    if (n_ops == 1) {
+      // a single operand: contract with a scalar (no contracted legs)
+      TensorStruct one;
+      one.nl = 0;
+      one.keys.push_back({});
+      one.dims.push_back({});
+      one.offs.push_back(0);
+      one.total = 1;
+      p->ins.push_back(one);
+      p->has_scalar = true;
+      p->steps.push_back(plan_pair(p->ins[0], p->ins[1], osubs, filt, och.empty() ? nullptr : &och,
+                                   ofl.empty() ? nullptr : &ofl));
+      p->a_src.push_back(0);
+      p->b_src.push_back(1);
+    } else {
+      TensorStruct cur = p->ins[0];
+      for (int i = 1; i < n_ops; ++i) {
+        const TensorStruct& B = p->ins[i];
+        std::string step_out;
+        if (i == n_ops - 1) {
+          step_out = osubs;
+        } else {
+          for (char c : cur.subs)
+            if (B.subs.find(c) == std::string::npos) step_out.push_back(c);
+          for (char c : B.subs)
+            if (cur.subs.find(c) == std::string::npos) step_out.push_back(c);
+        }
+        const bool last = i == n_ops - 1;
+        PairPlan pp = plan_pair(cur, B, step_out, last ? filt : KeyFilter{}, last && !och.empty() ? &och : nullptr,
+                                last && !ofl.empty() ? &ofl : nullptr);
+        p->a_src.push_back(i == 1 ? 0 : -1);
+        p->b_src.push_back(i);
+        cur = pp.out;
+        // the intermediate's per-leg charge maps come from its blocks
+        cur.cdim.assign(cur.nl, {});
+        for (size_t b = 0; b < cur.keys.size(); ++b)
+          for (int l = 0; l < cur.nl; ++l) cur.cdim[l][cur.keys[b][l]] = cur.dims[b][l];
+        p->steps.push_back(std::move(pp));
+      }
+    }
+    for (auto& s : p->steps) p->flops += s.flops;
+    finalize_plan_out(p.get());
+    *plan = p.release();
+    return TNX_OK;
+  })
+}
+
+int tnx_plan_output(const tnx_plan* plan, int64_t* n_blocks, int32_t* keys, int64_t* total_elems,
+                    int32_t* has_target, int64_t* target) {
+  TNX_TRY({
+    const TensorStruct& o = plan->out;
+    if (n_blocks) *n_blocks = static_cast<int64_t>(o.keys.size());
+    if (total_elems) *total_elems = o.total;
+    if (has_target) *has_target = plan->has_target ? 1 : 0;
+    if (target) *target = plan->target;
+    if (keys)
+      for (size_t b = 0; b < o.keys.size(); ++b)
+        for (int l = 0; l < o.nl; ++l) keys[b * o.nl + l] = o.keys[b][l];
+    return TNX_OK;
+  })
+}
+
+double tnx_plan_flops(const tnx_plan* plan) { return plan ? plan->flops : 0.0; }
+
+int tnx_plan_workspace(const tnx_plan* plan, int32_t precision, size_t* bytes) {
+  TNX_TRY({
+    (void)plan;
+    (void)precision;
+    *bytes = 0;  // plans own their scratch
+    return TNX_OK;
+  })
+}
+
+static void plan_build_device(tnx_plan* p, int precision) {
+  const int mode = img_mode_of(precision);
+  const ImgGeom ig = img_geom(mode);
+  p->dev.clear();
+  p->inter.clear();
+  p->err_flag.alloc(sizeof(int32_t));
+  CUDA_OK(cudaMemset(p->err_flag.p, 0, sizeof(int32_t)));
+  if (p->has_scalar) upload(p->scalar_one, std::vector<double>{1.0});
+  for (size_t s = 0; s + 1 < p->steps.size(); ++s) {
+    auto m = std::make_unique<DevMem>();
+    m->alloc(std::max<int64_t>(1, p->steps[s].out.total) * sizeof(double));
+    p->inter.push_back(std::move(m));
+  }
+  for (size_t s = 0; s < p->steps.size(); ++s) {
+    const PairPlan& P = p->steps[s];
+    auto d = std::make_unique<StepDev>();
+    d->mode = mode;
+    d->G = pair_geom(P, mode);
+    const int split = mode == IMG_BF16 ? 2 : 1;
+    d->a_img.alloc(std::max<int64_t>(1, d->G.a_tiles) * ig.tile_bytes * split);
+    d->b_img.alloc(std::max<int64_t>(1, d->G.b_tiles) * ig.tile_bytes * split);
+    d->a_lo = d->G.a_tiles * ig.tile_bytes;
+    d->b_lo = d->G.b_tiles * ig.tile_bytes;
+    d->res_f32 = mode != IMG_F64;
+    // result matrices
+    std::vector<int64_t> res_off;
+    int64_t roff = 0;
+    for (auto& g : P.groups) {
+      res_off.push_back(roff);
+      roff += g.M * g.N;
+    }
+    d->c_res.alloc(std::max<int64_t>(1, roff) * (d->res_f32 ? 4 : 8));
+    std::vector<DevPackSeg> pa, pb;
+    std::vector<DevChunk> ca, cb;
+    build_pack(P.packA, d->G, true, reinterpret_cast<uint64_t>(d->a_img.p), d->a_lo, ig.tile_bytes, 0, pa, ca);
+    build_pack(P.packB, d->G, false, reinterpret_cast<uint64_t>(d->b_img.p), d->b_lo, ig.tile_bytes, 1, pb, cb);
+    upload(d->packA, pa);
+    upload(d->chunksA, ca);
+    upload(d->packB, pb);
+    upload(d->chunksB, cb);
+    d->nA = static_cast<int>(ca.size());
+    d->nB = static_cast<int>(cb.size());
+    std::vector<DevGroup> gr;
+    std::vector<int64_t> ro;
+    for (size_t g = 0; g < P.groups.size(); ++g) {
+      DevGroup x{};
+      x.a_addr = reinterpret_cast<uint64_t>(d->a_img.p) + static_cast<uint64_t>(d->G.a_tile0[g]) * ig.tile_bytes;
+      x.b_addr = reinterpret_cast<uint64_t>(d->b_img.p) + static_cast<uint64_t>(d->G.b_tile0[g]) * ig.tile_bytes;
+      x.a_lo = d->a_lo;
+      x.b_lo = d->b_lo;
+      x.rowoff0 = static_cast<int64_t>(ro.size());
+      x.M = static_cast<int32_t>(P.groups[g].M);
+      x.N = static_cast<int32_t>(P.groups[g].N);
+      x.nKt = d->G.nKt[g];
+      x.out_slot = 0;
+      gr.push_back(x);
+      for (int64_t r = 0; r < P.groups[g].M; ++r) ro.push_back(res_off[g] + r * P.groups[g].N);
+    }
+    upload(d->groups, gr);
+    upload(d->rowoff, ro);
+    std::vector<std::pair<int64_t, DevTile>> tl;
+    build_tiles(P, d->G, 0, tl);
+    auto tiles = sorted_tiles(tl);
+    upload(d->tiles, tiles);
+    d->nT = static_cast<int>(tiles.size());
+    std::vector<DevScatSeg> ss;
+    std::vector<DevChunk> cs;
+    for (auto& sc : P.scatter) {
+      DevScatSeg x{};
+      x.dst_off = sc.dst_off;
+      x.ld = P.groups[sc.group].N;
+      x.src_base = res_off[sc.group] + static_cast<int64_t>(sc.row0) * x.ld + sc.col0;
+      x.nlegs = sc.nlegs;
+      for (int l = 0; l < sc.nlegs; ++l) {
+        x.dims[l] = sc.dims[l];
+        x.rstr[l] = sc.rstr[l];
+        x.cstr[l] = sc.cstr[l];
+      }
+      int id = static_cast<int>(ss.size());
+      ss.push_back(x);
+      for (int64_t st = 0; st < sc.count; st += 2048) cs.push_back({id, 0, st, std::min<int64_t>(2048, sc.count - st)});
+    }
+    upload(d->scat, ss);
+    upload(d->chunksS, cs);
+    d->nS = static_cast<int>(cs.size());
+    d->out_tab.alloc(sizeof(PtrTab));
+    p->dev.push_back(std::move(d));
+  }
+  CUDA_OK(cudaDeviceSynchronize());
+  p->dev_prec = precision;
+}
+
+int tnx_plan_execute(tnx_plan* plan, const double* const* inputs, double* out, int32_t precision, void* workspace,
+                     size_t workspace_bytes, void* stream) {
+  TNX_TRY({
+    (void)workspace;
+    (void)workspace_bytes;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (plan->empty_result) return TNX_OK;
+    if (plan->dev_prec != precision) plan_build_device(plan, precision);
+    const ImgGeom ig = img_geom(img_mode_of(precision));
+    const int split = precision == TNX_PREC_BF16X3 ? 2 : 1;
+    for (size_t s = 0; s < plan->steps.size(); ++s) {
+      StepDev& d = *plan->dev[s];
+      const PairPlan& P = plan->steps[s];
+      const double* a_ptr = plan->a_src[s] >= 0 ? inputs[plan->a_src[s]] : plan->inter[s - 1]->as<double>();
+      const double* b_ptr = plan->has_scalar ? plan->scalar_one.as<double>() : inputs[plan->b_src[s]];
+      double* o_ptr = (s + 1 == plan->steps.size()) ? out : plan->inter[s]->as<double>();
+      PtrTab src{};
+      src.p[0] = reinterpret_cast<uint64_t>(a_ptr);
+      src.p[1] = reinterpret_cast<uint64_t>(b_ptr);
+      // the pack kernels read operand pointers from a device table
+      DevMem& srcdev = plan->src_tab;
+      if (!srcdev.p) srcdev.alloc(sizeof(PtrTab));
+      CUDA_OK(cudaMemcpyAsync(srcdev.p, &src, 2 * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+      CUDA_OK(cudaMemsetAsync(d.a_img.p, 0, std::max<int64_t>(1, d.G.a_tiles) * ig.tile_bytes * split, st));
+      CUDA_OK(cudaMemsetAsync(d.b_img.p, 0, std::max<int64_t>(1, d.G.b_tiles) * ig.tile_bytes * split, st));
+      launch_pack(srcdev.as<uint64_t>(), d.packA.as<DevPackSeg>(), d.chunksA.as<DevChunk>(), d.nA, d.mode, nullptr,
+                  st);
+      launch_pack(srcdev.as<uint64_t>(), d.packB.as<DevPackSeg>(), d.chunksB.as<DevChunk>(), d.nB, d.mode, nullptr,
+                  st);
+      PtrTab ot{};
+      ot.p[0] = reinterpret_cast<uint64_t>(d.c_res.p);
+      gemm_launch(d.mode, d.groups, d.tiles, d.nT, d.rowoff, ot, false, plan->err_flag.as<int32_t>(), nullptr, st,
+                  d.out_tab);
+      if (P.out.total > 0)
+        CUDA_OK(cudaMemsetAsync(o_ptr, 0, P.out.total * sizeof(double), st));
+      launch_scatter(d.c_res.p, d.res_f32, o_ptr, d.scat.as<DevScatSeg>(), d.chunksS.as<DevChunk>(), d.nS, st);
+      CUDA_OK(cudaGetLastError());
+    }
+    return TNX_OK;
+  })
+}
+
+void tnx_plan_destroy(tnx_plan* plan) { delete plan; }
+
+// ---------------------------------------------------------------------------
+// H_eff
+// ---------------------------------------------------------------------------
+struct tnx_heff {
+  HeffPlan H;
+  int prec = -1;
+  DevMem l_img, r_img;  // stage-1 A image (L), stage-4 B image (R)
+  int64_t l_lo = 0, r_lo = 0;
+  PairGeom g1, g4;
+  bool terms_ready = false;
+};
+
+int tnx_heff_create(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, const tnx_tensor_desc* Wl,
+                    const tnx_tensor_desc* Wr, const tnx_tensor_desc* R, tnx_heff** h) {
+  TNX_TRY({
+    auto x = std::make_unique<tnx_heff>();
+    TensorStruct tL = parse_desc(L, "abc"), tT = parse_desc(theta, "apqd"), tWl = parse_desc(Wl, "bpse"),
+                 tWr = parse_desc(Wr, "eqtf"), tR = parse_desc(R, "dfg");
+    tL.subs = "abc";
+    tT.subs = "apqd";
+    tWl.subs = "bpse";
+    tWr.subs = "eqtf";
+    tR.subs = "dfg";
+    x->H = plan_heff(tL, tT, tWl, tWr, tR);
+    *h = x.release();
+    return TNX_OK;
+  })
+}
+
+int tnx_heff_closed(const tnx_heff* h, int32_t* closed) {
+  *closed = (h->H.closed && h->H.s4_separable) ? 1 : 0;
+  return TNX_OK;
+}
+
+int tnx_heff_out_keys(const tnx_heff* h, int64_t* n_keys, int32_t* keys) {
+  *n_keys = static_cast<int64_t>(h->H.out_keys.size());
+  if (keys)
+    for (size_t i = 0; i < h->H.out_keys.size(); ++i)
+      for (int l = 0; l < 4; ++l) keys[i * 4 + l] = h->H.out_keys[i][l];
+  return TNX_OK;
+}
+
+double tnx_heff_flops(const tnx_heff* h) { return h ? h->H.flops : 0.0; }
+
+int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const double* Wr, const double* R,
+                           int32_t precision, void* stream) {
+  TNX_TRY({
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    HeffPlan& H = h->H;
+    if (!H.closed || !H.s4_separable)
+      return set_err(TNX_ERR_VALUE, "H_eff output keys are not a subset of theta's keys; extend theta first");
+    const int mode = img_mode_of(precision);
+    const ImgGeom ig = img_geom(mode);
+    const int split = mode == IMG_BF16 ? 2 : 1;
+    // W data to host for the fused MPO terms
+    std::vector<double> wl(H.Wl.total), wr(H.Wr.total);
+    if (H.Wl.total) CUDA_OK(cudaMemcpyAsync(wl.data(), Wl, H.Wl.total * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (H.Wr.total) CUDA_OK(cudaMemcpyAsync(wr.data(), Wr, H.Wr.total * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    heff_mpo_terms(H, wl, wr);
+    h->terms_ready = true;
+    h->g1 = pair_geom(H.s1, mode);
+    h->g4 = pair_geom(H.s4, mode);
+    h->l_img.alloc(std::max<int64_t>(1, h->g1.a_tiles) * ig.tile_bytes * split);
+    h->r_img.alloc(std::max<int64_t>(1, h->g4.b_tiles) * ig.tile_bytes * split);
+    h->l_lo = h->g1.a_tiles * ig.tile_bytes;
+    h->r_lo = h->g4.b_tiles * ig.tile_bytes;
+    CUDA_OK(cudaMemsetAsync(h->l_img.p, 0, h->l_img.n, st));
+    CUDA_OK(cudaMemsetAsync(h->r_img.p, 0, h->r_img.n, st));
+    std::vector<DevPackSeg> pl, pr;
+    std::vector<DevChunk> cl, cr;
+    build_pack(H.s1.packA, h->g1, true, reinterpret_cast<uint64_t>(h->l_img.p), h->l_lo, ig.tile_bytes, 0, pl, cl);
+    build_pack(H.s4.packB, h->g4, false, reinterpret_cast<uint64_t>(h->r_img.p), h->r_lo, ig.tile_bytes, 1, pr, cr);
+    DevMem dpl, dcl, dpr, dcr, tab;
+    upload(dpl, pl, st);
+    upload(dcl, cl, st);
+    upload(dpr, pr, st);
+    upload(dcr, cr, st);
+    uint64_t ptrs[2] = {reinterpret_cast<uint64_t>(L), reinterpret_cast<uint64_t>(R)};
+    tab.alloc(sizeof(ptrs));
+    CUDA_OK(cudaMemcpyAsync(tab.p, ptrs, sizeof(ptrs), cudaMemcpyHostToDevice, st));
+    launch_pack(tab.as<uint64_t>(), dpl.as<DevPackSeg>(), dcl.as<DevChunk>(), static_cast<int>(cl.size()), mode,
+                nullptr, st);
+    launch_pack(tab.as<uint64_t>(), dpr.as<DevPackSeg>(), dcr.as<DevChunk>(), static_cast<int>(cr.size()), mode,
+                nullptr, st);
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(cudaStreamSynchronize(st));
+    h->prec = precision;
+    return TNX_OK;
+  })
+}
+
+void tnx_heff_destroy(tnx_heff* h) { delete h; }
+
+// ---------------------------------------------------------------------------
+// batched H_eff
+// ---------------------------------------------------------------------------
+struct tnx_heff_batch {
+  std::vector<tnx_heff*> hs;
+  int prec = 0, mode = 0;
+  DevMem th_img, x1, x3_img;
+  int64_t th_lo = 0, x3_lo = 0;
+  DevMem th_pack, th_chunks;
+  int n_th_chunks = 0;
+  DevMem g1, t1, ro1, g4, t4, ro4;
+  int n_t1 = 0, n_t4 = 0;
+  DevMem mpo_pairs, mpo_ins, mpo_oslots, mpo_terms, mpo_chunks;
+  int n_mpo_chunks = 0, max_in_slots = 0;
+  DevMem zero_segs;  // not used when every output block is written
+  DevMem err, src_tab, out_tab1, out_tab4;
+  const int32_t* skip = nullptr;
+  int n_launches = 0;
+  std::vector<uint64_t> last_src, last_out;
+};
+
+int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx_heff_batch** out) {
+  TNX_TRY({
+    if (n < 1 || n > kMaxSlots - 1) return set_err(TNX_ERR_VALUE, "batch size must be in [1, 255]");
+    auto b = std::make_unique<tnx_heff_batch>();
+    b->prec = precision;
+    b->mode = img_mode_of(precision);
+    const int mode = b->mode;
+    const ImgGeom ig = img_geom(mode);
+    const int split = mode == IMG_BF16 ? 2 : 1;
+    const bool f32 = mode != IMG_F64;
+    for (int i = 0; i < n; ++i) {
+      if (hs[i]->prec != precision) return set_err(TNX_ERR_VALUE, "operators were packed for another precision");
+      b->hs.push_back(hs[i]);
+    }
+    // sizes: theta images (stage-1 B), X1 results, X3 images (stage-4 A)
+    int64_t th_tiles = 0, x3_tiles = 0, x1_elems = 0;
+    std::vector<int64_t> th_t0(n), x3_t0(n), x1_0(n);
+    for (int i = 0; i < n; ++i) {
+      const HeffPlan& H = hs[i]->H;
+      th_t0[i] = th_tiles;
+      x3_t0[i] = x3_tiles;
+      x1_0[i] = x1_elems;
+      th_tiles += hs[i]->g1.b_tiles;
+      x3_tiles += hs[i]->g4.a_tiles;
+      for (auto& g : H.s1.groups) x1_elems += g.M * g.N;
+    }
+    b->th_img.alloc(std::max<int64_t>(1, th_tiles) * ig.tile_bytes * split);
+    b->x3_img.alloc(std::max<int64_t>(1, x3_tiles) * ig.tile_bytes * split);
+    b->th_lo = th_tiles * ig.tile_bytes;
+    b->x3_lo = x3_tiles * ig.tile_bytes;
+    b->x1.alloc(std::max<int64_t>(1, x1_elems) * (f32 ? 4 : 8));
+    CUDA_OK(cudaMemset(b->th_img.p, 0, b->th_img.n));
+    CUDA_OK(cudaMemset(b->x3_img.p, 0, b->x3_img.n));
+    const uint64_t th_base = reinterpret_cast<uint64_t>(b->th_img.p);
+    const uint64_t x3_base = reinterpret_cast<uint64_t>(b->x3_img.p);
+    const uint64_t x1_base = reinterpret_cast<uint64_t>(b->x1.p);
+    const int esz = f32 ? 4 : 8;
+    std::vector<DevPackSeg> tp;
+    std::vector<DevChunk> tc;
+    std::vector<DevGroup> G1, G4;
+    std::vector<int64_t> R1, R4;
+    std::vector<std::pair<int64_t, DevTile>> T1, T4;
+    std::vector<DevMpoPair> MP;
+    std::vector<DevMpoIn> MI;
+    std::vector<DevMpoOutSlot> MO;
+    std::vector<DevMpoTerm> MT;
+    std::vector<int2> MC;
+    for (int i = 0; i < n; ++i) {
+      tnx_heff* h = hs[i];
+      const HeffPlan& H = h->H;
+      // theta pack: source slot i, images into the batch theta buffer
+      PairGeom gth = h->g1;  // b_tile0 relative to this problem
+      for (auto& t : gth.b_tile0) t += th_t0[i];
+      build_pack(H.s1.packB, gth, false, th_base, b->th_lo, ig.tile_bytes, i, tp, tc);
+      // stage-1 groups
+      std::vector<int64_t> x1_goff;
+      int64_t xo = x1_0[i];
+      for (size_t g = 0; g < H.s1.groups.size(); ++g) {
+        x1_goff.push_back(xo);
+        DevGroup x{};
+        x.a_addr = reinterpret_cast<uint64_t>(h->l_img.p) + static_cast<uint64_t>(h->g1.a_tile0[g]) * ig.tile_bytes;
+        x.b_addr = th_base + static_cast<uint64_t>(gth.b_tile0[g]) * ig.tile_bytes;
+        x.a_lo = h->l_lo;
+        x.b_lo = b->th_lo;
+        x.rowoff0 = static_cast<int64_t>(R1.size());
+        x.M = static_cast<int32_t>(H.s1.groups[g].M);
+        x.N = static_cast<int32_t>(H.s1.groups[g].N);
+        x.nKt = h->g1.nKt[g];
+        x.out_slot = 0;
+        for (int64_t r = 0; r < H.s1.groups[g].M; ++r) R1.push_back(xo + r * H.s1.groups[g].N);
+        xo += H.s1.groups[g].M * H.s1.groups[g].N;
+        G1.push_back(x);
+      }
+      std::vector<std::pair<int64_t, DevTile>> tl;
+      build_tiles(H.s1, h->g1, static_cast<int>(G1.size() - H.s1.groups.size()), tl);
+      T1.insert(T1.end(), tl.begin(), tl.end());
+      // stage-4 groups
+      PairGeom gx3 = h->g4;
+      for (auto& t : gx3.a_tile0) t += x3_t0[i];
+      const int g4base = static_cast<int>(G4.size());
+      for (size_t g = 0; g < H.s4.groups.size(); ++g) {
+        DevGroup x{};
+        x.a_addr = x3_base + static_cast<uint64_t>(gx3.a_tile0[g]) * ig.tile_bytes;
+        x.b_addr = reinterpret_cast<uint64_t>(h->r_img.p) + static_cast<uint64_t>(h->g4.b_tile0[g]) * ig.tile_bytes;
+        x.a_lo = b->x3_lo;
+        x.b_lo = h->r_lo;
+        x.rowoff0 = static_cast<int64_t>(R4.size());
+        x.M = static_cast<int32_t>(H.s4.groups[g].M);
+        x.N = static_cast<int32_t>(H.s4.groups[g].N);
+        x.nKt = h->g4.nKt[g];
+        x.out_slot = 1 + i;
+        for (auto v : H.s4_rowoff[g]) R4.push_back(v);
+        G4.push_back(x);
+      }
+      tl.clear();
+      build_tiles(H.s4, h->g4, g4base, tl);
+      T4.insert(T4.end(), tl.begin(), tl.end());
+      // MPO tables
+      for (size_t pi = 0; pi < H.pairs.size(); ++pi) {
+        const MpoPair& mp = H.pairs[pi];
+        DevMpoPair dp{};
+        dp.mc = mp.mc;
+        dp.md = mp.md;
+        dp.in0 = static_cast<int32_t>(MI.size());
+        dp.n_in = static_cast<int32_t>(mp.ins.size());
+        dp.out0 = static_cast<int32_t>(MO.size());
+        dp.n_out = mp.n_out_slots;
+        dp.term0 = static_cast<int32_t>(MT.size());
+        dp.n_terms = static_cast<int32_t>(mp.terms.size());
+        dp.n_in_slots = mp.n_in_slots;
+        dp.n_out_slots = mp.n_out_slots;
+        b->max_in_slots = std::max(b->max_in_slots, mp.n_in_slots);
+        for (size_t k = 0; k < mp.ins.size(); ++k) {
+          const MpoIn& in = mp.ins[k];
+          DevMpoIn di{};
+          const int64_t ld = H.s1.groups[in.g1].N;
+          di.x1_addr = x1_base + static_cast<uint64_t>(x1_goff[in.g1] + static_cast<int64_t>(in.row0) * ld + in.col0) * esz;
+          di.ld = ld;
+          di.mb = in.mb;
+          di.mp = in.mp;
+          di.mq = in.mq;
+          di.slot0 = mp.in_slot0[k];
+          MI.push_back(di);
+        }
+        for (size_t k = 0; k < mp.outs.size(); ++k) {
+          const MpoOut& o = mp.outs[k];
+          for (int s = 0; s < o.ms; ++s)
+            for (int t = 0; t < o.mt; ++t)
+              for (int f = 0; f < o.mf; ++f) {
+                DevMpoOutSlot os{};
+                os.img_addr = x3_base + static_cast<uint64_t>(gx3.a_tile0[o.g4]) * ig.tile_bytes;
+                os.lo_off = b->x3_lo;
+                os.nKt = h->g4.nKt[o.g4];
+                os.row0 = o.row0;
+                os.k0 = o.k0;
+                os.rows_per_c = o.ms * o.mt;
+                os.row_add = s * o.mt + t;
+                os.k_add = f * mp.md;
+                MO.push_back(os);
+              }
+        }
+        for (auto& t : mp.terms) MT.push_back({t.out_slot, t.in_slot, t.w});
+        const int pair_id = static_cast<int>(MP.size());
+        MP.push_back(dp);
+        for (int p0 = 0; p0 < mp.mc * mp.md; p0 += 128) MC.push_back(make_int2(pair_id, p0));
+      }
+    }
+    if (b->max_in_slots * 128 * esz > 200 * 1024)
+      return set_err(TNX_ERR_UNSUPPORTED, "MPO input vector too long for the fused MPO kernel");
+    upload(b->th_pack, tp);
+    upload(b->th_chunks, tc);
+    b->n_th_chunks = static_cast<int>(tc.size());
+    upload(b->g1, G1);
+    upload(b->ro1, R1);
+    auto t1 = sorted_tiles(T1);
+    upload(b->t1, t1);
+    b->n_t1 = static_cast<int>(t1.size());
+    upload(b->g4, G4);
+    upload(b->ro4, R4);
+    auto t4 = sorted_tiles(T4);
+    upload(b->t4, t4);
+    b->n_t4 = static_cast<int>(t4.size());
+    upload(b->mpo_pairs, MP);
+    upload(b->mpo_ins, MI);
+    upload(b->mpo_oslots, MO);
+    upload(b->mpo_terms, MT);
+    upload(b->mpo_chunks, MC);
+    b->n_mpo_chunks = static_cast<int>(MC.size());
+    b->err.alloc(sizeof(int32_t));
+    CUDA_OK(cudaMemset(b->err.p, 0, sizeof(int32_t)));
+    b->src_tab.alloc(sizeof(PtrTab));
+    b->out_tab1.alloc(sizeof(PtrTab));
+    b->out_tab4.alloc(sizeof(PtrTab));
+    // stage-1 output table is fixed (slot 0 = X1 buffer)
+    PtrTab t1tab{};
+    t1tab.p[0] = x1_base;
+    CUDA_OK(cudaMemcpy(b->out_tab1.p, &t1tab, sizeof(PtrTab), cudaMemcpyHostToDevice));
+    CUDA_OK(cudaDeviceSynchronize());
+    b->n_launches = 4;
+    *out = b.release();
+    return TNX_OK;
+  })
+}
+
+int tnx_heff_batch_set_skip_flag(tnx_heff_batch* b, const int32_t* flag) {
+  b->skip = flag;
+  return TNX_OK;
+}
+
+int tnx_heff_batch_launches(const tnx_heff_batch* b, int32_t* n_launches) {
+  *n_launches = b->n_launches;
+  return TNX_OK;
+}
+
+// stage 0: pack theta; 1: stage-1 GEMM; 2: fused MPO; 3: stage-4 GEMM into theta layout
+static void heff_batch_stage(tnx_heff_batch* b, int stage, cudaStream_t st) {
+  const bool f32 = b->mode != IMG_F64;
+  switch (stage) {
+    case 0:
+      launch_pack(b->src_tab.as<uint64_t>(), b->th_pack.as<DevPackSeg>(), b->th_chunks.as<DevChunk>(),
+                  b->n_th_chunks, b->mode, b->skip, st);
+      break;
+    case 1:
+      if (b->mode == IMG_F64)
+        launch_gemm_f64(b->g1.as<DevGroup>(), b->t1.as<DevTile>(), b->n_t1, b->ro1.as<int64_t>(),
+                        b->out_tab1.as<uint64_t>(), b->skip, st);
+      else
+        launch_gemm_tc(b->mode, b->g1.as<DevGroup>(), b->t1.as<DevTile>(), b->n_t1, b->ro1.as<int64_t>(),
+                       b->out_tab1.as<uint64_t>(), false, b->err.as<int32_t>(), b->skip, st);
+      break;
+    case 2:
+      launch_mpo_apply(f32, b->mode, b->mpo_pairs.as<DevMpoPair>(), b->mpo_ins.as<DevMpoIn>(),
+                       b->mpo_oslots.as<DevMpoOutSlot>(), b->mpo_terms.as<DevMpoTerm>(), b->mpo_chunks.as<int2>(),
+                       b->n_mpo_chunks, b->max_in_slots, b->skip, st);
+      break;
+    default:
+      if (b->mode == IMG_F64)
+        launch_gemm_f64(b->g4.as<DevGroup>(), b->t4.as<DevTile>(), b->n_t4, b->ro4.as<int64_t>(),
+                        b->out_tab4.as<uint64_t>(), b->skip, st);
+      else
+        launch_gemm_tc(b->mode, b->g4.as<DevGroup>(), b->t4.as<DevTile>(), b->n_t4, b->ro4.as<int64_t>(),
+                       b->out_tab4.as<uint64_t>(), true, b->err.as<int32_t>(), b->skip, st);
+  }
+}
+
+int tnx_heff_batch_apply(tnx_heff_batch* b, const double* const* thetas, double* const* outs, void* stream) {
+  TNX_TRY({
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int n = static_cast<int>(b->hs.size());
+    std::vector<uint64_t> src(n), o4(n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+      src[i] = reinterpret_cast<uint64_t>(thetas[i]);
+      o4[1 + i] = reinterpret_cast<uint64_t>(outs[i]);
+    }
+    // pointer tables are re-uploaded only when they change, so an apply with
+    // the same buffers issues kernels only (and can be captured in a graph)
+    if (src != b->last_src) {
+      CUDA_OK(cudaMemcpyAsync(b->src_tab.p, src.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+      b->last_src = src;
+    }
+    if (o4 != b->last_out) {
+      CUDA_OK(cudaMemcpyAsync(b->out_tab4.p, o4.data(), (n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+      b->last_out = o4;
+    }
+    for (int stage = 0; stage < 4; ++stage) heff_batch_stage(b, stage, st);
+    CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
+
+int tnx_heff_batch_apply_stage(tnx_heff_batch* b, int32_t stage, void* stream) {
+  TNX_TRY({
+    if (stage < 0 || stage > 3) return set_err(TNX_ERR_VALUE, "stage must be 0..3");
+    if (b->last_src.empty()) return set_err(TNX_ERR_VALUE, "call tnx_heff_batch_apply once first");
+    heff_batch_stage(b, stage, static_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
+
+int tnx_heff_stage_flops(const tnx_heff* h, double* flops3) {
+  flops3[0] = h->H.flops_s1;
+  flops3[1] = h->H.flops_mpo;
+  flops3[2] = h->H.flops_s4;
+  return TNX_OK;
+}
+
+void tnx_heff_batch_destroy(tnx_heff_batch* b) { delete b; }
+
+int tnx_heff_batch_error(tnx_heff_batch* b, int32_t* err) {
+  TNX_TRY({
+    CUDA_OK(cudaMemcpy(err, b->err.p, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    return TNX_OK;
+  })
+}
+
+// ---------------------------------------------------------------------------
+// vectors
+// ---------------------------------------------------------------------------
+int64_t tnx_reduce_scratch_len(void) { return reduce_partials_count(); }
+
+int tnx_dot(const double* x, const double* y, int64_t n, double* result, double* scratch, void* stream) {
+  TNX_TRY({
+    launch_dot(x, y, n, 0, result, scratch, nullptr, static_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
+
+int tnx_nrm2(const double* x, int64_t n, double* result, double* scratch, void* stream) {
+  TNX_TRY({
+    launch_dot(x, x, n, 1, result, scratch, nullptr, static_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
+
+int tnx_lanczos_step(double* w, const double* v, const double* v_prev, double* v_next, int64_t n, double* alpha,
+                     double* beta, int32_t k, double tol, int32_t* done, double* scratch, void* stream) {
+  TNX_TRY({
+    launch_lanczos_step(w, v, k > 0 ? v_prev : nullptr, v_next, n, alpha + k, beta + k + 1, beta + k, tol, done,
+                        scratch, static_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
+
+int tnx_combine(const double* const* basis_dev_table, const double* coefs_dev, int32_t n_vec, int64_t n, double* out,
+                void* stream) {
+  TNX_TRY({
+    launch_combine(basis_dev_table, coefs_dev, n_vec, n, out, static_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
+
+int tnx_scale(const double* x, double* out, int64_t n, const double* scale_dev, int32_t mode, void* stream) {
+  TNX_TRY({
+    launch_scale(x, out, n, scale_dev, mode, nullptr, static_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
+
+}  // extern "C"

@@ -1,0 +1,176 @@
+// Device-side shared definitions: operand-image layouts, table structs,
+// and thin PTX wrappers (mbarrier, bulk copy, tcgen05) with bounded waits.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tnx {
+
+// ---------------------------------------------------------------------------
+// GEMM operand images.  A group's operand matrix (rows x K, K contiguous) is
+// stored as consecutive tiles, tile (rt, kt) at index rt * nKt + kt; a tile is
+// the exact shared-memory image the MMA consumes, so it moves with one bulk
+// copy.  Padding rows/cols are zero.
+//   FP64   : 64 x 16 doubles, element (r,k) at r*16 + (k ^ ((r & 3) << 2))
+//            (XOR spreads the DMMA fragment loads over all banks)
+//   BF16   : 128 x 64 bf16, byte r*128 + (((2k)>>4) ^ (r&7))*16 + (2k & 15)
+//            (the SWIZZLE_128B K-major canonical layout of tcgen05)
+//   TF32   : 128 x 32 fp32, byte r*128 + (((4k)>>4) ^ (r&7))*16 + (4k & 15)
+// ---------------------------------------------------------------------------
+enum ImgMode { IMG_F64 = 0, IMG_BF16 = 1, IMG_TF32 = 2 };
+
+struct ImgGeom {
+  int tm, tk, tile_bytes, elem_bytes;
+};
+
+__host__ __device__ inline ImgGeom img_geom(int mode) {
+  if (mode == IMG_F64) return {64, 16, 8192, 8};
+  if (mode == IMG_BF16) return {128, 64, 16384, 2};
+  return {128, 32, 16384, 4};
+}
+
+// byte offset of element (row, k) inside a group image starting at tile0
+__host__ __device__ inline int64_t img_byte_offset(int mode, int64_t tile0, int nKt, int64_t row, int64_t k) {
+  if (mode == IMG_F64) {
+    int64_t rt = row >> 6, kt = k >> 4;
+    int r = static_cast<int>(row & 63), kk = static_cast<int>(k & 15);
+    int64_t tile = tile0 + rt * nKt + kt;
+    return tile * 8192 + static_cast<int64_t>(r * 16 + (kk ^ ((r & 3) << 2))) * 8;
+  }
+  if (mode == IMG_BF16) {
+    int64_t rt = row >> 7, kt = k >> 6;
+    int r = static_cast<int>(row & 127), kb = static_cast<int>(k & 63) * 2;
+    int64_t tile = tile0 + rt * nKt + kt;
+    return tile * 16384 + r * 128 + (((kb >> 4) ^ (r & 7)) << 4) + (kb & 15);
+  }
+  int64_t rt = row >> 7, kt = k >> 5;
+  int r = static_cast<int>(row & 127), kb = static_cast<int>(k & 31) * 4;
+  int64_t tile = tile0 + rt * nKt + kt;
+  return tile * 16384 + r * 128 + (((kb >> 4) ^ (r & 7)) << 4) + (kb & 15);
+}
+
+// ---------------------------------------------------------------------------
+// device tables
+// ---------------------------------------------------------------------------
+constexpr int kMaxLegsDev = 8;
+
+struct DevPackSeg {
+  int64_t src_off;    // element offset of the block in operand buffer src_tab[src_slot]
+  uint64_t img_addr;  // absolute address of the destination group image (tile 0)
+  int64_t lo_off;     // byte offset of the low-part image (BF16 split) from img_addr
+  int32_t row0, k0, nKt, nlegs;
+  int32_t src_slot, pad;
+  int32_t dims[kMaxLegsDev];
+  int32_t rstr[kMaxLegsDev];
+  int32_t kstr[kMaxLegsDev];
+};
+
+struct DevScatSeg {
+  int64_t dst_off;
+  int64_t src_base;  // element offset of (row0, col0) in the result scratch
+  int64_t ld;
+  int32_t nlegs, pad;
+  int32_t dims[kMaxLegsDev];
+  int32_t rstr[kMaxLegsDev];
+  int32_t cstr[kMaxLegsDev];
+};
+
+struct DevChunk {  // one CTA's share of a segment list
+  int32_t seg;
+  int32_t pad;
+  int64_t start;
+  int64_t count;
+};
+
+struct DevGroup {
+  uint64_t a_addr, b_addr;  // absolute addresses of the group's A / B images
+  int64_t a_lo, b_lo;       // byte offsets of the low-part images (BF16 split)
+  int64_t rowoff0;          // index of row 0 in the row-offset table
+  int32_t M, N, nKt, out_slot;  // result rows go to out_tab[out_slot] + rowoff[.] + col
+};
+
+struct DevTile {
+  int32_t g, mt, nt, pad;
+};
+
+struct DevMpoPair {
+  int32_t mc, md;
+  int32_t in0, n_in;
+  int32_t out0, n_out;
+  int32_t term0, n_terms;
+  int32_t n_in_slots, n_out_slots;
+};
+struct DevMpoIn {
+  uint64_t x1_addr;  // absolute address of element (b=0,c=0,p=0,q=0,d=0) of the stage-1 result
+  int64_t ld;
+  int32_t mb, mp, mq, slot0;
+};
+struct DevMpoOutSlot {  // one output slot (s,t,f) of one X3 block
+  uint64_t img_addr;    // stage-4 A image of the group (tile 0)
+  int64_t lo_off;
+  int32_t nKt, row0, k0, rows_per_c, row_add, k_add;
+};
+struct DevMpoTerm {
+  int32_t out_slot, in_slot;
+  double w;
+};
+
+// ---------------------------------------------------------------------------
+// PTX wrappers (sm_100a)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: returns false (and never blocks forever) after max_polls.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t max_polls) {
+  for (uint32_t i = 0; i < max_polls; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// 1-D bulk async copy global -> shared, completion counted on an mbarrier.
+__device__ __forceinline__ void bulk_g2s(void* smem_dst, const void* gmem_src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(smem_dst)),
+      "l"(gmem_src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+
+}  // namespace tnx

@@ -1,0 +1,328 @@
+// Persistent grouped GEMM on the 5th-generation tensor cores (tcgen05 + TMEM).
+//
+// C_g[row, col] = sum_k A_g[row, k] * B_g[col, k] over every sector group g,
+// one work-list entry per 128x128 output tile.  Operands are pre-swizzled
+// SWIZZLE_128B K-major image tiles (16 KB each) moved by 1-D bulk async copies
+// (cp.async.bulk, no tensor map, no multicast) into a STAGES-deep ring.
+//   BF16X3: A = A_hi + A_lo, B = B_hi + B_lo (bf16 splits of FP64 data);
+//           acc += A_hi B_hi + A_hi B_lo + A_lo B_hi, FP32 accumulation in TMEM.
+//   TF32:   acc += A B with kind::tf32.
+// Warp roles: warp 0 = copy producer, warp 1 = TMEM owner + single-thread MMA
+// issuer, warps 2..5 = epilogue (TMEM -> registers -> global through a
+// per-row offset table).  Two TMEM accumulators let the epilogue of tile i
+// overlap the MMAs of tile i+1.  Every wait is bounded by a globaltimer
+// deadline; on expiry the kernel raises *err_flag, drains its own copies and
+// MMAs, frees TMEM and returns.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace tnx {
+
+namespace {
+constexpr int TBM = 128, TBN = 128;
+constexpr int TILE_BYTES = 16384;
+constexpr int THREADS = 192;
+constexpr int TMEM_COLS = 2 * TBN;
+constexpr uint64_t kTimeoutNs = 2000000000ull;  // 2 s per wait
+
+__device__ __forceinline__ uint64_t gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// wait for phase `parity` of `bar`; false on abort (own deadline or another role's abort)
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                              int32_t* err_flag) {
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 255u) == 255u) {
+      if (*abort_flag) return false;
+      uint64_t now = gtimer();
+      if (t0 == 0) t0 = now;
+      if (now - t0 > kTimeoutNs) {
+        *abort_flag = 1;
+        if (err_flag) atomicExch(err_flag, 1);
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4);  // start address
+  d |= static_cast<uint64_t>(1) << 16;                  // LBO (unused for SW128 K-major)
+  d |= static_cast<uint64_t>(1024 >> 4) << 32;          // SBO: 8 rows x 128 B
+  d |= static_cast<uint64_t>(1) << 46;                  // descriptor version (sm_100)
+  d |= static_cast<uint64_t>(2) << 61;                  // SWIZZLE_128B
+  return d;
+}
+
+template <bool TF32>
+__device__ __forceinline__ void mma_issue(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  if constexpr (TF32) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\ntcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\ntcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+  }
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <bool TF32, typename OutT>
+__global__ void __launch_bounds__(THREADS, 1)
+    gemm_tc_kernel(const DevGroup* __restrict__ groups, const DevTile* __restrict__ tiles, int n_tiles,
+                   const int64_t* __restrict__ rowoff, const uint64_t* __restrict__ out_tab, int32_t* err_flag,
+                   const int32_t* __restrict__ skip) {
+  constexpr int NT = TF32 ? 2 : 4;          // operand tiles per stage
+  constexpr int STAGES = TF32 ? 6 : 3;      // 192 KB of operand ring either way
+  constexpr int KSUB = 4;                   // MMAs per 128-byte K slab (32 B each)
+  if (skip && *skip) return;
+
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw_addr = smem_u32(smem_raw);
+  uint8_t* smem = smem_raw + ((1024u - (raw_addr & 1023u)) & 1023u);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * NT * TILE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* tfull = empty + STAGES;
+  uint64_t* tempty = tfull + 2;
+  uint64_t* drain = tempty + 2;
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&tfull[a], 1);
+      mbar_init(&tempty[a], 128);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_holder)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_holder;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      int last_par[STAGES];
+      for (int i = 0; i < STAGES; ++i) last_par[i] = -1;
+      bool ok = true;
+      for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+        const DevTile tl = tiles[t];
+        const DevGroup g = groups[tl.g];
+        const uint8_t* ga = reinterpret_cast<const uint8_t*>(g.a_addr) + static_cast<int64_t>(tl.mt) * g.nKt * TILE_BYTES;
+        const uint8_t* gb = reinterpret_cast<const uint8_t*>(g.b_addr) + static_cast<int64_t>(tl.nt) * g.nKt * TILE_BYTES;
+        for (int kt = 0; kt < g.nKt; ++kt) {
+          if (!wait_or_abort(&empty[s], ph ^ 1u, abort_flag, err_flag)) {
+            ok = false;
+            break;
+          }
+          uint8_t* st = smem + s * NT * TILE_BYTES;
+          mbar_expect_tx(&full[s], NT * TILE_BYTES);
+          const int64_t ko = static_cast<int64_t>(kt) * TILE_BYTES;
+          bulk_g2s(st, ga + ko, TILE_BYTES, &full[s]);
+          if (TF32) {
+            bulk_g2s(st + TILE_BYTES, gb + ko, TILE_BYTES, &full[s]);
+          } else {
+            bulk_g2s(st + TILE_BYTES, ga + g.a_lo + ko, TILE_BYTES, &full[s]);
+            bulk_g2s(st + 2 * TILE_BYTES, gb + ko, TILE_BYTES, &full[s]);
+            bulk_g2s(st + 3 * TILE_BYTES, gb + g.b_lo + ko, TILE_BYTES, &full[s]);
+          }
+          last_par[s] = static_cast<int>(ph);
+          if (++s == STAGES) {
+            s = 0;
+            ph ^= 1u;
+          }
+        }
+      }
+      if (!ok) {
+        // let every copy this thread issued land before the CTA exits
+        for (int i = 0; i < STAGES; ++i) {
+          if (last_par[i] < 0) continue;
+          uint64_t t0 = gtimer();
+          while (!mbar_try_wait(&full[i], static_cast<uint32_t>(last_par[i])) && gtimer() - t0 < kTimeoutNs) {
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = (1u << 4) | ((TF32 ? 2u : 1u) << 7) | ((TF32 ? 2u : 1u) << 10) |
+                             (static_cast<uint32_t>(TBN >> 3) << 17) | (static_cast<uint32_t>(TBM >> 4) << 24);
+      int s = 0;
+      uint32_t ph = 0;
+      int acc = 0;
+      uint32_t aph = 0;
+      bool ok = true;
+      bool issued = false;
+      for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+        const DevGroup g = groups[tiles[t].g];
+        if (!wait_or_abort(&tempty[acc], aph ^ 1u, abort_flag, err_flag)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d_tmem = tmem_base + static_cast<uint32_t>(acc * TBN);
+        for (int kt = 0; kt < g.nKt; ++kt) {
+          if (!wait_or_abort(&full[s], ph, abort_flag, err_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sa = smem_u32(smem + s * NT * TILE_BYTES);
+          const uint64_t da = sw128_desc(sa);
+          if (TF32) {
+            const uint64_t db = sw128_desc(sa + TILE_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < KSUB; ++kk)
+              mma_issue<TF32>(d_tmem, da + 2 * kk, db + 2 * kk, idesc, (kt | kk) ? 1u : 0u);
+          } else {
+            const uint64_t dal = sw128_desc(sa + TILE_BYTES);
+            const uint64_t db = sw128_desc(sa + 2 * TILE_BYTES);
+            const uint64_t dbl = sw128_desc(sa + 3 * TILE_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < KSUB; ++kk) {
+              mma_issue<TF32>(d_tmem, da + 2 * kk, db + 2 * kk, idesc, (kt | kk) ? 1u : 0u);
+              mma_issue<TF32>(d_tmem, da + 2 * kk, dbl + 2 * kk, idesc, 1u);
+              mma_issue<TF32>(d_tmem, dal + 2 * kk, db + 2 * kk, idesc, 1u);
+            }
+          }
+          issued = true;
+          mma_commit(&empty[s]);
+          if (++s == STAGES) {
+            s = 0;
+            ph ^= 1u;
+          }
+        }
+        if (!ok) break;
+        mma_commit(&tfull[acc]);
+        if (++acc == 2) {
+          acc = 0;
+          aph ^= 1u;
+        }
+      }
+      if (!ok && issued) {
+        // wait for every MMA this thread issued before TMEM is freed
+        mma_commit(drain);
+        uint64_t t0 = gtimer();
+        while (!mbar_try_wait(drain, 0) && gtimer() - t0 < kTimeoutNs) {
+        }
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int r_in_tile = q * 32 + lane;
+    int acc = 0;
+    uint32_t aph = 0;
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+      const DevTile tl = tiles[t];
+      const DevGroup g = groups[tl.g];
+      // all lanes wait (the tcgen05.ld below is warp-collective)
+      if (!wait_or_abort(&tfull[acc], aph, abort_flag, err_flag)) break;
+      tc_fence_after();
+      const int row = tl.mt * TBM + r_in_tile;
+      const int64_t ro = row < g.M ? rowoff[g.rowoff0 + row] : -1;
+      OutT* out = reinterpret_cast<OutT*>(out_tab[g.out_slot]);
+      const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * TBN);
+#pragma unroll 1
+      for (int c0 = 0; c0 < TBN; c0 += 16) {
+        uint32_t v[16];
+        tmem_ld16(tbase + c0, v);
+        if (ro >= 0) {
+          const int col0 = tl.nt * TBN + c0;
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (col0 + j < g.N) out[ro + col0 + j] = static_cast<OutT>(__uint_as_float(v[j]));
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&tempty[acc]);
+      if (++acc == 2) {
+        acc = 0;
+        aph ^= 1u;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS)
+                 : "memory");
+  }
+}
+
+template <bool TF32, typename OutT>
+void launch_tc_impl(const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
+                    const uint64_t* out_tab, int32_t* err_flag, const int32_t* skip, cudaStream_t st) {
+  constexpr int NT = TF32 ? 2 : 4;
+  constexpr int STAGES = TF32 ? 6 : 3;
+  const int smem = STAGES * NT * TILE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+  cudaFuncSetAttribute(gemm_tc_kernel<TF32, OutT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  int grid = device_sm_count();
+  if (grid > n_tiles) grid = n_tiles;
+  gemm_tc_kernel<TF32, OutT>
+      <<<grid, THREADS, smem, st>>>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip);
+}
+}  // namespace
+
+void launch_gemm_tc(int mode, const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
+                    const uint64_t* out_tab, bool out_f64, int32_t* err_flag, const int32_t* skip, cudaStream_t st) {
+  if (n_tiles <= 0) return;
+  if (mode == IMG_TF32) {
+    if (out_f64)
+      launch_tc_impl<true, double>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st);
+    else
+      launch_tc_impl<true, float>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st);
+  } else {
+    if (out_f64)
+      launch_tc_impl<false, double>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st);
+    else
+      launch_tc_impl<false, float>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st);
+  }
+}
+
+}  // namespace tnx

@@ -1,0 +1,305 @@
+// HBM-bound kernels: operand-image packing, result scatter, the fused MPO
+// application of the two-site H_eff, and FP64 vector primitives.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace tnx {
+
+// ---------------------------------------------------------------------------
+// image stores
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void img_store(int mode, uint8_t* img, int64_t lo_offset, int64_t tile0, int nKt,
+                                          int64_t row, int64_t k, double v) {
+  int64_t off = img_byte_offset(mode, tile0, nKt, row, k);
+  if (mode == IMG_F64) {
+    *reinterpret_cast<double*>(img + off) = v;
+  } else if (mode == IMG_BF16) {
+    __nv_bfloat16 hi = __double2bfloat16(v);
+    __nv_bfloat16 lo = __double2bfloat16(v - static_cast<double>(__bfloat162float(hi)));
+    *reinterpret_cast<__nv_bfloat16*>(img + off) = hi;
+    *reinterpret_cast<__nv_bfloat16*>(img + lo_offset + off) = lo;
+  } else {
+    float f = static_cast<float>(v);
+    uint32_t t;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(f));
+    *reinterpret_cast<uint32_t*>(img + off) = t;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pack: operand blocks -> group operand images
+// ---------------------------------------------------------------------------
+__global__ void pack_image_kernel(const uint64_t* __restrict__ src_tab, const DevPackSeg* __restrict__ segs,
+                                  const DevChunk* __restrict__ chunks, int mode, const int32_t* __restrict__ skip) {
+  if (skip && *skip) return;
+  const DevChunk ch = chunks[blockIdx.x];
+  const DevPackSeg& s = segs[ch.seg];
+  const double* src = reinterpret_cast<const double*>(src_tab[s.src_slot]) + s.src_off;
+  uint8_t* img = reinterpret_cast<uint8_t*>(s.img_addr);
+  for (int64_t e = ch.start + threadIdx.x; e < ch.start + ch.count; e += blockDim.x) {
+    int64_t rem = e, row = s.row0, k = s.k0;
+    for (int l = s.nlegs - 1; l >= 0; --l) {
+      int64_t d = s.dims[l];
+      int64_t idx = rem % d;
+      rem /= d;
+      row += idx * s.rstr[l];
+      k += idx * s.kstr[l];
+    }
+    img_store(mode, img, s.lo_off, 0, s.nKt, row, k, src[e]);
+  }
+}
+
+void launch_pack(const uint64_t* src_tab, const DevPackSeg* segs, const DevChunk* chunks, int n_chunks, int mode,
+                 const int32_t* skip, cudaStream_t st) {
+  if (n_chunks <= 0) return;
+  pack_image_kernel<<<n_chunks, 256, 0, st>>>(src_tab, segs, chunks, mode, skip);
+}
+
+// ---------------------------------------------------------------------------
+// scatter: group result matrices -> output blocks (any leg permutation)
+// ---------------------------------------------------------------------------
+template <typename TS>
+__global__ void scatter_kernel(const TS* __restrict__ res, double* __restrict__ out,
+                               const DevScatSeg* __restrict__ segs, const DevChunk* __restrict__ chunks) {
+  const DevChunk ch = chunks[blockIdx.x];
+  const DevScatSeg& s = segs[ch.seg];
+  for (int64_t e = ch.start + threadIdx.x; e < ch.start + ch.count; e += blockDim.x) {
+    int64_t rem = e, row = 0, col = 0;
+    for (int l = s.nlegs - 1; l >= 0; --l) {
+      int64_t d = s.dims[l];
+      int64_t idx = rem % d;
+      rem /= d;
+      row += idx * s.rstr[l];
+      col += idx * s.cstr[l];
+    }
+    out[s.dst_off + e] = static_cast<double>(res[s.src_base + row * s.ld + col]);
+  }
+}
+
+void launch_scatter(const void* res, bool res_f32, double* out, const DevScatSeg* segs, const DevChunk* chunks,
+                    int n_chunks, cudaStream_t st) {
+  if (n_chunks <= 0) return;
+  if (res_f32)
+    scatter_kernel<float><<<n_chunks, 256, 0, st>>>(static_cast<const float*>(res), out, segs, chunks);
+  else
+    scatter_kernel<double><<<n_chunks, 256, 0, st>>>(static_cast<const double*>(res), out, segs, chunks);
+}
+
+// ---------------------------------------------------------------------------
+// fused MPO application (stages 2+3 of the two-site H_eff):
+//   X3[c,s,t,f,d] = sum_{b,p,q} Wlr[b,p,q,s,t,f] X1[b,c,p,q,d]
+// One CTA = 128 points (c,d) of one (qc,qd) pair; the point's input vector
+// is staged column-wise in shared memory, the sparse Wlr terms (uniform over
+// the CTA) accumulate per output slot, results go straight into the stage-4
+// A-operand image.
+// ---------------------------------------------------------------------------
+constexpr int kMpoPoints = 128;
+
+template <typename TI>
+__global__ void __launch_bounds__(kMpoPoints) mpo_apply_kernel(
+    int mode, const DevMpoPair* __restrict__ pairs, const DevMpoIn* __restrict__ ins,
+    const DevMpoOutSlot* __restrict__ oslots, const DevMpoTerm* __restrict__ terms,
+    const int2* __restrict__ chunks, const int32_t* __restrict__ skip) {
+  if (skip && *skip) return;
+  extern __shared__ __align__(16) unsigned char mpo_smem[];
+  TI* xs = reinterpret_cast<TI*>(mpo_smem);
+  const int2 ch = chunks[blockIdx.x];
+  const DevMpoPair pr = pairs[ch.x];
+  const int npts = pr.mc * pr.md;
+  const int p = ch.y + threadIdx.x;
+  const bool valid = p < npts;
+  const int c = valid ? p / pr.md : 0;
+  const int d = valid ? p % pr.md : 0;
+  // phase 1: inputs of this point
+  for (int i = 0; i < pr.n_in; ++i) {
+    const DevMpoIn in = ins[pr.in0 + i];
+    const int nq = in.mq;
+    const int npq = in.mp * in.mq;
+    for (int j = 0; j < in.mb * npq; ++j) {
+      int b = j / npq, pq = j - b * npq;
+      int pp = pq / nq, q = pq - pp * nq;
+      TI v = TI(0);
+      if (valid)
+        v = reinterpret_cast<const TI*>(in.x1_addr)[(static_cast<int64_t>(b) * pr.mc + c) * in.ld + (pp * nq + q) * pr.md + d];
+      xs[(in.slot0 + j) * kMpoPoints + threadIdx.x] = v;
+    }
+  }
+  // phase 2: sparse terms sorted by output slot
+  double acc = 0.0;
+  int cur = -1;
+  for (int t = 0; t < pr.n_terms; ++t) {
+    const DevMpoTerm tm = terms[pr.term0 + t];
+    if (tm.out_slot != cur) {
+      if (cur >= 0 && valid) {
+        const DevMpoOutSlot o = oslots[pr.out0 + cur];
+        img_store(mode, reinterpret_cast<uint8_t*>(o.img_addr), o.lo_off, 0, o.nKt,
+                  o.row0 + static_cast<int64_t>(c) * o.rows_per_c + o.row_add, o.k0 + o.k_add + d, acc);
+      }
+      cur = tm.out_slot;
+      acc = 0.0;
+    }
+    acc += tm.w * static_cast<double>(xs[tm.in_slot * kMpoPoints + threadIdx.x]);
+  }
+  if (cur >= 0 && valid) {
+    const DevMpoOutSlot o = oslots[pr.out0 + cur];
+    img_store(mode, reinterpret_cast<uint8_t*>(o.img_addr), o.lo_off, 0, o.nKt,
+              o.row0 + static_cast<int64_t>(c) * o.rows_per_c + o.row_add, o.k0 + o.k_add + d, acc);
+  }
+}
+
+void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevMpoIn* ins, const DevMpoOutSlot* oslots,
+                      const DevMpoTerm* terms, const int2* chunks, int n_chunks, int max_in_slots,
+                      const int32_t* skip, cudaStream_t st) {
+  if (n_chunks <= 0) return;
+  size_t smem = static_cast<size_t>(max_in_slots) * kMpoPoints * (x1_f32 ? 4 : 8);
+  if (x1_f32) {
+    cudaFuncSetAttribute(mpo_apply_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    mpo_apply_kernel<float><<<n_chunks, kMpoPoints, smem, st>>>(mode, pairs, ins, oslots, terms, chunks, skip);
+  } else {
+    cudaFuncSetAttribute(mpo_apply_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    mpo_apply_kernel<double><<<n_chunks, kMpoPoints, smem, st>>>(mode, pairs, ins, oslots, terms, chunks, skip);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 vector primitives: deterministic two-pass reductions
+// ---------------------------------------------------------------------------
+constexpr int kRedBlocks = 592;  // 4 x 148 SMs
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double ws[32];
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) ws[w] = v;
+  __syncthreads();
+  v = (threadIdx.x < (blockDim.x >> 5)) ? ws[threadIdx.x] : 0.0;
+  if (w == 0) v = warp_sum(v);
+  return v;
+}
+
+// kind 0: sum x*y; kind 1: sum x*x
+__global__ void partial_dot_kernel(const double* __restrict__ x, const double* __restrict__ y, int64_t n, int kind,
+                                   double* __restrict__ partials, const int32_t* __restrict__ skip) {
+  if (skip && *skip) return;
+  double acc = 0.0;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const int64_t n2 = n / 2;
+  const double2* x2 = reinterpret_cast<const double2*>(x);
+  const double2* y2 = reinterpret_cast<const double2*>(y);
+  bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
+  if (aligned) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n2; i += stride) {
+      double2 a = x2[i];
+      double2 b = kind ? a : y2[i];
+      acc += a.x * b.x + a.y * b.y;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && (n & 1)) acc += x[n - 1] * (kind ? x[n - 1] : y[n - 1]);
+  } else {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride)
+      acc += x[i] * (kind ? x[i] : y[i]);
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+// final: result = sum partials (op 0), sqrt(sum) (op 1)
+__global__ void finish_sum_kernel(const double* __restrict__ partials, int np, double* __restrict__ result, int op,
+                                  const int32_t* __restrict__ skip) {
+  if (skip && *skip) return;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) acc += partials[i];
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) *result = op == 1 ? sqrt(acc) : acc;
+}
+
+void launch_dot(const double* x, const double* y, int64_t n, int kind, double* result, double* partials,
+                const int32_t* skip, cudaStream_t st) {
+  partial_dot_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(x, y, n, kind, partials, skip);
+  finish_sum_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, result, kind, skip);
+}
+
+// w -= alpha v (+ beta v_prev); partial sums of w*w
+__global__ void lanczos_axpy_kernel(double* __restrict__ w, const double* __restrict__ v,
+                                    const double* __restrict__ vp, int64_t n, const double* __restrict__ alpha,
+                                    const double* __restrict__ beta, double* __restrict__ partials,
+                                    const int32_t* __restrict__ skip) {
+  if (skip && *skip) return;
+  const double a = *alpha;
+  const double b = vp ? *beta : 0.0;
+  double acc = 0.0;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride) {
+    double x = w[i] - v[i] * a;
+    if (vp) x = x - vp[i] * b;
+    w[i] = x;
+    acc += x * x;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+__global__ void lanczos_beta_kernel(const double* __restrict__ partials, int np, double* __restrict__ beta_out,
+                                    double tol, int32_t* __restrict__ done) {
+  if (*done) return;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) acc += partials[i];
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) {
+    double b = sqrt(acc);
+    *beta_out = b;
+    if (b < tol) *done = 1;
+  }
+}
+
+__global__ void scale_into_kernel(const double* __restrict__ w, double* __restrict__ out, int64_t n,
+                                  const double* __restrict__ s, int mode, const int32_t* __restrict__ skip) {
+  if (skip && *skip) return;
+  // mode 0: out = w * s; mode 1: out = w / s; mode 2: out = w * (1 / (s + 1e-15))
+  double f = *s;
+  if (mode == 2) f = 1.0 / (f + 1e-15);
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride)
+    out[i] = mode == 1 ? w[i] * (1.0 / f) : w[i] * f;
+}
+
+void launch_lanczos_step(double* w, const double* v, const double* vp, double* vnext, int64_t n, double* alpha,
+                         double* beta_next, const double* beta_prev, double tol, int32_t* done, double* partials,
+                         cudaStream_t st) {
+  // alpha = <v, w>
+  partial_dot_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(v, w, n, 0, partials, done);
+  finish_sum_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, alpha, 0, done);
+  lanczos_axpy_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(w, v, vp, n, alpha, beta_prev, partials, done);
+  lanczos_beta_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, beta_next, tol, done);
+  if (vnext) scale_into_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(w, vnext, n, beta_next, 1, done);
+}
+
+void launch_scale(const double* w, double* out, int64_t n, const double* s, int mode, const int32_t* skip,
+                  cudaStream_t st) {
+  scale_into_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(w, out, n, s, mode, skip);
+}
+
+__global__ void combine_kernel(const double* const* __restrict__ basis, const double* __restrict__ coefs, int nv,
+                               int64_t n, double* __restrict__ out) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride) {
+    // same association as the reference: ((b0 c0 + b1 c1) + b2 c2) + ...
+    double acc = basis[0][i] * coefs[0];
+    for (int k = 1; k < nv; ++k) acc = acc + basis[k][i] * coefs[k];
+    out[i] = acc;
+  }
+}
+
+void launch_combine(const double* const* basis, const double* coefs, int nv, int64_t n, double* out,
+                    cudaStream_t st) {
+  combine_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(basis, coefs, nv, n, out);
+}
+
+int reduce_partials_count() { return kRedBlocks; }
+
+}  // namespace tnx

@@ -1,0 +1,37 @@
+// Host-side launch wrappers of the device kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace tnx {
+
+void launch_pack(const uint64_t* src_tab, const DevPackSeg* segs, const DevChunk* chunks, int n_chunks, int mode,
+                 const int32_t* skip, cudaStream_t st);
+void launch_scatter(const void* res, bool res_f32, double* out, const DevScatSeg* segs, const DevChunk* chunks,
+                    int n_chunks, cudaStream_t st);
+void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevMpoIn* ins, const DevMpoOutSlot* oslots,
+                      const DevMpoTerm* terms, const int2* chunks, int n_chunks, int max_in_slots,
+                      const int32_t* skip, cudaStream_t st);
+void launch_dot(const double* x, const double* y, int64_t n, int kind, double* result, double* partials,
+                const int32_t* skip, cudaStream_t st);
+void launch_lanczos_step(double* w, const double* v, const double* vp, double* vnext, int64_t n, double* alpha,
+                         double* beta_next, const double* beta_prev, double tol, int32_t* done, double* partials,
+                         cudaStream_t st);
+void launch_scale(const double* w, double* out, int64_t n, const double* s, int mode, const int32_t* skip,
+                  cudaStream_t st);
+void launch_combine(const double* const* basis, const double* coefs, int nv, int64_t n, double* out,
+                    cudaStream_t st);
+int reduce_partials_count();
+
+// grouped GEMMs: out_tab[g.out_slot][rowoff[g.rowoff0 + row] + col] = sum_k A_g[row,k] B_g[col,k]
+void launch_gemm_f64(const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
+                     const uint64_t* out_tab, const int32_t* skip, cudaStream_t st);
+// tcgen05 grouped GEMM; mode IMG_BF16 (3 products over hi/lo images) or IMG_TF32
+void launch_gemm_tc(int mode, const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
+                    const uint64_t* out_tab, bool out_f64, int32_t* err_flag, const int32_t* skip, cudaStream_t st);
+int device_sm_count();
+
+}  // namespace tnx

@@ -1,0 +1,147 @@
+"""Two-site effective-Hamiltonian matvec on the GPU.
+
+``Y[c,s,t,g] = L[a,b,c] th[a,p,q,d] W_l[b,p,s,e] W_r[e,q,t,f] R[d,f,g]``
+(tenax algorithms/dmrg.py:1282-1289, evaluated there by
+``_blockwise_contract`` one block combination at a time).  Here it runs as
+three stages over all sectors at once:
+
+1. ``X1 = L . th`` over a -- grouped sector GEMM (DMMA FP64 or tcgen05),
+2. ``X3 = (W_l W_r) . X1`` over (b,p,q) -- fused sparse MPO kernel that
+   writes the stage-3 operand images directly,
+3. ``Y = X3 . R`` over (f,d) -- grouped sector GEMM whose epilogue writes
+   the theta block layout.
+
+Operator images (L, R, W_l W_r terms) are packed once per site; a matvec
+only packs theta.  Many independent problems share each launch
+(``HeffBatch``).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from tenax_b200 import _capi
+from tenax_b200.tensor import SymmetricTensor
+
+
+def _desc(t_indices, keys):
+    return _capi.DescHolder([i.charges for i in t_indices], [int(i.flow) for i in t_indices], keys, None)
+
+
+def _create(L, th_indices, th_keys, Wl, Wr, R):
+    hold = [_desc(L.indices, L.keys), _desc(th_indices, th_keys), _desc(Wl.indices, Wl.keys),
+            _desc(Wr.indices, Wr.keys), _desc(R.indices, R.keys)]
+    h = C.c_void_p()
+    _capi.check(_capi.LIB.tnx_heff_create(*[C.byref(x.desc) for x in hold], C.byref(h)))
+    return h, hold
+
+
+def _out_keys(h):
+    n = C.c_int64()
+    _capi.check(_capi.LIB.tnx_heff_out_keys(h, C.byref(n), None))
+    buf = np.zeros(max(1, 4 * n.value), dtype=np.int32)
+    _capi.check(_capi.LIB.tnx_heff_out_keys(h, C.byref(n), buf.ctypes.data))
+    return [tuple(int(q) for q in r) for r in buf[: 4 * n.value].reshape(-1, 4)]
+
+
+def heff_key_closure(L, th_indices, th_keys, Wl, Wr, R, max_iter: int = 64):
+    """Key sets K_0 = theta's keys, K_{k+1} = K_k | out(K_k), up to the fixed point.
+
+    The reference's Lanczos grows the key set of its Krylov vectors exactly
+    this way (key-union addition, core/tensor.py:933-952, of matvec outputs
+    whose keys are never filtered, dmrg.py:1097).
+    """
+    seq = [sorted(th_keys)]
+    for _ in range(max_iter):
+        h, _hold = _create(L, th_indices, seq[-1], Wl, Wr, R)
+        out = _out_keys(h)
+        _capi.LIB.tnx_heff_destroy(h)
+        nxt = sorted(set(seq[-1]) | set(out))
+        if nxt == seq[-1]:
+            return seq
+        seq.append(nxt)
+    raise RuntimeError("H_eff key closure did not converge")
+
+
+class HeffOperator:
+    """H_eff of one two-site problem; theta/outputs live on a closed key set."""
+
+    def __init__(self, L: SymmetricTensor, Wl: SymmetricTensor, Wr: SymmetricTensor, R: SymmetricTensor,
+                 theta_indices, theta_keys, precision: str = "fp64"):
+        self.theta_indices = tuple(theta_indices)
+        self.key_seq = heff_key_closure(L, theta_indices, theta_keys, Wl, Wr, R)
+        self.keys = self.key_seq[-1]
+        self.handle, self._hold = _create(L, theta_indices, self.keys, Wl, Wr, R)
+        closed = C.c_int32()
+        _capi.check(_capi.LIB.tnx_heff_closed(self.handle, C.byref(closed)))
+        if not closed.value:
+            raise _capi.TnxUnsupported("H_eff sector structure outside the fused path (a stage-4 group spans "
+                                       "several output charges)")
+        self.precision = precision
+        self.flops = float(_capi.LIB.tnx_heff_flops(self.handle))
+        _capi.check(_capi.LIB.tnx_heff_set_operators(self.handle, L.data.data_ptr(), Wl.data.data_ptr(),
+                                                     Wr.data.data_ptr(), R.data.data_ptr(),
+                                                     _capi.PRECISIONS[precision],
+                                                     torch.cuda.current_stream().cuda_stream))
+        sizes = [int(np.prod([int(np.count_nonzero(i.charges == q)) for i, q in zip(self.theta_indices, k)]))
+                 for k in self.keys]
+        self.size = int(sum(sizes))
+        self._batch = None
+
+    def out_like(self) -> torch.Tensor:
+        return torch.empty(self.size, dtype=torch.float64, device=torch.device("cuda", torch.cuda.current_device()))
+
+    def apply(self, x: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        if self._batch is None:
+            self._batch = HeffBatch([self])
+        if out is None:
+            out = self.out_like()
+        self._batch.apply([x], [out])
+        return out
+
+    def __del__(self):
+        if getattr(self, "handle", None) is not None and _capi.LIB is not None:
+            self._batch = None
+            _capi.LIB.tnx_heff_destroy(self.handle)
+            self.handle = None
+
+
+class HeffBatch:
+    """Independent H_eff problems applied together: one launch per stage."""
+
+    def __init__(self, ops, skip_flag: torch.Tensor | None = None):
+        self.ops = list(ops)
+        prec = {o.precision for o in self.ops}
+        if len(prec) != 1:
+            raise ValueError("all problems of a batch must use one precision")
+        self.precision = prec.pop()
+        arr = (C.c_void_p * len(self.ops))(*[o.handle for o in self.ops])
+        h = C.c_void_p()
+        _capi.check(_capi.LIB.tnx_heff_batch_create(arr, len(self.ops), _capi.PRECISIONS[self.precision],
+                                                    C.byref(h)))
+        self.handle = h
+        self.skip_flag = skip_flag
+        if skip_flag is not None:
+            _capi.check(_capi.LIB.tnx_heff_batch_set_skip_flag(h, skip_flag.data_ptr()))
+        n = C.c_int32()
+        _capi.check(_capi.LIB.tnx_heff_batch_launches(h, C.byref(n)))
+        self.launches_per_apply = n.value
+        self.flops = sum(o.flops for o in self.ops)
+
+    def apply(self, thetas, outs):
+        tp = (C.c_void_p * len(thetas))(*[t.data_ptr() for t in thetas])
+        op = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
+        _capi.check(_capi.LIB.tnx_heff_batch_apply(self.handle, tp, op, torch.cuda.current_stream().cuda_stream))
+
+    def device_error(self) -> int:
+        e = C.c_int32()
+        _capi.check(_capi.LIB.tnx_heff_batch_error(self.handle, C.byref(e)))
+        return e.value
+
+    def __del__(self):
+        if getattr(self, "handle", None) is not None and _capi.LIB is not None:
+            _capi.LIB.tnx_heff_batch_destroy(self.handle)
+            self.handle = None

@@ -1,0 +1,145 @@
+"""Seeded synthetic two-site H_eff problems (host structure + device data).
+
+A problem is (L, theta, W_l, W_r, R) with the flow/charge conventions of
+tenax's symmetric DMRG (algorithms/dmrg.py:1165-1299):
+  L[a,b,c]: keys with q_a = q_b + q_c      (environment of the left block)
+  theta[a,p,q,d]: q_d = q_a + q_p + q_q    (flows IN, IN, IN, OUT)
+  R[d,f,g]: keys with q_d = q_f + q_g
+W_l, W_r are bulk sites of the Heisenberg cylinder MPO (width 6, J=1).
+Bond sectors: ``n_sectors`` U(1) charges of one parity, sizes proportional
+to exp(-q^2 / (2 sigma^2)) clipped to [lo, hi] and adjusted to sum to chi.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from tenax_b200.auto_mpo import heisenberg_chain_sites, heisenberg_cylinder_sites, to_symmetric
+from tenax_b200.core import FlowDirection, TensorIndex, U1Symmetry
+from tenax_b200.tensor import SymmetricTensor, _device, block_shape
+
+U1 = U1Symmetry()
+PHYS = np.array([1, -1], np.int32)
+
+
+def sector_sizes(chi: int, n_sectors: int = 30, sigma: float = 3.0, lo: int = 4, hi: int = 256,
+                 parity: int = 1) -> tuple:
+    """(charges, sizes) of one bond; deterministic integer rounding."""
+    k = np.arange(n_sectors) - n_sectors // 2
+    q = (parity % 2) + 2 * k
+    g = np.exp(-(q.astype(np.float64) ** 2) / (2 * sigma * sigma))
+    if chi < n_sectors * lo or chi > n_sectors * hi:
+        raise ValueError(f"chi={chi} cannot be split into {n_sectors} sectors of size [{lo},{hi}]")
+
+    def sizes(s):
+        return np.clip(np.rint(s * g), lo, hi).astype(np.int64)
+
+    a, b = 0.0, float(chi) * 1e6
+    for _ in range(200):
+        m = 0.5 * (a + b)
+        if sizes(m).sum() < chi:
+            a = m
+        else:
+            b = m
+    sz = sizes(b)
+    order = np.argsort(-g, kind="stable")
+    while sz.sum() > chi:
+        for i in order[::-1]:
+            if sz.sum() <= chi:
+                break
+            if sz[i] > lo:
+                sz[i] -= 1
+    while sz.sum() < chi:
+        for i in order:
+            if sz.sum() >= chi:
+                break
+            if sz[i] < hi:
+                sz[i] += 1
+    return q.astype(np.int32), sz
+
+
+def bond_charges(chi: int, parity: int = 1, **kw) -> np.ndarray:
+    q, sz = sector_sizes(chi, parity=parity, **kw)
+    return np.concatenate([np.full(int(s), int(c), np.int32) for c, s in zip(q, sz)])
+
+
+@dataclass
+class HeffProblem:
+    L: SymmetricTensor
+    theta: SymmetricTensor
+    Wl: SymmetricTensor
+    Wr: SymmetricTensor
+    R: SymmetricTensor
+    chi: int
+
+
+def _env_keys(leg0, mpo, leg2):
+    """Keys (q0, qb, q2) with q0 = qb + q2."""
+    s0 = set(np.unique(leg0).tolist())
+    keys = []
+    for qb in np.unique(mpo):
+        for q2 in np.unique(leg2):
+            if int(qb + q2) in s0:
+                keys.append((int(qb + q2), int(qb), int(q2)))
+    return sorted(keys)
+
+
+def _fill(indices, keys, gen, dtype=torch.float64):
+    sizes = [int(np.prod(block_shape(indices, k))) for k in keys]
+    n = int(sum(sizes))
+    dev = _device()
+    if isinstance(gen, np.random.Generator):
+        data = torch.from_numpy(gen.standard_normal(n)).to(dev)
+    else:
+        data = torch.randn(n, generator=gen, dtype=torch.float64, device=dev)
+    return SymmetricTensor.from_flat(indices, keys, data)
+
+
+def make_heff_problem(chi_l: int, chi_r: int, Wl: SymmetricTensor, Wr: SymmetricTensor, gen,
+                      parity: int = 1, **kw) -> HeffProblem:
+    vl = bond_charges(chi_l, parity=parity, **kw)
+    vr = bond_charges(chi_r, parity=parity, **kw)
+    mpo_l = Wl.indices[0].charges
+    mpo_r = Wr.indices[3].charges
+    Lidx = (TensorIndex(U1, vl, FlowDirection.OUT, "vl"), TensorIndex(U1, mpo_l, FlowDirection.OUT, "wl"),
+            TensorIndex(U1, vl, FlowDirection.OUT, "vl_c"))
+    Ridx = (TensorIndex(U1, vr, FlowDirection.IN, "vr"), TensorIndex(U1, mpo_r, FlowDirection.IN, "wr"),
+            TensorIndex(U1, vr, FlowDirection.IN, "vr_c"))
+    Tidx = (TensorIndex(U1, vl, FlowDirection.IN, "vl"), TensorIndex(U1, PHYS, FlowDirection.IN, "p1"),
+            TensorIndex(U1, PHYS, FlowDirection.IN, "p2"), TensorIndex(U1, vr, FlowDirection.OUT, "vr"))
+    L = _fill(Lidx, _env_keys(vl, mpo_l, vl), gen)
+    R = _fill(Ridx, _env_keys(vr, mpo_r, vr), gen)
+    sr = set(np.unique(vr).tolist())
+    tkeys = sorted((int(a), int(p), int(q), int(a + p + q)) for a in np.unique(vl) for p in PHYS for q in PHYS
+                   if int(a + p + q) in sr)
+    th = _fill(Tidx, tkeys, gen)
+    return HeffProblem(L, th, Wl, Wr, R, chi_l)
+
+
+def cylinder_bulk_w(Lx: int = 4, Ly: int = 6, site: int = 7):
+    """Device W_l, W_r: two neighbouring bulk sites of the width-Ly cylinder MPO."""
+    sites = heisenberg_cylinder_sites(Lx, Ly)
+    return to_symmetric(sites[site]), to_symmetric(sites[site + 1])
+
+
+def chain_bulk_w(L: int = 20, site: int = 9):
+    sites = heisenberg_chain_sites(L)
+    return to_symmetric(sites[site]), to_symmetric(sites[site + 1])
+
+
+def batched_problems(n: int = 64, chis=(256, 512, 1024, 2048), seed: int = 0, gen_backend: str = "torch",
+                     **kw) -> list:
+    """The batched grouped-sector workload: n independent two-site problems,
+    chi drawn uniformly from ``chis`` with a seeded generator."""
+    Wl, Wr = cylinder_bulk_w()
+    rng = np.random.default_rng(seed)
+    draw = rng.choice(np.asarray(chis), size=n)
+    if gen_backend == "torch":
+        gen = torch.Generator(device=_device())
+        gen.manual_seed(seed)
+    else:
+        gen = np.random.default_rng(seed + 1)
+    return [make_heff_problem(int(c), int(c), Wl, Wr, gen, **kw) for c in draw]

@@ -1,0 +1,334 @@
+"""Generate the golden fixtures by executing the reference's own tenax source.
+
+Run in the development container only (it needs the read-only reference
+checkout; nothing at test or bench time reads it):
+
+    python tests/golden/make_golden.py --ref /root/reference/src
+
+The reference modules are loaded by file path under the NumPy stand-in for
+jax (``_jax_standin.py``); their outputs -- plus the inputs that produced
+them -- are written as small ``.npz``/``.json`` files next to this script.
+Inputs are drawn from seeded ``numpy.random.default_rng`` generators so the
+same inputs can be rebuilt anywhere.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+import _jax_standin  # noqa: E402
+from fixture_io import pack_tensor  # noqa: E402
+
+
+def ref_tensor_to_legs(t):
+    return [(np.asarray(i.charges), int(i.flow), i.label) for i in t.indices]
+
+
+def ref_blocks(t):
+    return {tuple(int(q) for q in k): np.asarray(v, dtype=np.float64) for k, v in t.blocks.items()}
+
+
+def dump_tensor(prefix, t, modulus=None):
+    return pack_tensor(prefix, ref_tensor_to_legs(t), ref_blocks(t), modulus)
+
+
+def make_sym_tensor(M, legs, rng, modulus=None, target=None):
+    """Build a reference SymmetricTensor with N(0,1) blocks from ``rng``
+    over the reference's own valid-block set (sorted-key order)."""
+    core = M["tenax.core.tensor"]
+    idx = M["tenax.core.index"]
+    sym_mod = M["tenax.core.symmetry"]
+    sym = sym_mod.U1Symmetry() if modulus is None else sym_mod.ZnSymmetry(modulus)
+    indices = tuple(
+        idx.TensorIndex(sym, np.asarray(c, np.int32), idx.FlowDirection(f), label=lab) for c, f, lab in legs
+    )
+    keys = core._compute_valid_blocks(indices, target=target)
+    blocks = {}
+    for k in sorted(keys):
+        _, shp = core._block_slices(indices, k)
+        if all(s > 0 for s in shp):
+            blocks[k] = rng.standard_normal(shp)
+    if target not in (None, 0):
+        obj = object.__new__(core.SymmetricTensor)
+        obj._indices = indices
+        obj._blocks = blocks
+        return obj
+    return core.SymmetricTensor(blocks, indices)
+
+
+def c1_virtual_charges():
+    """Virtual charges -4..4 with multiplicities proportional to C(8,k),
+    total 64: floor with a minimum of 1, then the largest sector absorbs
+    the difference.  Result: [1, 2, 7, 14, 16, 14, 7, 2, 1]."""
+    from math import comb
+
+    x = np.array([comb(8, k) / 256 * 64 for k in range(9)])
+    m = np.maximum(1, np.floor(x)).astype(int)
+    diff = 64 - int(m.sum())
+    if diff < 0:
+        m[int(np.argmax(m))] += diff
+    elif diff > 0:
+        rem = x - np.floor(x)
+        for i in np.argsort(-rem, kind="stable")[:diff]:
+            m[i] += 1
+    charges = np.concatenate([np.full(mk, q, np.int32) for q, mk in zip(range(-4, 5), m)])
+    return charges, m
+
+
+def gen_valid_blocks(M):
+    core = M["tenax.core.tensor"]
+    idx = M["tenax.core.index"]
+    sm = M["tenax.core.symmetry"]
+    cases = [
+        ("u1_3leg", None, [[-1, 0, 1, 0], [1, -1], [0, 1, 1, -1, 2]], [1, 1, -1], None),
+        ("u1_4leg_target", None, [[-2, 0, 2], [1, -1], [1, -1], [-3, -1, 1, 3]], [1, 1, 1, -1], 2),
+        ("u1_env_out", None, [[-3, -1, 1, 3], [0, 2, -2, 0], [-3, -1, 1, 3]], [-1, -1, -1], None),
+        ("z3_3leg", 3, [[0, 1, 2, 1], [0, 2], [0, 1, 2]], [1, 1, -1], None),
+        ("z3_4leg", 3, [[0, 1, 2], [1, 2], [0, 0, 1], [2, 1, 0]], [1, -1, 1, -1], 1),
+        ("z2_2leg", 2, [[0, 1, 1], [1, 0]], [1, -1], None),
+        ("u1_1leg", None, [[0, 1, -1]], [1], None),
+        ("u1_5leg", None, [[-1, 1], [0, 2, -2], [1, -1], [1, -1], [-2, 0, 2, 4]], [1, 1, -1, 1, -1], None),
+    ]
+    out = []
+    for name, mod, charges, flows, target in cases:
+        sym = sm.U1Symmetry() if mod is None else sm.ZnSymmetry(mod)
+        inds = tuple(
+            idx.TensorIndex(sym, np.array(c, np.int32), idx.FlowDirection(f), label=f"l{i}")
+            for i, (c, f) in enumerate(zip(charges, flows))
+        )
+        keys = core._compute_valid_blocks(inds, target=target)
+        out.append(
+            {"name": name, "modulus": mod, "charges": charges, "flows": flows, "target": target,
+             "keys": [list(map(int, k)) for k in keys]}
+        )
+    with open(os.path.join(HERE, "valid_blocks.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
+def gen_contract(M):
+    contractor = M["tenax.contraction.contractor"]
+    rng = np.random.default_rng(7)
+    arrays = {}
+    cases = []
+
+    def add(name, tensors, output_labels=None, modulus=None):
+        res = contractor.contract(*tensors, output_labels=output_labels)
+        subs, _ = contractor._labels_to_subscripts(tensors, output_labels)
+        d = {}
+        for i, t in enumerate(tensors):
+            d.update(dump_tensor(f"{name}.in{i}", t, modulus))
+        d.update(dump_tensor(f"{name}.out", res, modulus))
+        arrays.update(d)
+        cases.append({"name": name, "n_in": len(tensors), "subscripts": subs,
+                      "output_labels": output_labels, "modulus": modulus, "n_out_blocks": len(res.blocks)})
+
+    phys = [-1, 1]
+    bond = [-1, 0, 1]
+    A = make_sym_tensor(M, [(phys, 1, "p0"), (bond, 1, "bond_left"), (bond, -1, "bond")], rng)
+    B = make_sym_tensor(M, [(phys, 1, "p1"), (bond, 1, "bond"), (bond, -1, "bond_right")], rng)
+    add("pair_u1", [A, B])
+    add("pair_u1_perm", [A, B], output_labels=["bond_right", "p0", "p1", "bond_left"])
+    # MPS-like pair with degenerate sectors
+    v = [-2, -2, 0, 0, 0, 2, 1, -1, 1]
+    A2 = make_sym_tensor(M, [(v, 1, "vl"), ([1, -1], 1, "p"), (v, -1, "m")], rng)
+    B2 = make_sym_tensor(M, [(v, 1, "m"), ([1, -1], 1, "q"), (v, -1, "vr")], rng)
+    add("mps_pair", [A2, B2])
+    # two contracted legs
+    C = make_sym_tensor(M, [([0, 1, -1, 1], 1, "x"), ([1, -1], 1, "y"), ([0, 2, 1, -1, 0], -1, "z")], rng)
+    D = make_sym_tensor(M, [([0, 2, 1, -1, 0], 1, "z"), ([1, -1], -1, "y"), ([0, 0, 1], -1, "w")], rng)
+    add("two_legs", [C, D])
+    # Z3
+    E = make_sym_tensor(M, [([0, 1, 2, 1], 1, "a"), ([0, 2, 1], -1, "b")], rng, modulus=3)
+    F = make_sym_tensor(M, [([0, 2, 1], 1, "b"), ([1, 1, 0, 2], -1, "c"), ([0, 1], 1, "d")], rng, modulus=3)
+    add("z3_pair", [E, F], modulus=3)
+    # non-zero target on one operand (boundary-site style)
+    G = make_sym_tensor(M, [([1, -1, 3], 1, "u"), ([1, -1], 1, "s")], rng, target=2)
+    H = make_sym_tensor(M, [([1, -1], -1, "s"), ([1, -1, 3], -1, "t")], rng)
+    add("target_pair", [G, H])
+    # three operands with differing contracted sets (reference returns no blocks)
+    P = make_sym_tensor(M, [(bond, 1, "i"), (bond, -1, "j")], rng)
+    Q = make_sym_tensor(M, [(bond, 1, "j"), (bond, -1, "k")], rng)
+    R = make_sym_tensor(M, [(bond, 1, "k"), (bond, -1, "l")], rng)
+    add("three_chain", [P, Q, R])
+    # three operands all contracting the same set
+    S1 = make_sym_tensor(M, [(bond, 1, "i"), (bond, -1, "j"), (phys, 1, "p")], rng)
+    S2 = make_sym_tensor(M, [(bond, 1, "j"), (phys, -1, "q"), (bond, -1, "k")], rng)
+    add("outer_free", [S1, S2])
+
+    np.savez_compressed(os.path.join(HERE, "contract.npz"), **arrays)
+    with open(os.path.join(HERE, "contract.json"), "w") as f:
+        json.dump(cases, f, indent=1)
+
+
+def chain_mps_site_legs(i, L, v):
+    if i == 0:
+        return [([1, -1], 1, f"p{i}"), (v, -1, f"v{i}_{i+1}")]
+    if i == L - 1:
+        return [(v, 1, f"v{i-1}_{i}"), ([1, -1], 1, f"p{i}")]
+    return [(v, 1, f"v{i-1}_{i}"), ([1, -1], 1, f"p{i}"), (v, -1, f"v{i}_{i+1}")]
+
+
+def build_c1_mps(M, L, seed):
+    v, _ = c1_virtual_charges()
+    rng = np.random.default_rng(seed)
+    core = M["tenax.core.tensor"]
+    sites = []
+    for i in range(L):
+        t = make_sym_tensor(M, chain_mps_site_legs(i, L, v), rng, target=0 if i == L - 1 else None)
+        nrm = np.sqrt(sum(np.sum(b ** 2) for b in t.blocks.values()))
+        t._blocks = {k: b / nrm for k, b in t.blocks.items()}
+        sites.append(t)
+    return sites
+
+
+def gen_dmrg_pieces(M):
+    """Small H_eff matvec, env updates, Lanczos and SVD with the reference."""
+    dm = M["tenax.algorithms.dmrg"]
+    arrays = {}
+    L = 6
+    mpo = dm.build_mpo_heisenberg(L)
+    Ws = [mpo.get_tensor(i) for i in range(L)]
+    v = [-2, -1, -1, 0, 0, 0, 1, 1, 2, -1, 0, 1, 3, -3]
+    rng = np.random.default_rng(11)
+    sites = [make_sym_tensor(M, chain_mps_site_legs(i, L, v), rng, target=0 if i == L - 1 else None)
+             for i in range(L)]
+    # left env at site 2 and right env at site 4 built by the reference
+    envL = dm._build_trivial_left_env_symmetric()
+    for i in range(2):
+        envL = dm._update_left_env_symmetric(envL, sites[i], Ws[i])
+    envR = dm._build_trivial_right_env_symmetric()
+    for i in range(L - 1, 3, -1):
+        envR = dm._update_right_env_symmetric(envR, sites[i], Ws[i])
+    contractor = M["tenax.contraction.contractor"]
+    theta = contractor.contract(sites[2], sites[3])
+    cache = {}
+    hv = dm._blockwise_contract([envL, theta, Ws[2], Ws[3], envR], "abc,apqd,bpse,eqtf,dfg->cstg",
+                                output_indices=theta.indices, expr_cache=cache)
+    arrays.update(dump_tensor("heff.L", envL))
+    arrays.update(dump_tensor("heff.theta", theta))
+    arrays.update(dump_tensor("heff.Wl", Ws[2]))
+    arrays.update(dump_tensor("heff.Wr", Ws[3]))
+    arrays.update(dump_tensor("heff.R", envR))
+    arrays.update(dump_tensor("heff.out", hv))
+    # env update step outputs
+    newL = dm._update_left_env_symmetric(envL, sites[2], Ws[2])
+    newR = dm._update_right_env_symmetric(envR, sites[3], Ws[3])
+    arrays.update(dump_tensor("envl.A", sites[2]))
+    arrays.update(dump_tensor("envl.out", newL))
+    arrays.update(dump_tensor("envr.B", sites[3]))
+    arrays.update(dump_tensor("envr.out", newR))
+    # Lanczos on this H_eff
+    matvec = lambda x: dm._blockwise_contract([envL, x, Ws[2], Ws[3], envR], "abc,apqd,bpse,eqtf,dfg->cstg",
+                                             output_indices=x.indices, expr_cache=cache)
+    e, vec = dm._lanczos_solve_tensor(matvec, theta, 8, 1e-12)
+    arrays["lanczos.energy"] = np.array(e)
+    arrays.update(dump_tensor("lanczos.vec", vec))
+    # truncated SVD of the Lanczos vector (two-site update style)
+    U, s, Vh, err = dm._svd_and_truncate_site(vec, 2, M["cfg"](max_bond_dim=5))
+    arrays.update(dump_tensor("svd.U", U))
+    arrays.update(dump_tensor("svd.Vh", Vh))
+    arrays["svd.s"] = np.asarray(s)
+    arrays["svd.err"] = np.array(err)
+    np.savez_compressed(os.path.join(HERE, "dmrg_pieces.npz"), **arrays)
+
+
+def gen_dmrg_c1(M, L=20, sweeps=2, lanczos=10, seed=1234):
+    dm = M["tenax.algorithms.dmrg"]
+    net = M["tenax.network.network"]
+    mpo = dm.build_mpo_heisenberg(L)
+    sites = build_c1_mps(M, L, seed)
+    mps = net.TensorNetwork(name="c1")
+    for i, t in enumerate(sites):
+        mps.add_node(i, t)
+    for i in range(L - 1):
+        mps.connect(i, f"v{i}_{i+1}", i + 1, f"v{i}_{i+1}")
+    arrays = {}
+    for i, t in enumerate(sites):
+        arrays.update(dump_tensor(f"mps{i}", t))
+    for i in range(L):
+        arrays.update(dump_tensor(f"mpo{i}", mpo.get_tensor(i)))
+    t0 = time.time()
+    cfg = dm.DMRGConfig(max_bond_dim=64, num_sweeps=sweeps, lanczos_max_iter=lanczos, two_site=True)
+    res = dm.dmrg(mpo, mps, cfg)
+    wall = time.time() - t0
+    arrays["energy"] = np.array(res.energy)
+    arrays["energies_per_sweep"] = np.array(res.energies_per_sweep)
+    arrays["truncation_errors"] = np.array(res.truncation_errors)
+    for i in range(L):
+        t = res.mps.get_tensor(i)
+        arrays.update(dump_tensor(f"final{i}", t))
+    np.savez_compressed(os.path.join(HERE, f"dmrg_c1_L{L}.npz"), **arrays)
+    v, m = c1_virtual_charges()
+    with open(os.path.join(HERE, f"dmrg_c1_L{L}.json"), "w") as f:
+        json.dump({"L": L, "sweeps": sweeps, "lanczos": lanczos, "seed": seed, "multiplicities": m.tolist(),
+                   "energy": float(res.energy), "energies_per_sweep": [float(x) for x in res.energies_per_sweep],
+                   "reference_wall_s_standin": wall}, f, indent=1)
+    print(f"C1 L={L}: E={res.energy:.15f} in {wall:.1f}s")
+
+
+def gen_mpo(M):
+    am = M["tenax.algorithms.auto_mpo"]
+    arrays = {}
+    Lx, Ly = 3, 6
+    terms = []
+    for (i, j) in cylinder_bonds(Lx, Ly):
+        terms += [(1.0, "Sz", i, "Sz", j), (0.5, "Sp", i, "Sm", j), (0.5, "Sm", i, "Sp", j)]
+    mpo = am.build_auto_mpo(terms, L=Lx * Ly, symmetric=True, compress=False)
+    for i in range(Lx * Ly):
+        arrays.update(dump_tensor(f"cyl{i}", mpo.get_tensor(i)))
+    dm = M["tenax.algorithms.dmrg"]
+    chain = dm.build_mpo_heisenberg(7)
+    for i in range(7):
+        arrays.update(dump_tensor(f"chain{i}", chain.get_tensor(i)))
+    np.savez_compressed(os.path.join(HERE, "mpo.npz"), **arrays)
+
+
+def cylinder_bonds(Lx, Ly):
+    """Nearest-neighbour bonds of an Lx x Ly cylinder, each bond once,
+    column-major site order i = x*Ly + y (examples/heisenberg_cylinder.py:43-66)."""
+    bonds = []
+    for x in range(Lx):
+        for y in range(Ly):
+            i, j = x * Ly + y, x * Ly + (y + 1) % Ly
+            bonds.append((min(i, j), max(i, j)))
+            if x < Lx - 1:
+                bonds.append((x * Ly + y, (x + 1) * Ly + y))
+    return bonds
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference/src")
+    ap.add_argument("--only", default="")
+    args = ap.parse_args()
+    mods = _jax_standin.load_reference(args.ref, [
+        "tenax.core.symmetry", "tenax.core.index", "tenax.core.tensor", "tenax.linalg",
+        "tenax.contraction.contractor", "tenax.network.network", "tenax.algorithms._tensor_utils",
+        "tenax.algorithms.auto_mpo", "tenax.algorithms.dmrg",
+    ])
+    mods["cfg"] = mods["tenax.algorithms.dmrg"].DMRGConfig
+    todo = args.only.split(",") if args.only else ["valid", "contract", "pieces", "mpo", "c1"]
+    if "valid" in todo:
+        gen_valid_blocks(mods)
+    if "contract" in todo:
+        gen_contract(mods)
+    if "pieces" in todo:
+        gen_dmrg_pieces(mods)
+    if "mpo" in todo:
+        gen_mpo(mods)
+    if "c1" in todo:
+        gen_dmrg_c1(mods)
+
+
+if __name__ == "__main__":
+    main()
