@@ -662,7 +662,8 @@ struct tnx_heff_batch {
   int n_t1 = 0, n_t4 = 0;
   DevMem mpo_pairs, mpo_ins, mpo_oslots, mpo_terms, mpo_chunks;
   int n_mpo_chunks = 0, max_in_slots = 0;
-  DevMem zero_segs;  // not used when every output block is written
+  DevMem zero_chunks;  // theta-layout blocks H_eff never writes (slot = problem + 1)
+  int n_zero_chunks = 0;
   DevMem err, src_tab, out_tab1, out_tab4;
   const int32_t* skip = nullptr;
   int n_launches = 0;
@@ -716,6 +717,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     std::vector<DevMpoOutSlot> MO;
     std::vector<DevMpoTerm> MT;
     std::vector<int2> MC;
+    std::vector<DevChunk> ZC;
     for (int i = 0; i < n; ++i) {
       tnx_heff* h = hs[i];
       const HeffPlan& H = h->H;
@@ -766,6 +768,9 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
       tl.clear();
       build_tiles(H.s4, h->g4, g4base, tl);
       T4.insert(T4.end(), tl.begin(), tl.end());
+      for (auto& zr : H.zero_ranges)
+        for (int64_t st = 0; st < zr.second; st += 4096)
+          ZC.push_back({1 + i, 0, zr.first + st, std::min<int64_t>(4096, zr.second - st)});
       // MPO tables
       for (size_t pi = 0; pi < H.pairs.size(); ++pi) {
         const MpoPair& mp = H.pairs[pi];
@@ -836,6 +841,8 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     upload(b->mpo_oslots, MO);
     upload(b->mpo_terms, MT);
     upload(b->mpo_chunks, MC);
+    upload(b->zero_chunks, ZC);
+    b->n_zero_chunks = static_cast<int>(ZC.size());
     b->n_mpo_chunks = static_cast<int>(MC.size());
     b->err.alloc(sizeof(int32_t));
     CUDA_OK(cudaMemset(b->err.p, 0, sizeof(int32_t)));
@@ -847,7 +854,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     t1tab.p[0] = x1_base;
     CUDA_OK(cudaMemcpy(b->out_tab1.p, &t1tab, sizeof(PtrTab), cudaMemcpyHostToDevice));
     CUDA_OK(cudaDeviceSynchronize());
-    b->n_launches = 4;
+    b->n_launches = 4 + (b->n_zero_chunks > 0 ? 1 : 0);
     *out = b.release();
     return TNX_OK;
   })
@@ -885,6 +892,7 @@ static void heff_batch_stage(tnx_heff_batch* b, int stage, cudaStream_t st) {
                        b->n_mpo_chunks, b->max_in_slots, b->skip, st);
       break;
     default:
+      launch_zero_ranges(b->out_tab4.as<uint64_t>(), b->zero_chunks.as<DevChunk>(), b->n_zero_chunks, b->skip, st);
       if (b->mode == IMG_F64)
         launch_gemm_f64(b->g4.as<DevGroup>(), b->t4.as<DevTile>(), b->n_t4, b->ro4.as<int64_t>(),
                         b->out_tab4.as<uint64_t>(), b->skip, st);

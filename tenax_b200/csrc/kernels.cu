@@ -86,6 +86,23 @@ void launch_scatter(const void* res, bool res_f32, double* out, const DevScatSeg
 }
 
 // ---------------------------------------------------------------------------
+// zero fill of output ranges addressed through a pointer table
+// ---------------------------------------------------------------------------
+__global__ void zero_ranges_kernel(const uint64_t* __restrict__ out_tab, const DevChunk* __restrict__ chunks,
+                                   const int32_t* __restrict__ skip) {
+  if (skip && *skip) return;
+  const DevChunk ch = chunks[blockIdx.x];  // seg = pointer slot, start = element offset
+  double* out = reinterpret_cast<double*>(out_tab[ch.seg]) + ch.start;
+  for (int64_t e = threadIdx.x; e < ch.count; e += blockDim.x) out[e] = 0.0;
+}
+
+void launch_zero_ranges(const uint64_t* out_tab, const DevChunk* chunks, int n_chunks, const int32_t* skip,
+                        cudaStream_t st) {
+  if (n_chunks <= 0) return;
+  zero_ranges_kernel<<<n_chunks, 256, 0, st>>>(out_tab, chunks, skip);
+}
+
+// ---------------------------------------------------------------------------
 // fused MPO application (stages 2+3 of the two-site H_eff):
 //   X3[c,s,t,f,d] = sum_{b,p,q} Wlr[b,p,q,s,t,f] X1[b,c,p,q,d]
 // One CTA = 128 points (c,d) of one (qc,qd) pair; the point's input vector

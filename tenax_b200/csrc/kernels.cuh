@@ -10,6 +10,9 @@ namespace tnx {
 
 void launch_pack(const uint64_t* src_tab, const DevPackSeg* segs, const DevChunk* chunks, int n_chunks, int mode,
                  const int32_t* skip, cudaStream_t st);
+// chunks: seg = pointer-table slot, [start, start+count) elements set to 0
+void launch_zero_ranges(const uint64_t* out_tab, const DevChunk* chunks, int n_chunks, const int32_t* skip,
+                        cudaStream_t st);
 void launch_scatter(const void* res, bool res_f32, double* out, const DevScatSeg* segs, const DevChunk* chunks,
                     int n_chunks, cudaStream_t st);
 void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevMpoIn* ins, const DevMpoOutSlot* oslots,

@@ -585,6 +585,16 @@ HeffPlan plan_heff(const TensorStruct& L, const TensorStruct& th, const TensorSt
   H.closed = true;
   for (auto& k : H.out_keys)
     if (!th_idx.count(k)) H.closed = false;
+  {
+    std::unordered_map<Key, int, KeyHash> written;
+    for (auto& k : H.out_keys) written[k] = 1;
+    for (size_t i = 0; i < th.keys.size(); ++i) {
+      if (written.count(th.keys[i])) continue;
+      int64_t n = 1;
+      for (auto x : th.dims[i]) n *= x;
+      if (n > 0) H.zero_ranges.push_back({th.offs[i], n});
+    }
+  }
   // stage-4 epilogue row offsets into theta's layout: each group must hold a
   // single col block (one qg) for the direct store
   H.s4_separable = true;

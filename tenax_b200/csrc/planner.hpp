@@ -161,6 +161,8 @@ struct HeffPlan {
   std::vector<std::vector<int64_t>> s4_rowoff;
   // charge tuples of each MPO pair's inputs (qb,qp,qq) and outputs (qs,qt,qf)
   std::vector<std::vector<Key>> mpo_in_keys, mpo_out_keys;
+  // theta-layout (offset, length) of blocks H_eff never writes: zeroed per apply
+  std::vector<std::pair<int64_t, int64_t>> zero_ranges;
 };
 
 HeffPlan plan_heff(const TensorStruct& L, const TensorStruct& th, const TensorStruct& Wl, const TensorStruct& Wr,
