@@ -119,7 +119,7 @@ def run_ours(args):
     from tenax_b200.tensor import embed_in_keys
     from tenax_b200.workloads import batched_problems
 
-    problems = batched_problems(N_PROBLEMS, CHIS, seed=args.seed + 1000 * rank)
+    problems = batched_problems(args.problems, CHIS, seed=args.seed + 1000 * rank)
     chi_counts = {int(c): sum(1 for p in problems if p.chi == c) for c in CHIS}
     dev = torch.device("cuda", local)
 
@@ -230,7 +230,7 @@ def run_ours(args):
             "metric": METRIC, "value": round(value, 3), "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(rmx["ms"], 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": args.precision, "data": "synthetic (seeded N(0,1) blocks; no dataset)",
-            "config": {"workload": WORKLOAD, "problems_per_gpu": N_PROBLEMS, "chi_counts": chi_counts,
+            "config": {"workload": WORKLOAD, "problems_per_gpu": args.problems, "chi_counts": chi_counts,
                        "flops_per_step_per_gpu": rmx["flops"], "flop_count": "block-sparse 4-stage sector GEMM "
                        "flops from stored block dims", "l2": "inputs larger than L2 (operators+theta >> 126 MB); "
                        "no flush", "parallelism": f"replicas x{world} (independent problems per GPU)"},
@@ -378,6 +378,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-problems", type=int, default=2)
+    ap.add_argument("--problems", type=int, default=N_PROBLEMS,
+                    help="problems per GPU (64 = the benchmark workload; smaller only for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

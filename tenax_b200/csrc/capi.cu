@@ -151,10 +151,12 @@ void build_pack(const std::vector<PackSeg>& segs, const PairGeom& G, bool a_side
     d.nKt = G.nKt[s.group];
     d.nlegs = s.nlegs;
     d.src_slot = src_slot;
+    d.kcount = 1;
     for (int l = 0; l < s.nlegs; ++l) {
       d.dims[l] = s.dims[l];
       d.rstr[l] = s.rstr[l];
       d.kstr[l] = s.kstr[l];
+      if (s.kstr[l]) d.kcount *= s.dims[l];
     }
     int seg_id = static_cast<int>(out.size());
     out.push_back(d);
@@ -660,8 +662,9 @@ struct tnx_heff_batch {
   int n_th_chunks = 0;
   DevMem g1, t1, ro1, g4, t4, ro4;
   int n_t1 = 0, n_t4 = 0;
-  DevMem mpo_pairs, mpo_ins, mpo_oslots, mpo_terms, mpo_chunks;
-  int n_mpo_chunks = 0, max_in_slots = 0;
+  DevMem mpo_pairs, mpo_slots, mpo_oslots, mpo_terms, mpo_chunks;
+  int n_mpo_chunks = 0;
+  size_t mpo_smem = 16;
   DevMem zero_chunks;  // theta-layout blocks H_eff never writes (slot = problem + 1)
   int n_zero_chunks = 0;
   DevMem err, src_tab, out_tab1, out_tab4;
@@ -713,7 +716,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     std::vector<int64_t> R1, R4;
     std::vector<std::pair<int64_t, DevTile>> T1, T4;
     std::vector<DevMpoPair> MP;
-    std::vector<DevMpoIn> MI;
+    std::vector<DevMpoSlot> MI;
     std::vector<DevMpoOutSlot> MO;
     std::vector<DevMpoTerm> MT;
     std::vector<int2> MC;
@@ -785,18 +788,24 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         dp.n_terms = static_cast<int32_t>(mp.terms.size());
         dp.n_in_slots = mp.n_in_slots;
         dp.n_out_slots = mp.n_out_slots;
-        b->max_in_slots = std::max(b->max_in_slots, mp.n_in_slots);
+        b->mpo_smem = std::max<size_t>(b->mpo_smem, mp.terms.size() * sizeof(DevMpoTerm) +
+                                                       mp.n_in_slots * sizeof(DevMpoSlot) +
+                                                       mp.n_out_slots * sizeof(DevMpoOutSlot));
         for (size_t k = 0; k < mp.ins.size(); ++k) {
+          // one record per input slot (b,p,q): address of its point (c=0, d=0)
           const MpoIn& in = mp.ins[k];
-          DevMpoIn di{};
           const int64_t ld = H.s1.groups[in.g1].N;
-          di.x1_addr = x1_base + static_cast<uint64_t>(x1_goff[in.g1] + static_cast<int64_t>(in.row0) * ld + in.col0) * esz;
-          di.ld = ld;
-          di.mb = in.mb;
-          di.mp = in.mp;
-          di.mq = in.mq;
-          di.slot0 = mp.in_slot0[k];
-          MI.push_back(di);
+          const int64_t blk = x1_goff[in.g1] + static_cast<int64_t>(in.row0) * ld + in.col0;
+          for (int bb = 0; bb < in.mb; ++bb)
+            for (int pp = 0; pp < in.mp; ++pp)
+              for (int qq = 0; qq < in.mq; ++qq) {
+                DevMpoSlot sl{};
+                sl.base = x1_base + static_cast<uint64_t>(blk + static_cast<int64_t>(bb) * mp.mc * ld +
+                                                          static_cast<int64_t>(pp * in.mq + qq) * mp.md) *
+                                        esz;
+                sl.ld = ld;
+                MI.push_back(sl);
+              }
         }
         for (size_t k = 0; k < mp.outs.size(); ++k) {
           const MpoOut& o = mp.outs[k];
@@ -818,11 +827,12 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         for (auto& t : mp.terms) MT.push_back({t.out_slot, t.in_slot, t.w});
         const int pair_id = static_cast<int>(MP.size());
         MP.push_back(dp);
-        for (int p0 = 0; p0 < mp.mc * mp.md; p0 += 128) MC.push_back(make_int2(pair_id, p0));
+        const int ppc = mpo_points_per_cta();
+        for (int p0 = 0; p0 < mp.mc * mp.md; p0 += ppc) MC.push_back(make_int2(pair_id, p0));
       }
     }
-    if (b->max_in_slots * 128 * esz > 200 * 1024)
-      return set_err(TNX_ERR_UNSUPPORTED, "MPO input vector too long for the fused MPO kernel");
+    if (b->mpo_smem > 200 * 1024)
+      return set_err(TNX_ERR_UNSUPPORTED, "MPO term tables too large for the fused MPO kernel");
     upload(b->th_pack, tp);
     upload(b->th_chunks, tc);
     b->n_th_chunks = static_cast<int>(tc.size());
@@ -837,7 +847,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     upload(b->t4, t4);
     b->n_t4 = static_cast<int>(t4.size());
     upload(b->mpo_pairs, MP);
-    upload(b->mpo_ins, MI);
+    upload(b->mpo_slots, MI);
     upload(b->mpo_oslots, MO);
     upload(b->mpo_terms, MT);
     upload(b->mpo_chunks, MC);
@@ -887,9 +897,9 @@ static void heff_batch_stage(tnx_heff_batch* b, int stage, cudaStream_t st) {
                        b->out_tab1.as<uint64_t>(), false, b->err.as<int32_t>(), b->skip, st);
       break;
     case 2:
-      launch_mpo_apply(f32, b->mode, b->mpo_pairs.as<DevMpoPair>(), b->mpo_ins.as<DevMpoIn>(),
+      launch_mpo_apply(f32, b->mode, b->mpo_pairs.as<DevMpoPair>(), b->mpo_slots.as<DevMpoSlot>(),
                        b->mpo_oslots.as<DevMpoOutSlot>(), b->mpo_terms.as<DevMpoTerm>(), b->mpo_chunks.as<int2>(),
-                       b->n_mpo_chunks, b->max_in_slots, b->skip, st);
+                       b->n_mpo_chunks, b->mpo_smem, b->skip, st);
       break;
     default:
       launch_zero_ranges(b->out_tab4.as<uint64_t>(), b->zero_chunks.as<DevChunk>(), b->n_zero_chunks, b->skip, st);

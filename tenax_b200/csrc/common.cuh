@@ -61,7 +61,7 @@ struct DevPackSeg {
   uint64_t img_addr;  // absolute address of the destination group image (tile 0)
   int64_t lo_off;     // byte offset of the low-part image (BF16 split) from img_addr
   int32_t row0, k0, nKt, nlegs;
-  int32_t src_slot, pad;
+  int32_t src_slot, kcount;  // kcount: k extent of the block (product of contracted dims)
   int32_t dims[kMaxLegsDev];
   int32_t rstr[kMaxLegsDev];
   int32_t kstr[kMaxLegsDev];
@@ -102,10 +102,9 @@ struct DevMpoPair {
   int32_t term0, n_terms;
   int32_t n_in_slots, n_out_slots;
 };
-struct DevMpoIn {
-  uint64_t x1_addr;  // absolute address of element (b=0,c=0,p=0,q=0,d=0) of the stage-1 result
-  int64_t ld;
-  int32_t mb, mp, mq, slot0;
+struct DevMpoSlot {  // one input slot (b,p,q) of one X1 block
+  uint64_t base;      // absolute address of the slot's point (c=0, d=0) in the stage-1 result
+  int64_t ld;         // element stride between consecutive c (the result matrix's row length)
 };
 struct DevMpoOutSlot {  // one output slot (s,t,f) of one X3 block
   uint64_t img_addr;    // stage-4 A image of the group (tile 0)

@@ -85,14 +85,21 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+// 32 lanes x 32 consecutive fp32 columns: lane i receives row (quarter*32 + i)
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
       : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+        "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+
+constexpr int kStagePitch = 33;  // fp32 words per staged row (+1 breaks bank conflicts)
+constexpr int kEpiStageBytes = 4 * 32 * kStagePitch * 4;
 
 template <bool TF32, typename OutT>
 __global__ void __launch_bounds__(THREADS, 1)
@@ -114,6 +121,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint64_t* drain = tempty + 2;
   uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
+  // epilogue staging: one 32 x 33 fp32 buffer per epilogue warp, after 256 B of barriers
+  float* epi_stage = reinterpret_cast<float*>(smem + STAGES * NT * TILE_BYTES + 256);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -255,6 +264,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     // ------------------------------------------------------------ epilogue
     const int q = warp & 3;  // TMEM lane quarter this warp may access
     const int r_in_tile = q * 32 + lane;
+    float* stg = epi_stage + (warp - 2) * 32 * kStagePitch;
     int acc = 0;
     uint32_t aph = 0;
     for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
@@ -267,16 +277,23 @@ __global__ void __launch_bounds__(THREADS, 1)
       const int64_t ro = row < g.M ? rowoff[g.rowoff0 + row] : -1;
       OutT* out = reinterpret_cast<OutT*>(out_tab[g.out_slot]);
       const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * TBN);
+      // Each lane holds one row; stage 32x32 chunks through shared memory so
+      // that every store instruction writes 32 consecutive columns of one row.
 #pragma unroll 1
-      for (int c0 = 0; c0 < TBN; c0 += 16) {
-        uint32_t v[16];
-        tmem_ld16(tbase + c0, v);
-        if (ro >= 0) {
-          const int col0 = tl.nt * TBN + c0;
+      for (int c0 = 0; c0 < TBN; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld32(tbase + c0, v);
 #pragma unroll
-          for (int j = 0; j < 16; ++j)
-            if (col0 + j < g.N) out[ro + col0 + j] = static_cast<OutT>(__uint_as_float(v[j]));
+        for (int j = 0; j < 32; ++j) stg[lane * kStagePitch + j] = __uint_as_float(v[j]);
+        __syncwarp();
+        const int col = tl.nt * TBN + c0 + lane;
+        const bool col_ok = col < g.N;
+#pragma unroll 4
+        for (int r = 0; r < 32; ++r) {
+          const int64_t ro_r = __shfl_sync(0xffffffffu, ro, r);
+          if (ro_r >= 0 && col_ok) out[ro_r + col] = static_cast<OutT>(stg[r * kStagePitch + lane]);
         }
+        __syncwarp();
       }
       tc_fence_before();
       mbar_arrive(&tempty[acc]);
@@ -300,7 +317,7 @@ void launch_tc_impl(const DevGroup* groups, const DevTile* tiles, int n_tiles, c
                     const uint64_t* out_tab, int32_t* err_flag, const int32_t* skip, cudaStream_t st) {
   constexpr int NT = TF32 ? 2 : 4;
   constexpr int STAGES = TF32 ? 6 : 3;
-  const int smem = STAGES * NT * TILE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+  const int smem = STAGES * NT * TILE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + kEpiStageBytes;
   cudaFuncSetAttribute(gemm_tc_kernel<TF32, OutT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   int grid = device_sm_count();
   if (grid > n_tiles) grid = n_tiles;

@@ -36,16 +36,18 @@ __global__ void pack_image_kernel(const uint64_t* __restrict__ src_tab, const De
   const DevPackSeg& s = segs[ch.seg];
   const double* src = reinterpret_cast<const double*>(src_tab[s.src_slot]) + s.src_off;
   uint8_t* img = reinterpret_cast<uint8_t*>(s.img_addr);
+  // walk the block in destination order (k fastest) so consecutive threads
+  // write consecutive k of one image row; the strided source reads hit cache
   for (int64_t e = ch.start + threadIdx.x; e < ch.start + ch.count; e += blockDim.x) {
-    int64_t rem = e, row = s.row0, k = s.k0;
+    const int64_t kl = e % s.kcount, rl = e / s.kcount;
+    int64_t src_off = 0, stride = 1;
     for (int l = s.nlegs - 1; l >= 0; --l) {
-      int64_t d = s.dims[l];
-      int64_t idx = rem % d;
-      rem /= d;
-      row += idx * s.rstr[l];
-      k += idx * s.kstr[l];
+      const int64_t d = s.dims[l];
+      const int64_t idx = s.rstr[l] ? (rl / s.rstr[l]) % d : (s.kstr[l] ? (kl / s.kstr[l]) % d : 0);
+      src_off += idx * stride;
+      stride *= d;
     }
-    img_store(mode, img, s.lo_off, 0, s.nKt, row, k, src[e]);
+    img_store(mode, img, s.lo_off, 0, s.nKt, s.row0 + rl, s.k0 + kl, src[src_off]);
   }
 }
 
@@ -104,79 +106,86 @@ void launch_zero_ranges(const uint64_t* out_tab, const DevChunk* chunks, int n_c
 
 // ---------------------------------------------------------------------------
 // fused MPO application (stages 2+3 of the two-site H_eff):
-//   X3[c,s,t,f,d] = sum_{b,p,q} Wlr[b,p,q,s,t,f] X1[b,c,p,q,d]
-// One CTA = 128 points (c,d) of one (qc,qd) pair; the point's input vector
-// is staged column-wise in shared memory, the sparse Wlr terms (uniform over
-// the CTA) accumulate per output slot, results go straight into the stage-4
-// A-operand image.
+//   X3[c,s,t,f,d] = sum_{b,p,q} Wlr[b,p,q,s,t,f] X1[b,c,p,q,d],  Wlr = W_l W_r over e
+// One thread = one point (c,d) of one (qc,qd) pair.  Wlr is very sparse (an
+// MPO is mostly pass-through states), so each output slot is a short sum of
+// scaled input slots: the kernel walks the pair's terms (sorted by output
+// slot, staged in shared memory with the input-slot and output-slot tables),
+// keeps kMpoLoads independent loads in flight per thread, and writes every
+// finished output straight into the stage-4 A-operand image.
 // ---------------------------------------------------------------------------
-constexpr int kMpoPoints = 128;
+constexpr int kMpoThreads = 256;
+constexpr int kMpoLoads = 8;
 
 template <typename TI>
-__global__ void __launch_bounds__(kMpoPoints) mpo_apply_kernel(
-    int mode, const DevMpoPair* __restrict__ pairs, const DevMpoIn* __restrict__ ins,
+__global__ void __launch_bounds__(kMpoThreads) mpo_apply_kernel(
+    int mode, const DevMpoPair* __restrict__ pairs, const DevMpoSlot* __restrict__ islots,
     const DevMpoOutSlot* __restrict__ oslots, const DevMpoTerm* __restrict__ terms,
     const int2* __restrict__ chunks, const int32_t* __restrict__ skip) {
   if (skip && *skip) return;
   extern __shared__ __align__(16) unsigned char mpo_smem[];
-  TI* xs = reinterpret_cast<TI*>(mpo_smem);
   const int2 ch = chunks[blockIdx.x];
   const DevMpoPair pr = pairs[ch.x];
+  DevMpoTerm* st = reinterpret_cast<DevMpoTerm*>(mpo_smem);
+  DevMpoSlot* si = reinterpret_cast<DevMpoSlot*>(st + pr.n_terms);
+  DevMpoOutSlot* so = reinterpret_cast<DevMpoOutSlot*>(si + pr.n_in_slots);
+  for (int i = threadIdx.x; i < pr.n_terms; i += blockDim.x) st[i] = terms[pr.term0 + i];
+  for (int i = threadIdx.x; i < pr.n_in_slots; i += blockDim.x) si[i] = islots[pr.in0 + i];
+  for (int i = threadIdx.x; i < pr.n_out_slots; i += blockDim.x) so[i] = oslots[pr.out0 + i];
+  __syncthreads();
   const int npts = pr.mc * pr.md;
   const int p = ch.y + threadIdx.x;
-  const bool valid = p < npts;
-  const int c = valid ? p / pr.md : 0;
-  const int d = valid ? p % pr.md : 0;
-  // phase 1: inputs of this point
-  for (int i = 0; i < pr.n_in; ++i) {
-    const DevMpoIn in = ins[pr.in0 + i];
-    const int nq = in.mq;
-    const int npq = in.mp * in.mq;
-    for (int j = 0; j < in.mb * npq; ++j) {
-      int b = j / npq, pq = j - b * npq;
-      int pp = pq / nq, q = pq - pp * nq;
-      TI v = TI(0);
-      if (valid)
-        v = reinterpret_cast<const TI*>(in.x1_addr)[(static_cast<int64_t>(b) * pr.mc + c) * in.ld + (pp * nq + q) * pr.md + d];
-      xs[(in.slot0 + j) * kMpoPoints + threadIdx.x] = v;
-    }
-  }
-  // phase 2: sparse terms sorted by output slot
+  if (p >= npts || pr.n_terms == 0) return;
+  const int64_t c = p / pr.md;
+  const int d = p - static_cast<int>(c) * pr.md;
   double acc = 0.0;
-  int cur = -1;
-  for (int t = 0; t < pr.n_terms; ++t) {
-    const DevMpoTerm tm = terms[pr.term0 + t];
-    if (tm.out_slot != cur) {
-      if (cur >= 0 && valid) {
-        const DevMpoOutSlot o = oslots[pr.out0 + cur];
-        img_store(mode, reinterpret_cast<uint8_t*>(o.img_addr), o.lo_off, 0, o.nKt,
-                  o.row0 + static_cast<int64_t>(c) * o.rows_per_c + o.row_add, o.k0 + o.k_add + d, acc);
+  int cur = st[0].out_slot;
+  for (int t0 = 0; t0 < pr.n_terms; t0 += kMpoLoads) {
+    TI xv[kMpoLoads];
+#pragma unroll
+    for (int u = 0; u < kMpoLoads; ++u) {
+      xv[u] = TI(0);
+      if (t0 + u < pr.n_terms) {
+        const DevMpoSlot sl = si[st[t0 + u].in_slot];
+        xv[u] = reinterpret_cast<const TI*>(sl.base)[c * sl.ld + d];
       }
-      cur = tm.out_slot;
-      acc = 0.0;
     }
-    acc += tm.w * static_cast<double>(xs[tm.in_slot * kMpoPoints + threadIdx.x]);
+#pragma unroll
+    for (int u = 0; u < kMpoLoads; ++u) {
+      if (t0 + u >= pr.n_terms) break;
+      const DevMpoTerm tm = st[t0 + u];
+      if (tm.out_slot != cur) {
+        const DevMpoOutSlot o = so[cur];
+        img_store(mode, reinterpret_cast<uint8_t*>(o.img_addr), o.lo_off, 0, o.nKt,
+                  o.row0 + c * o.rows_per_c + o.row_add, o.k0 + o.k_add + d, acc);
+        cur = tm.out_slot;
+        acc = 0.0;
+      }
+      acc += tm.w * static_cast<double>(xv[u]);
+    }
   }
-  if (cur >= 0 && valid) {
-    const DevMpoOutSlot o = oslots[pr.out0 + cur];
-    img_store(mode, reinterpret_cast<uint8_t*>(o.img_addr), o.lo_off, 0, o.nKt,
-              o.row0 + static_cast<int64_t>(c) * o.rows_per_c + o.row_add, o.k0 + o.k_add + d, acc);
+  if (pr.n_terms > 0) {
+    const DevMpoOutSlot o = so[cur];
+    img_store(mode, reinterpret_cast<uint8_t*>(o.img_addr), o.lo_off, 0, o.nKt, o.row0 + c * o.rows_per_c + o.row_add,
+              o.k0 + o.k_add + d, acc);
   }
 }
 
-void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevMpoIn* ins, const DevMpoOutSlot* oslots,
-                      const DevMpoTerm* terms, const int2* chunks, int n_chunks, int max_in_slots,
-                      const int32_t* skip, cudaStream_t st) {
+void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevMpoSlot* islots,
+                      const DevMpoOutSlot* oslots, const DevMpoTerm* terms, const int2* chunks, int n_chunks,
+                      size_t smem_bytes, const int32_t* skip, cudaStream_t st) {
   if (n_chunks <= 0) return;
-  size_t smem = static_cast<size_t>(max_in_slots) * kMpoPoints * (x1_f32 ? 4 : 8);
+  const int smem = static_cast<int>(smem_bytes);
   if (x1_f32) {
-    cudaFuncSetAttribute(mpo_apply_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    mpo_apply_kernel<float><<<n_chunks, kMpoPoints, smem, st>>>(mode, pairs, ins, oslots, terms, chunks, skip);
+    cudaFuncSetAttribute(mpo_apply_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    mpo_apply_kernel<float><<<n_chunks, kMpoThreads, smem, st>>>(mode, pairs, islots, oslots, terms, chunks, skip);
   } else {
-    cudaFuncSetAttribute(mpo_apply_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    mpo_apply_kernel<double><<<n_chunks, kMpoPoints, smem, st>>>(mode, pairs, ins, oslots, terms, chunks, skip);
+    cudaFuncSetAttribute(mpo_apply_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    mpo_apply_kernel<double><<<n_chunks, kMpoThreads, smem, st>>>(mode, pairs, islots, oslots, terms, chunks, skip);
   }
 }
+
+int mpo_points_per_cta() { return kMpoThreads; }
 
 // ---------------------------------------------------------------------------
 // FP64 vector primitives: deterministic two-pass reductions

@@ -15,9 +15,10 @@ void launch_zero_ranges(const uint64_t* out_tab, const DevChunk* chunks, int n_c
                         cudaStream_t st);
 void launch_scatter(const void* res, bool res_f32, double* out, const DevScatSeg* segs, const DevChunk* chunks,
                     int n_chunks, cudaStream_t st);
-void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevMpoIn* ins, const DevMpoOutSlot* oslots,
-                      const DevMpoTerm* terms, const int2* chunks, int n_chunks, int max_in_slots,
-                      const int32_t* skip, cudaStream_t st);
+void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevMpoSlot* islots,
+                      const DevMpoOutSlot* oslots, const DevMpoTerm* terms, const int2* chunks, int n_chunks,
+                      size_t smem_bytes, const int32_t* skip, cudaStream_t st);
+int mpo_points_per_cta();
 void launch_dot(const double* x, const double* y, int64_t n, int kind, double* result, double* partials,
                 const int32_t* skip, cudaStream_t st);
 void launch_lanczos_step(double* w, const double* v, const double* vp, double* vnext, int64_t n, double* alpha,
