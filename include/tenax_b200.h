@@ -92,6 +92,21 @@ int tnx_plan_execute(tnx_plan* plan, const double* const* inputs, double* out, i
                      size_t workspace_bytes, void* stream);
 void tnx_plan_destroy(tnx_plan* plan);
 
+/* tnx_plan_execute (FP64 sector GEMMs) for callers that cannot allocate
+ * device memory.  No counterpart in the reference.  A caller embedded in a
+ * framework that owns the GPU's memory -- an XLA custom call inside a JAX
+ * process that has already reserved most of the device for its own pool, or
+ * any host code that must not cudaMalloc behind its framework's allocator --
+ * passes only its inputs and output; every scratch buffer (operand images,
+ * sector result matrices, intermediates, device index tables) comes from one
+ * file-scope 16 MiB device array that every GPU loading this library holds
+ * until exit.  Plans that need more scratch fail with TNX_ERR_VALUE.  The
+ * first call on a device looks up that array's device address (with that
+ * device current), so make it before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race on it.  Allocates nothing:
+ * no cudaMalloc/cudaFree and no allocating library routine. */
+int tnx_plan_execute_static(const tnx_plan* plan, const double* const* inputs, double* out, void* stream);
+
 /* Two-site effective Hamiltonian "abc,apqd,bpse,eqtf,dfg->cstg"
  * (dmrg.py:1282-1289) over the block structures of L, theta, W_l, W_r, R.
  * The output uses theta's block layout; tnx_heff_closed() reports whether

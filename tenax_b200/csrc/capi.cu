@@ -556,6 +556,179 @@ int tnx_plan_execute(tnx_plan* plan, const double* const* inputs, double* out, i
 
 void tnx_plan_destroy(tnx_plan* plan) { delete plan; }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Contraction without device allocation.
+//
+// Some callers cannot call cudaMalloc: an XLA custom call runs inside a
+// process where JAX has already reserved most of the GPU's memory for its own
+// pool, and code that must not allocate behind its host framework's allocator
+// cannot create the per-plan buffers tnx_plan_execute owns.  For them,
+// tnx_plan_execute_static carves every buffer it needs (operand images,
+// sector result matrices, intermediates of multi-operand plans and the
+// device-side index tables) out of one file-scope device array of
+// kStaticArenaBytes.  Every GPU that loads this library holds that array
+// until the process exits.  The array is shared by all calls and keeps the
+// previous call's contents, so each call zeroes what must start at zero (the
+// operand images and the output); calls that overlap on the GPU race on it.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kStaticArenaBytes = static_cast<size_t>(16) << 20;  // 16 MiB
+__device__ __align__(256) unsigned char g_static_arena[kStaticArenaBytes];
+
+std::mutex g_static_mu;
+std::map<int, uint8_t*> g_static_ptr;  // device ordinal -> device address of g_static_arena
+
+// Device address of the arena for the current device (host code must not use
+// the symbol itself: on the host it is only a stand-in).  Looked up once per
+// device, with that device current.
+uint8_t* static_arena_for_current_device() {
+  int dev = 0;
+  CUDA_OK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  auto it = g_static_ptr.find(dev);
+  if (it != g_static_ptr.end()) return it->second;
+  void* ptr = nullptr;
+  CUDA_OK(cudaGetSymbolAddress(&ptr, g_static_arena));
+  g_static_ptr[dev] = static_cast<uint8_t*>(ptr);
+  return static_cast<uint8_t*>(ptr);
+}
+
+struct ArenaCursor {
+  uint8_t* base;
+  size_t used = 0;
+  uint8_t* take(size_t bytes) {
+    used = (used + 255) & ~static_cast<size_t>(255);
+    uint8_t* p = base + used;
+    used += bytes;
+    return p;
+  }
+};
+}  // namespace
+
+extern "C" int tnx_plan_execute_static(const tnx_plan* plan, const double* const* inputs, double* out,
+                                       void* stream) {
+  TNX_TRY({
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (plan->empty_result) return TNX_OK;
+    const int mode = IMG_F64;
+    const ImgGeom ig = img_geom(mode);
+    // layout pass (sizes only), then the real pass against the arena
+    struct Tables {
+      std::vector<DevPackSeg> pa, pb;
+      std::vector<DevChunk> ca, cb, cs;
+      std::vector<DevGroup> gr;
+      std::vector<int64_t> ro;
+      std::vector<DevTile> tiles;
+      std::vector<DevScatSeg> ss;
+    };
+    uint8_t* arena = static_arena_for_current_device();
+    for (int pass = 0; pass < 2; ++pass) {
+      ArenaCursor cur{pass == 0 ? nullptr : arena};
+      uint64_t* src_tab = reinterpret_cast<uint64_t*>(cur.take(2 * sizeof(uint64_t)));
+      uint64_t* out_tab = reinterpret_cast<uint64_t*>(cur.take(sizeof(uint64_t)));
+      double* one = reinterpret_cast<double*>(cur.take(sizeof(double)));
+      std::vector<double*> inter(plan->steps.size(), nullptr);
+      for (size_t s = 0; s + 1 < plan->steps.size(); ++s)
+        inter[s] = reinterpret_cast<double*>(cur.take(std::max<int64_t>(1, plan->steps[s].out.total) * 8));
+      for (size_t s = 0; s < plan->steps.size(); ++s) {
+        const PairPlan& P = plan->steps[s];
+        PairGeom G = pair_geom(P, mode);
+        const size_t a_bytes = std::max<int64_t>(1, G.a_tiles) * ig.tile_bytes;
+        const size_t b_bytes = std::max<int64_t>(1, G.b_tiles) * ig.tile_bytes;
+        uint8_t* a_img = cur.take(a_bytes);
+        uint8_t* b_img = cur.take(b_bytes);
+        int64_t roff = 0;
+        std::vector<int64_t> res_off;
+        for (auto& g : P.groups) {
+          res_off.push_back(roff);
+          roff += g.M * g.N;
+        }
+        double* res = reinterpret_cast<double*>(cur.take(std::max<int64_t>(1, roff) * 8));
+        Tables T;
+        build_pack(P.packA, G, true, reinterpret_cast<uint64_t>(a_img), 0, ig.tile_bytes, 0, T.pa, T.ca);
+        build_pack(P.packB, G, false, reinterpret_cast<uint64_t>(b_img), 0, ig.tile_bytes, 1, T.pb, T.cb);
+        for (size_t g = 0; g < P.groups.size(); ++g) {
+          DevGroup x{};
+          x.a_addr = reinterpret_cast<uint64_t>(a_img) + static_cast<uint64_t>(G.a_tile0[g]) * ig.tile_bytes;
+          x.b_addr = reinterpret_cast<uint64_t>(b_img) + static_cast<uint64_t>(G.b_tile0[g]) * ig.tile_bytes;
+          x.rowoff0 = static_cast<int64_t>(T.ro.size());
+          x.M = static_cast<int32_t>(P.groups[g].M);
+          x.N = static_cast<int32_t>(P.groups[g].N);
+          x.nKt = G.nKt[g];
+          x.out_slot = 0;
+          T.gr.push_back(x);
+          for (int64_t r = 0; r < P.groups[g].M; ++r) T.ro.push_back(res_off[g] + r * P.groups[g].N);
+        }
+        std::vector<std::pair<int64_t, DevTile>> tl;
+        build_tiles(P, G, 0, tl);
+        T.tiles = sorted_tiles(tl);
+        for (auto& sc : P.scatter) {
+          DevScatSeg x{};
+          x.dst_off = sc.dst_off;
+          x.ld = P.groups[sc.group].N;
+          x.src_base = res_off[sc.group] + static_cast<int64_t>(sc.row0) * x.ld + sc.col0;
+          x.nlegs = sc.nlegs;
+          for (int l = 0; l < sc.nlegs; ++l) {
+            x.dims[l] = sc.dims[l];
+            x.rstr[l] = sc.rstr[l];
+            x.cstr[l] = sc.cstr[l];
+          }
+          const int id = static_cast<int>(T.ss.size());
+          T.ss.push_back(x);
+          for (int64_t k = 0; k < sc.count; k += 2048)
+            T.cs.push_back({id, 0, k, std::min<int64_t>(2048, sc.count - k)});
+        }
+        auto put = [&](const auto& v) {
+          using E = typename std::decay_t<decltype(v)>::value_type;
+          E* d = reinterpret_cast<E*>(cur.take(std::max<size_t>(1, v.size()) * sizeof(E)));
+          if (pass == 1 && !v.empty())
+            CUDA_OK(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(E), cudaMemcpyHostToDevice, st));
+          return d;
+        };
+        DevPackSeg* dpa = put(T.pa);
+        DevChunk* dca = put(T.ca);
+        DevPackSeg* dpb = put(T.pb);
+        DevChunk* dcb = put(T.cb);
+        DevGroup* dgr = put(T.gr);
+        int64_t* dro = put(T.ro);
+        DevTile* dtl = put(T.tiles);
+        DevScatSeg* dss = put(T.ss);
+        DevChunk* dcs = put(T.cs);
+        if (cur.used > kStaticArenaBytes)
+          return set_err(TNX_ERR_VALUE, "contraction needs " + std::to_string(cur.used) +
+                                            " bytes of device scratch; the static arena of tnx_plan_execute_static "
+                                            "holds " + std::to_string(kStaticArenaBytes) + " bytes");
+        if (pass == 0) continue;
+        const double* a_ptr = plan->a_src[s] >= 0 ? inputs[plan->a_src[s]] : inter[s - 1];
+        const double* b_ptr = inputs[plan->b_src[s]];
+        if (plan->has_scalar) {
+          const double v1 = 1.0;
+          CUDA_OK(cudaMemcpyAsync(one, &v1, sizeof(double), cudaMemcpyHostToDevice, st));
+          b_ptr = one;
+        }
+        double* o_ptr = (s + 1 == plan->steps.size()) ? out : inter[s];
+        const uint64_t src2[2] = {reinterpret_cast<uint64_t>(a_ptr), reinterpret_cast<uint64_t>(b_ptr)};
+        const uint64_t res1 = reinterpret_cast<uint64_t>(res);
+        CUDA_OK(cudaMemcpyAsync(src_tab, src2, sizeof(src2), cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(out_tab, &res1, sizeof(res1), cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemsetAsync(a_img, 0, a_bytes, st));
+        CUDA_OK(cudaMemsetAsync(b_img, 0, b_bytes, st));
+        launch_pack(src_tab, dpa, dca, static_cast<int>(T.ca.size()), mode, nullptr, st);
+        launch_pack(src_tab, dpb, dcb, static_cast<int>(T.cb.size()), mode, nullptr, st);
+        launch_gemm_f64(dgr, dtl, static_cast<int>(T.tiles.size()), dro, out_tab, nullptr, st);
+        if (P.out.total > 0) CUDA_OK(cudaMemsetAsync(o_ptr, 0, P.out.total * sizeof(double), st));
+        launch_scatter(res, false, o_ptr, dss, dcs, static_cast<int>(T.cs.size()), st);
+        CUDA_OK(cudaGetLastError());
+      }
+    }
+    return TNX_OK;
+  })
+}
+
+extern "C" {
+
 // ---------------------------------------------------------------------------
 // H_eff
 // ---------------------------------------------------------------------------
