@@ -1,0 +1,422 @@
+"""Two-site symmetric DMRG on the GPU.
+
+Same driver, configuration and result as tenax's symmetric back-end
+(algorithms/dmrg.py:44-305, 890-1365): environment updates via the
+unfiltered block contraction, theta via ``contract``, the two-site H_eff
+matvec via the fused ``HeffOperator``, a device-side Lanczos (FP64 scalars
+and vectors, one host read-back per solve), and the block-diagonal truncated
+SVD (linalg.py:75-333) with cuSOLVER per charge sector.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass
+from typing import NamedTuple
+
+import numpy as np
+import torch
+
+from tenax_b200 import _capi, vector
+from tenax_b200.contraction import blockwise_contract, contract
+from tenax_b200.core import FlowDirection, TensorIndex, U1Symmetry
+from tenax_b200.heff import HeffBatch, HeffOperator
+from tenax_b200.network import TensorNetwork
+from tenax_b200.tensor import SymmetricTensor, _device, block_shape, embed_in_keys, restrict_to_keys
+
+
+@dataclass
+class DMRGConfig:
+    """(algorithms/dmrg.py:44-77); ``precision`` selects the H_eff sector GEMMs:
+    "fp64" (DMMA), "bf16x3" or "tf32" (tcgen05).  With a mixed precision the
+    Lanczos recurrence stays FP64 and the reported energy is the FP64 Rayleigh
+    quotient of the Ritz vector when ``fp64_energy`` is set."""
+
+    max_bond_dim: int = 100
+    num_sweeps: int = 10
+    convergence_tol: float = 1e-10
+    num_states: int = 1
+    two_site: bool = True
+    lanczos_max_iter: int = 50
+    lanczos_tol: float = 1e-12
+    noise: float = 0.0
+    svd_trunc_err: float | None = None
+    target_charge: int | None = None
+    verbose: bool = False
+    precision: str = "fp64"
+    fp64_energy: bool = True
+
+
+class DMRGResult(NamedTuple):
+    energy: float
+    energies_per_sweep: list
+    mps: TensorNetwork
+    truncation_errors: list
+    converged: bool
+
+
+# ---------------------------------------------------------------------------
+# padding and environments
+# ---------------------------------------------------------------------------
+
+def _pad(t: SymmetricTensor, pad_left: bool) -> SymmetricTensor:
+    """Add a trivial charge-0 leg (dmrg.py:924-952); the flat data is unchanged."""
+    u1 = U1Symmetry()
+    z = np.zeros(1, np.int32)
+    if pad_left:
+        idx = (TensorIndex(u1, z, FlowDirection.IN, "_pad_l"),) + t.indices
+        keys = [(0,) + k for k in t.keys]
+    else:
+        idx = t.indices + (TensorIndex(u1, z, FlowDirection.OUT, "_pad_r"),)
+        keys = [k + (0,) for k in t.keys]
+    return SymmetricTensor.from_flat(idx, keys, t.data)
+
+
+def _unpad(t: SymmetricTensor, pad_left: bool) -> SymmetricTensor:
+    """(dmrg.py:955-975)"""
+    if pad_left:
+        return SymmetricTensor.from_flat(t.indices[1:], [k[1:] for k in t.keys], t.data)
+    return SymmetricTensor.from_flat(t.indices[:-1], [k[:-1] for k in t.keys], t.data)
+
+
+def _trivial_env(left: bool) -> SymmetricTensor:
+    """(dmrg.py:890-921)"""
+    u1 = U1Symmetry()
+    z = np.zeros(1, np.int32)
+    if left:
+        idx = (TensorIndex(u1, z, FlowDirection.IN, "env_mps_l"), TensorIndex(u1, z, FlowDirection.IN, "env_mpo_l"),
+               TensorIndex(u1, z, FlowDirection.OUT, "env_mps_conj_l"))
+    else:
+        idx = (TensorIndex(u1, z, FlowDirection.OUT, "env_mps_r"), TensorIndex(u1, z, FlowDirection.OUT, "env_mpo_r"),
+               TensorIndex(u1, z, FlowDirection.IN, "env_mps_conj_r"))
+    return SymmetricTensor.from_flat(idx, [(0, 0, 0)], torch.ones(1, dtype=torch.float64, device=_device()))
+
+
+def _pad_site(A: SymmetricTensor) -> SymmetricTensor:
+    if A.ndim == 2:
+        lab0 = A.labels()[0]
+        return _pad(A, pad_left=isinstance(lab0, str) and lab0.startswith("p"))
+    return A
+
+
+def update_left_env(env, A, W, precision="fp64"):
+    """new_L[d,e,f] = L[a,b,c] A[a,p,d] W[b,p,x,e] A*[c,x,f] (dmrg.py:1165-1198)."""
+    A = _pad_site(A)
+    out_idx = (A.indices[2], W.indices[3], A.indices[2])
+    return blockwise_contract([env, A, W, A], "abc,apd,bpxe,cxf->def", out_idx, precision)
+
+
+def update_right_env(env, B, W, precision="fp64"):
+    """new_R[d,e,f] = R[a,b,c] B[d,p,a] W[e,p,x,b] B*[f,x,c] (dmrg.py:1201-1232)."""
+    B = _pad_site(B)
+    out_idx = (B.indices[0], W.indices[0], B.indices[0])
+    return blockwise_contract([env, B, W, B], "abc,dpa,epxb,fxc->def", out_idx, precision)
+
+
+# ---------------------------------------------------------------------------
+# Lanczos on the device
+# ---------------------------------------------------------------------------
+
+class LanczosStats(NamedTuple):
+    steps: int
+    alphas: np.ndarray
+    betas: np.ndarray
+    seconds: float
+
+
+def lanczos(op: HeffOperator, theta: SymmetricTensor, num_steps: int, tol: float, fp64_op: HeffOperator | None = None):
+    """Plain three-term Lanczos without reorthogonalisation (dmrg.py:978-1045).
+
+    Krylov vectors live on the operator's closed key layout; alpha/beta and
+    the early-exit flag stay on the device until the single read-back after
+    the loop.  Returns (eigenvalue, eigenvector SymmetricTensor with the
+    reference's key set, LanczosStats).
+    """
+    t0 = time.perf_counter()
+    dev = theta.data.device
+    n = op.size
+    x0 = embed_in_keys(theta, op.keys).data
+    basis = torch.empty((num_steps + 1, max(n, 1)), dtype=torch.float64, device=dev)
+    alpha = torch.zeros(num_steps + 1, dtype=torch.float64, device=dev)
+    beta = torch.zeros(num_steps + 2, dtype=torch.float64, device=dev)
+    done = torch.zeros(1, dtype=torch.int32, device=dev)
+    w = torch.empty(max(n, 1), dtype=torch.float64, device=dev)
+    nrm = vector.nrm2(x0)
+    vector.scale(x0, nrm, 2, out=basis[0, :n])
+    batch = HeffBatch([op], skip_flag=done)
+    scr = vector.scratch(dev)
+    st = torch.cuda.current_stream().cuda_stream
+    for k in range(num_steps):
+        batch.apply([basis[k, :n]], [w[:n]])
+        _capi.check(_capi.LIB.tnx_lanczos_step(
+            w.data_ptr(), basis[k].data_ptr(), basis[k - 1].data_ptr() if k > 0 else 0,
+            basis[k + 1].data_ptr(), n, alpha.data_ptr(), beta.data_ptr(), k, float(tol), done.data_ptr(),
+            scr.data_ptr(), st))
+    a = alpha.cpu().numpy()
+    b = beta.cpu().numpy()
+    if batch.device_error():
+        raise RuntimeError("tcgen05 GEMM reported a device-side timeout")
+    m = num_steps
+    for k in range(num_steps):
+        if b[k + 1] < tol:
+            m = k + 1
+            break
+    key_seq = op.key_seq
+    if m == 1 or num_steps == 0:
+        vec = basis[0, :n]
+        keys = key_seq[0]
+        energy = float(a[0]) if m == 1 else 0.0
+    else:
+        T = np.diag(a[:m]) + np.diag(b[1:m], 1) + np.diag(b[1:m], -1)
+        ev, evecs = np.linalg.eigh(T)
+        idx = int(np.argmin(ev))
+        energy = float(ev[idx])
+        coefs = torch.from_numpy(np.ascontiguousarray(evecs[:, idx])).to(dev)
+        table = torch.tensor([basis[k].data_ptr() for k in range(m)], dtype=torch.int64, device=dev)
+        out = torch.empty(max(n, 1), dtype=torch.float64, device=dev)
+        _capi.check(_capi.LIB.tnx_combine(table.data_ptr(), coefs.data_ptr(), m, n, out.data_ptr(), st))
+        nn = vector.nrm2(out[:n])
+        vec = vector.scale(out[:n], nn, 2)
+        keys = key_seq[min(m - 1, len(key_seq) - 1)]
+    full = SymmetricTensor.from_flat(theta.indices, op.keys, vec)
+    if fp64_op is not None and m > 1:
+        # Rayleigh quotient of the Ritz vector with the FP64 operator
+        hv = fp64_op.apply(vec)
+        energy = float(vector.dot(vec, hv)) / float(vector.dot(vec, vec))
+    result = restrict_to_keys(full, keys)
+    return energy, result, LanczosStats(m, a[:m], b[1:m + 1], time.perf_counter() - t0)
+
+
+# ---------------------------------------------------------------------------
+# truncated block SVD and bond scaling
+# ---------------------------------------------------------------------------
+
+def truncated_svd(t: SymmetricTensor, left_labels, right_labels, new_bond_label, max_singular_values=None,
+                  max_truncation_err=None, normalize=False):
+    """Block-diagonal SVD with global truncation (linalg.py:75-333).
+
+    Sectors = fused flow-weighted charge of the left legs; each sector matrix
+    is assembled on the device from the blocks reshaped in their stored leg
+    order (linalg.py:186), decomposed with torch.linalg.svd (cuSOLVER), and
+    the singular values are merged and stably sorted by -s on the host.
+    Returns (U, s_kept (numpy), Vh, s_full (numpy)).
+    """
+    labels = t.labels()
+    l2a = {l: i for i, l in enumerate(labels)}
+    la = [l2a[l] for l in left_labels]
+    ra = [l2a[l] for l in right_labels]
+    sym = t.indices[0].symmetry
+    mod = sym.n_values()
+    blocks = t.blocks
+    grouped: dict = {}
+    for key in t.keys:
+        q = sum(int(t.indices[i].flow) * int(key[i]) for i in la)
+        if mod is not None:
+            q %= mod
+        grouped.setdefault(q, []).append((tuple(key[i] for i in la), tuple(key[i] for i in ra), key))
+    results = {}
+    for q, entries in grouped.items():
+        lseen, rseen = {}, {}
+        for lk, rk, _ in entries:
+            lseen.setdefault(lk, len(lseen))
+            rseen.setdefault(rk, len(rseen))
+        lsz = [int(np.prod([np.count_nonzero(t.indices[a].charges == c) for a, c in zip(la, lk)])) for lk in lseen]
+        rsz = [int(np.prod([np.count_nonzero(t.indices[a].charges == c) for a, c in zip(ra, rk)])) for rk in rseen]
+        if sum(lsz) == 0 or sum(rsz) == 0:
+            continue
+        loff = np.concatenate([[0], np.cumsum(lsz)])
+        roff = np.concatenate([[0], np.cumsum(rsz)])
+        M = torch.zeros((int(loff[-1]), int(roff[-1])), dtype=torch.float64, device=t.data.device)
+        for lk, rk, key in entries:
+            li, ri = lseen[lk], rseen[rk]
+            M[loff[li]:loff[li + 1], roff[ri]:roff[ri + 1]] = blocks[key].reshape(lsz[li], rsz[ri])
+        U, S, Vh = torch.linalg.svd(M, full_matrices=False)
+        results[q] = (U, S, Vh, list(lseen), list(rseen), lsz, rsz, loff, roff)
+    s_host = {q: r[1].cpu().numpy() for q, r in results.items()}
+    pairs = [(float(v), q, i) for q in results for i, v in enumerate(s_host[q])]
+    pairs.sort(key=lambda x: -x[0])
+    s_full = np.array([v for v, _, _ in pairs])
+    n_total = len(pairs)
+    n_keep = n_total
+    if max_truncation_err is not None and n_total > 0:
+        tot = sum(x[0] ** 2 for x in pairs)
+        if tot > 0:
+            tr = 0.0
+            for i in range(n_total - 1, 0, -1):
+                tr += pairs[i][0] ** 2
+                if tr / tot > max_truncation_err ** 2:
+                    n_keep = i + 1
+                    break
+            else:
+                n_keep = n_total
+    if max_singular_values is not None:
+        n_keep = min(n_keep, max_singular_values)
+    n_keep = max(1, min(n_keep, n_total))
+    kept = pairs[:n_keep]
+    bond_charges = np.array([q for _, q, _ in kept], dtype=np.int32)
+    s_final = np.array([v for v, _, _ in kept])
+    if normalize and s_final.sum() > 0:
+        s_final = s_final / s_final.sum()
+    cols: dict = {}
+    for g, (_, q, i) in enumerate(kept):
+        cols.setdefault(q, []).append(i)
+    left_idx = tuple(t.indices[i] for i in la)
+    right_idx = tuple(t.indices[i] for i in ra)
+    U_idx = left_idx + (TensorIndex(sym, bond_charges, FlowDirection.OUT, new_bond_label),)
+    V_idx = (TensorIndex(sym, bond_charges, FlowDirection.IN, new_bond_label),) + right_idx
+    Ub, Vb = {}, {}
+    for q, sv in cols.items():
+        U, _, Vh, lks, rks, lsz, rsz, loff, roff = results[q]
+        sel = torch.as_tensor(sv, device=U.device)
+        Ut = U.index_select(1, sel)
+        Vt = Vh.index_select(0, sel)
+        for li, lk in enumerate(lks):
+            shp = tuple(int(np.count_nonzero(t.indices[a].charges == c)) for a, c in zip(la, lk))
+            Ub[lk + (q,)] = Ut[loff[li]:loff[li + 1]].reshape(shp + (len(sv),))
+        for ri, rk in enumerate(rks):
+            shp = tuple(int(np.count_nonzero(t.indices[a].charges == c)) for a, c in zip(ra, rk))
+            Vb[(q,) + rk] = Vt[:, roff[ri]:roff[ri + 1]].reshape((len(sv),) + shp)
+    validate = not any(int(sum(int(i.flow) * int(q) for i, q in zip(t.indices, k))) != 0 for k in t.keys[:1])
+    return (SymmetricTensor(Ub, U_idx, _validate=validate), s_final, SymmetricTensor(Vb, V_idx, _validate=validate),
+            s_full)
+
+
+def scale_bond_axis(t: SymmetricTensor, label, scale) -> SymmetricTensor:
+    """Scale along a labelled axis at the positions of each block's charge
+    (algorithms/_tensor_utils.py:17-62)."""
+    axis = t.labels().index(label)
+    idx = t.indices[axis]
+    s = torch.as_tensor(np.asarray(scale, dtype=np.float64), device=t.data.device)
+    out = torch.empty_like(t.data)
+    for i, k in enumerate(t.keys):
+        pos = np.nonzero(idx.charges == k[axis])[0]
+        shp = t._shapes[i]
+        view = [1] * t.ndim
+        view[axis] = shp[axis]
+        sel = s[torch.as_tensor(pos[: shp[axis]], device=s.device)].view(view)
+        out[t.offsets[i]:t.offsets[i + 1]] = (t.data[t.offsets[i]:t.offsets[i + 1]].view(shp) * sel).reshape(-1)
+    return SymmetricTensor.from_flat(t.indices, t.keys, out)
+
+
+def svd_and_truncate_site(theta, site, config, sweep_right=True):
+    """(dmrg.py:808-882)"""
+    labels = theta.labels()
+    left_virt = f"v{site - 1}_{site}" if site > 0 else None
+    right_virt = f"v{site + 1}_{site + 2}"
+    ll = [l for l in labels if l in (left_virt, f"p{site}") and l is not None]
+    rl = [l for l in labels if l in (right_virt, f"p{site + 1}") and l is not None]
+    if not ll or not rl:
+        n = len(labels)
+        ll, rl = list(labels[: n // 2]), list(labels[n // 2:])
+    bond = f"v{site}_{site + 1}"
+    A, s, B, s_full = truncated_svd(theta, ll, rl, bond, config.max_bond_dim, config.svd_trunc_err)
+    if len(s_full) > len(s):
+        err = float(np.sqrt(np.sum(s_full[len(s):] ** 2) / (np.sum(s_full ** 2) + 1e-15)))
+    else:
+        err = 0.0
+    if sweep_right:
+        B = scale_bond_axis(B, bond, s)
+    else:
+        A = scale_bond_axis(A, bond, s)
+    return A, s, B, err
+
+
+# ---------------------------------------------------------------------------
+# sweep driver
+# ---------------------------------------------------------------------------
+
+class SiteStats(NamedTuple):
+    site: int
+    chi_theta: int
+    lanczos_steps: int
+    seconds: float
+
+
+def two_site_update(site_l, site_r, L, Wl, Wr, R, config, stats: list | None = None):
+    """(dmrg.py:1235-1299)"""
+    t0 = time.perf_counter()
+    shared = set(site_l.labels()) & set(site_r.labels())
+    theta = contract(site_l, site_r) if shared else site_l
+    ndim0 = theta.ndim
+    pad_left = False
+    if ndim0 == 3:
+        lab0 = theta.labels()[0]
+        if not (isinstance(lab0, str) and lab0.startswith("v")):
+            pad_left = True
+            theta = _pad(theta, True)
+        else:
+            theta = _pad(theta, False)
+    op = HeffOperator(L, Wl, Wr, R, theta.indices, theta.keys, config.precision)
+    fp64_op = None
+    if config.precision != "fp64" and config.fp64_energy:
+        fp64_op = HeffOperator(L, Wl, Wr, R, theta.indices, theta.keys, "fp64")
+    energy, th, ls = lanczos(op, theta, config.lanczos_max_iter, config.lanczos_tol, fp64_op)
+    if ndim0 == 3:
+        th = _unpad(th, pad_left)
+    if stats is not None:
+        stats.append(SiteStats(-1, int(theta.indices[0].dim), ls.steps, time.perf_counter() - t0))
+    return th, energy
+
+
+def dmrg(hamiltonian: TensorNetwork, initial_mps: TensorNetwork, config: DMRGConfig, stats: list | None = None):
+    """Two-site symmetric DMRG (dmrg.py:125-305) with every contraction on the GPU."""
+    Ln = hamiltonian.n_nodes()
+    mps = [initial_mps.get_tensor(i) for i in range(Ln)]
+    mpo = [hamiltonian.get_tensor(i) for i in range(Ln)]
+    if not all(isinstance(t, SymmetricTensor) for t in mps + mpo):
+        raise TypeError("dmrg() requires uniform tensor types: all SymmetricTensor for the GPU back-end.")
+    if not config.two_site:
+        raise _capi.TnxUnsupported("only two-site DMRG is implemented on the GPU path")
+    prec = "fp64"
+
+    def build_left():
+        envs = [None] * (Ln + 1)
+        envs[0] = _trivial_env(True)
+        for i in range(Ln - 1):
+            envs[i + 1] = update_left_env(envs[i], mps[i], mpo[i], prec)
+        return envs
+
+    def build_right():
+        envs = [None] * (Ln + 1)
+        envs[Ln] = _trivial_env(False)
+        for i in range(Ln - 1, 0, -1):
+            envs[i] = update_right_env(envs[i + 1], mps[i], mpo[i], prec)
+        return envs
+
+    left, right = build_left(), build_right()
+    energies, terrs = [], []
+    energy, converged = 0.0, False
+    for sweep in range(config.num_sweeps):
+        prev = energy
+        if sweep > 0:
+            left = build_left()
+        for i in range(Ln - 1):
+            r = right[i + 2] if right[i + 2] is not None else _trivial_env(False)
+            th, e = two_site_update(mps[i], mps[i + 1], left[i], mpo[i], mpo[i + 1], r, config, stats)
+            energy = float(e)
+            A, s, B, err = svd_and_truncate_site(th, i, config)
+            mps[i], mps[i + 1] = A, B
+            terrs.append(err)
+            left[i + 1] = update_left_env(left[i], A, mpo[i], prec)
+        right = build_right()
+        for i in range(Ln - 2, -1, -1):
+            r2 = right[i + 2] if right[i + 2] is not None else _trivial_env(False)
+            th, e = two_site_update(mps[i], mps[i + 1], left[i], mpo[i], mpo[i + 1], r2, config, stats)
+            energy = float(e)
+            A, s, B, err = svd_and_truncate_site(th, i, config, sweep_right=False)
+            mps[i], mps[i + 1] = A, B
+            terrs.append(err)
+            right[i + 1] = update_right_env(r2, B, mpo[i + 1], prec)
+        energies.append(energy)
+        if config.verbose:
+            print(f"Sweep {sweep + 1}/{config.num_sweeps}: E = {energy:.10f}")
+        if sweep > 0 and abs(energy - prev) < config.convergence_tol:
+            converged = True
+            break
+    net = TensorNetwork(name="DMRG_MPS")
+    for i, t in enumerate(mps):
+        net.add_node(i, t)
+    for i in range(Ln - 1):
+        for lab in sorted(set(mps[i].labels()) & set(mps[i + 1].labels()), key=str):
+            net.connect(i, lab, i + 1, lab)
+    return DMRGResult(energy, energies, net, terrs, converged)

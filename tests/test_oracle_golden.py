@@ -78,3 +78,14 @@ def test_auto_mpo_matches_reference(golden_dir):
             assert sorted(blocks) == sorted(ref.blocks), (prefix, i)
             for k in blocks:
                 np.testing.assert_array_equal(blocks[k], ref.blocks[k])
+
+
+def test_oracle_dmrg_config1_energy(golden_dir):
+    """Full config-1 DMRG (L=20, chi=64, 2 sweeps, 10 Lanczos steps) from the
+    reference's own initial MPS: converged energy within 1e-9."""
+    z = np.load(os.path.join(golden_dir, "dmrg_c1_L20.npz"))
+    mps = [unpack_tensor(z, f"mps{i}") for i in range(20)]
+    mpo = [unpack_tensor(z, f"mpo{i}") for i in range(20)]
+    e, es, _, te = odmrg.dmrg(mpo, mps, 64, 2, lanczos_max_iter=10)
+    assert abs(e - float(z["energy"])) <= 1e-9
+    assert len(te) == len(z["truncation_errors"])
