@@ -367,8 +367,64 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def run_dmrg_study(args):
+    """Two-site DMRG on the width-6 Heisenberg cylinder at chi (default 2048):
+    sweep seconds and energies for FP64 and the mixed precisions; matvec
+    residual of the mixed H_eff against FP64 at every site; energy
+    difference to the FP64 run after every sweep."""
+    import torch
+
+    from tenax_b200.dmrg import DMRGConfig, SiteStats, SweepStats, dmrg
+    from tenax_b200.workloads import cylinder_mpo, random_symmetric_mps
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    Lx, Ly = args.cyl_lx, 6
+    mpo = cylinder_mpo(Lx, Ly)
+    out = {"study": "two-site DMRG, width-6 Heisenberg cylinder (U(1), J=1)", "sites": Lx * Ly, "chi": args.chi,
+           "sweeps": args.sweeps, "lanczos_max_iter": args.lanczos, "data": "seeded random initial MPS", "runs": {}}
+    fp64_e = None
+    for prec in args.dmrg_precisions.split(","):
+        mps = random_symmetric_mps(Lx * Ly, args.chi, seed=args.seed)
+        cfg = DMRGConfig(max_bond_dim=args.chi, num_sweeps=args.sweeps, lanczos_max_iter=args.lanczos,
+                         convergence_tol=0.0, precision=prec, check_matvec_residual=prec != "fp64")
+        stats: list = []
+        phases: dict = {}
+        res = dmrg(mpo, mps, cfg, stats, phases)
+        sw = [s for s in stats if isinstance(s, SweepStats)]
+        st = [s for s in stats if isinstance(s, SiteStats)]
+        nsite = (Lx * Ly - 1) * 2
+        rel = [s.matvec_rel_err for s in st if s.matvec_rel_err is not None]
+        te = np.array(res.truncation_errors).reshape(len(sw), -1)
+        diag = np.array([s.diag_seconds for s in st]).reshape(len(sw), nsite).sum(axis=1)
+        run = {"sweep_s": [round(s.seconds - d, 3) for s, d in zip(sw, diag)],
+               "diagnostic_s_excluded": [round(float(d), 3) for d in diag],
+               "phase_s": {k: round(v, 3) for k, v in phases.items()},
+               "energies": [float(e) for e in res.energies_per_sweep],
+               "max_bond": [s.max_bond for s in sw], "matvecs_per_sweep": [s.matvecs for s in sw],
+               "truncation_err_max": [float(x) for x in te.max(axis=1)],
+               "site_seconds_max": round(max(s.seconds for s in st), 3)}
+        if rel:
+            r = np.array(rel).reshape(len(sw), nsite)
+            run["matvec_rel_err_median"] = [float(np.median(x)) for x in r]
+            run["matvec_rel_err_max"] = [float(np.max(x)) for x in r]
+        if prec == "fp64":
+            fp64_e = run["energies"]
+        elif fp64_e is not None:
+            run["dE_vs_fp64"] = [float(a - b) for a, b in zip(run["energies"], fp64_e)]
+        out["runs"][prec] = run
+        del res, mps
+        torch.cuda.empty_cache()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--dmrg", action="store_true", help="run the cylinder DMRG precision study instead")
+    ap.add_argument("--chi", type=int, default=2048)
+    ap.add_argument("--sweeps", type=int, default=4)
+    ap.add_argument("--lanczos", type=int, default=20)
+    ap.add_argument("--cyl-lx", type=int, default=4)
+    ap.add_argument("--dmrg-precisions", default="fp64,bf16x3,tf32")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
@@ -384,7 +440,9 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     sys.path.insert(0, ROOT)
-    if args.impl == "reference":
+    if args.dmrg:
+        run_dmrg_study(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -154,11 +154,15 @@ int tnx_nrm2(const double* x, int64_t n, double* result, double* scratch, void* 
 
 /* One Lanczos orthogonalisation step (dmrg.py:1005-1019) on device:
  *   alpha[k] = <v, w>;  w -= alpha[k] v  (- beta[k] v_prev if k > 0);
- *   beta[k+1] = ||w||;  if beta[k+1] < tol: *done = 1  else v_next = w / beta[k+1]
+ *   beta[k+1] = ||w||;  if beta[k+1] < tol or beta[k+1] < tol_rel*|alpha[k]|: *done = 1
+ *   else v_next = w / beta[k+1]
+ * tol_rel = 0 is the reference's test; a mixed-precision matvec passes its
+ * relative noise level so the recurrence stops instead of orthogonalising noise.
  * alpha/beta live in device memory; nothing is read back to the host.
  * Every kernel of the step returns immediately once *done is set. */
 int tnx_lanczos_step(double* w, const double* v, const double* v_prev, double* v_next, int64_t n, double* alpha,
-                     double* beta, int32_t k, double tol, int32_t* done, double* scratch, void* stream);
+                     double* beta, int32_t k, double tol, double tol_rel, int32_t* done, double* scratch,
+                     void* stream);
 /* out = sum_k coefs[k] * basis[k], summed left to right as the reference's
  * eigenvector reconstruction (dmrg.py:1038-1040); device pointer table and
  * device coefficients. */

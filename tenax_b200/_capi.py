@@ -84,7 +84,7 @@ def _load():
         "tnx_reduce_scratch_len": (i64, []),
         "tnx_dot": (C.c_int, [P, P, i64, P, P, P]),
         "tnx_nrm2": (C.c_int, [P, i64, P, P, P]),
-        "tnx_lanczos_step": (C.c_int, [P, P, P, P, i64, P, P, i32, dbl, P, P, P]),
+        "tnx_lanczos_step": (C.c_int, [P, P, P, P, i64, P, P, i32, dbl, dbl, P, P, P]),
         "tnx_combine": (C.c_int, [P, P, i32, i64, P, P]),
         "tnx_scale": (C.c_int, [P, P, i64, P, i32, P]),
     }

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -48,6 +49,22 @@ static int set_err(int code, const std::string& msg) {
 // device memory
 // ---------------------------------------------------------------------------
 namespace {
+// Plans, operators and batches are created per DMRG site, so their buffers
+// come from the device's stream-ordered memory pool (cudaMallocAsync on the
+// legacy default stream, which orders against all blocking streams) with the
+// pool told to keep freed memory: no device-wide synchronisation per buffer.
+void retain_pool_memory() {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  });
+}
+
 struct DevMem {
   void* p = nullptr;
   size_t n = 0;
@@ -55,13 +72,14 @@ struct DevMem {
   DevMem(const DevMem&) = delete;
   DevMem& operator=(const DevMem&) = delete;
   ~DevMem() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, cudaStreamLegacy);
   }
   void alloc(size_t bytes) {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, cudaStreamLegacy);
     p = nullptr;
     n = bytes;
-    if (bytes) CUDA_OK(cudaMalloc(&p, bytes));
+    retain_pool_memory();
+    if (bytes) CUDA_OK(cudaMallocAsync(&p, bytes, cudaStreamLegacy));
   }
   template <class T>
   T* as() const {
@@ -139,7 +157,7 @@ PairGeom pair_geom(const PairPlan& P, int mode) {
 
 void build_pack(const std::vector<PackSeg>& segs, const PairGeom& G, bool a_side, uint64_t img_base,
                 int64_t lo_off, int tile_bytes, int src_slot, std::vector<DevPackSeg>& out,
-                std::vector<DevChunk>& chunks) {
+                std::vector<DevChunk>& chunks, double scale = 1.0) {
   for (auto& s : segs) {
     DevPackSeg d{};
     d.src_off = s.src_off;
@@ -152,6 +170,7 @@ void build_pack(const std::vector<PackSeg>& segs, const PairGeom& G, bool a_side
     d.nlegs = s.nlegs;
     d.src_slot = src_slot;
     d.kcount = 1;
+    d.scale = scale;
     for (int l = 0; l < s.nlegs; ++l) {
       d.dims[l] = s.dims[l];
       d.rstr[l] = s.rstr[l];
@@ -475,6 +494,7 @@ static void plan_build_device(tnx_plan* p, int precision) {
       x.N = static_cast<int32_t>(P.groups[g].N);
       x.nKt = d->G.nKt[g];
       x.out_slot = 0;
+      x.scale = 1.0;
       gr.push_back(x);
       for (int64_t r = 0; r < P.groups[g].M; ++r) ro.push_back(res_off[g] + r * P.groups[g].N);
     }
@@ -658,6 +678,7 @@ extern "C" int tnx_plan_execute_static(const tnx_plan* plan, const double* const
           x.N = static_cast<int32_t>(P.groups[g].N);
           x.nKt = G.nKt[g];
           x.out_slot = 0;
+          x.scale = 1.0;
           T.gr.push_back(x);
           for (int64_t r = 0; r < P.groups[g].M; ++r) T.ro.push_back(res_off[g] + r * P.groups[g].N);
         }
@@ -739,6 +760,7 @@ struct tnx_heff {
   int64_t l_lo = 0, r_lo = 0;
   PairGeom g1, g4;
   bool terms_ready = false;
+  double out_scale = 1.0;  // 2^(eL + eR): undoes the operator range scaling
 };
 
 int tnx_heff_create(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, const tnx_tensor_desc* Wl,
@@ -798,10 +820,27 @@ int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const
     h->r_lo = h->g4.b_tiles * ig.tile_bytes;
     CUDA_OK(cudaMemsetAsync(h->l_img.p, 0, h->l_img.n, st));
     CUDA_OK(cudaMemsetAsync(h->r_img.p, 0, h->r_img.n, st));
+    // Environments can sit far outside the FP32/BF16 range (a random MPS's
+    // environments shrink geometrically with length): pack L and R divided by
+    // powers of two near their max-abs and multiply 2^(eL+eR) back in the
+    // stage-4 epilogue.  Powers of two keep the FP64 path bit-exact.
+    DevMem red;
+    const int np = reduce_partials_count();
+    red.alloc((np + 2) * sizeof(double));
+    double mx[2] = {0.0, 0.0};
+    if (H.L.total) launch_maxabs(L, H.L.total, red.as<double>() + np, red.as<double>(), st);
+    if (H.R.total) launch_maxabs(R, H.R.total, red.as<double>() + np + 1, red.as<double>(), st);
+    CUDA_OK(cudaMemcpyAsync(mx, red.as<double>() + np, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    auto pow2_of = [](double m) { return (m > 0.0 && std::isfinite(m)) ? std::ldexp(1.0, std::ilogb(m)) : 1.0; };
+    const double sL = pow2_of(mx[0]), sR = pow2_of(mx[1]);
+    h->out_scale = sL * sR;
     std::vector<DevPackSeg> pl, pr;
     std::vector<DevChunk> cl, cr;
-    build_pack(H.s1.packA, h->g1, true, reinterpret_cast<uint64_t>(h->l_img.p), h->l_lo, ig.tile_bytes, 0, pl, cl);
-    build_pack(H.s4.packB, h->g4, false, reinterpret_cast<uint64_t>(h->r_img.p), h->r_lo, ig.tile_bytes, 1, pr, cr);
+    build_pack(H.s1.packA, h->g1, true, reinterpret_cast<uint64_t>(h->l_img.p), h->l_lo, ig.tile_bytes, 0, pl, cl,
+               1.0 / sL);
+    build_pack(H.s4.packB, h->g4, false, reinterpret_cast<uint64_t>(h->r_img.p), h->r_lo, ig.tile_bytes, 1, pr, cr,
+               1.0 / sR);
     DevMem dpl, dcl, dpr, dcr, tab;
     upload(dpl, pl, st);
     upload(dcl, cl, st);
@@ -916,6 +955,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         x.N = static_cast<int32_t>(H.s1.groups[g].N);
         x.nKt = h->g1.nKt[g];
         x.out_slot = 0;
+        x.scale = 1.0;
         for (int64_t r = 0; r < H.s1.groups[g].M; ++r) R1.push_back(xo + r * H.s1.groups[g].N);
         xo += H.s1.groups[g].M * H.s1.groups[g].N;
         G1.push_back(x);
@@ -938,6 +978,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         x.N = static_cast<int32_t>(H.s4.groups[g].N);
         x.nKt = h->g4.nKt[g];
         x.out_slot = 1 + i;
+        x.scale = h->out_scale;  // undoes the power-of-two scaling of L and R
         for (auto v : H.s4_rowoff[g]) R4.push_back(v);
         G4.push_back(x);
       }
@@ -1158,10 +1199,11 @@ int tnx_nrm2(const double* x, int64_t n, double* result, double* scratch, void* 
 }
 
 int tnx_lanczos_step(double* w, const double* v, const double* v_prev, double* v_next, int64_t n, double* alpha,
-                     double* beta, int32_t k, double tol, int32_t* done, double* scratch, void* stream) {
+                     double* beta, int32_t k, double tol, double tol_rel, int32_t* done, double* scratch,
+                     void* stream) {
   TNX_TRY({
-    launch_lanczos_step(w, v, k > 0 ? v_prev : nullptr, v_next, n, alpha + k, beta + k + 1, beta + k, tol, done,
-                        scratch, static_cast<cudaStream_t>(stream));
+    launch_lanczos_step(w, v, k > 0 ? v_prev : nullptr, v_next, n, alpha + k, beta + k + 1, beta + k, tol, tol_rel,
+                        done, scratch, static_cast<cudaStream_t>(stream));
     CUDA_OK(cudaGetLastError());
     return TNX_OK;
   })

@@ -62,6 +62,7 @@ struct DevPackSeg {
   int64_t lo_off;     // byte offset of the low-part image (BF16 split) from img_addr
   int32_t row0, k0, nKt, nlegs;
   int32_t src_slot, kcount;  // kcount: k extent of the block (product of contracted dims)
+  double scale;              // multiplies every packed value (an exact power of two)
   int32_t dims[kMaxLegsDev];
   int32_t rstr[kMaxLegsDev];
   int32_t kstr[kMaxLegsDev];
@@ -89,6 +90,7 @@ struct DevGroup {
   int64_t a_lo, b_lo;       // byte offsets of the low-part images (BF16 split)
   int64_t rowoff0;          // index of row 0 in the row-offset table
   int32_t M, N, nKt, out_slot;  // result rows go to out_tab[out_slot] + rowoff[.] + col
+  double scale;             // result = scale * sum_k A B (undoes operand range scaling)
 };
 
 struct DevTile {

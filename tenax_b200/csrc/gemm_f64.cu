@@ -114,8 +114,8 @@ __global__ void __launch_bounds__(THREADS) gemm_f64_kernel(const DevGroup* __res
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int col = tl.nt * BN + wn * 32 + j * 8 + (lane & 3) * 2;
-        if (col < g.N) out[ro + col] = acc[i][j][0];
-        if (col + 1 < g.N) out[ro + col + 1] = acc[i][j][1];
+        if (col < g.N) out[ro + col] = acc[i][j][0] * g.scale;
+        if (col + 1 < g.N) out[ro + col + 1] = acc[i][j][1] * g.scale;
       }
     }
     __syncthreads();

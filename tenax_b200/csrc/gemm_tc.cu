@@ -291,7 +291,8 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll 4
         for (int r = 0; r < 32; ++r) {
           const int64_t ro_r = __shfl_sync(0xffffffffu, ro, r);
-          if (ro_r >= 0 && col_ok) out[ro_r + col] = static_cast<OutT>(stg[r * kStagePitch + lane]);
+          if (ro_r >= 0 && col_ok)
+            out[ro_r + col] = static_cast<OutT>(static_cast<double>(stg[r * kStagePitch + lane]) * g.scale);
         }
         __syncwarp();
       }

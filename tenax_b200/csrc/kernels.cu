@@ -47,7 +47,7 @@ __global__ void pack_image_kernel(const uint64_t* __restrict__ src_tab, const De
       src_off += idx * stride;
       stride *= d;
     }
-    img_store(mode, img, s.lo_off, 0, s.nKt, s.row0 + rl, s.k0 + kl, src[src_off]);
+    img_store(mode, img, s.lo_off, 0, s.nKt, s.row0 + rl, s.k0 + kl, src[src_off] * s.scale);
   }
 }
 
@@ -234,6 +234,44 @@ __global__ void partial_dot_kernel(const double* __restrict__ x, const double* _
   if (threadIdx.x == 0) partials[blockIdx.x] = acc;
 }
 
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ double block_max(double v) {
+  __shared__ double wm[32];
+  v = warp_max(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) wm[w] = v;
+  __syncthreads();
+  v = (threadIdx.x < (blockDim.x >> 5)) ? wm[threadIdx.x] : 0.0;
+  if (w == 0) v = warp_max(v);
+  return v;
+}
+
+// max |x| in two passes (partials, then one block)
+__global__ void partial_maxabs_kernel(const double* __restrict__ x, int64_t n, double* __restrict__ partials) {
+  double m = 0.0;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += stride)
+    m = fmax(m, fabs(x[i]));
+  m = block_max(m);
+  if (threadIdx.x == 0) partials[blockIdx.x] = m;
+}
+
+__global__ void finish_max_kernel(const double* __restrict__ partials, int np, double* __restrict__ result) {
+  double m = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) m = fmax(m, partials[i]);
+  m = block_max(m);
+  if (threadIdx.x == 0) *result = m;
+}
+
+void launch_maxabs(const double* x, int64_t n, double* result, double* partials, cudaStream_t st) {
+  partial_maxabs_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(x, n, partials);
+  finish_max_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, result);
+}
+
 // final: result = sum partials (op 0), sqrt(sum) (op 1)
 __global__ void finish_sum_kernel(const double* __restrict__ partials, int np, double* __restrict__ result, int op,
                                   const int32_t* __restrict__ skip) {
@@ -270,8 +308,11 @@ __global__ void lanczos_axpy_kernel(double* __restrict__ w, const double* __rest
   if (threadIdx.x == 0) partials[blockIdx.x] = acc;
 }
 
+// beta = ||w||; stop when beta < tol (the reference's absolute test) or, with
+// an inexact matvec, when beta < tol_rel * |alpha| (below the matvec's noise)
 __global__ void lanczos_beta_kernel(const double* __restrict__ partials, int np, double* __restrict__ beta_out,
-                                    double tol, int32_t* __restrict__ done) {
+                                    const double* __restrict__ alpha, double tol, double tol_rel,
+                                    int32_t* __restrict__ done) {
   if (*done) return;
   double acc = 0.0;
   for (int i = threadIdx.x; i < np; i += blockDim.x) acc += partials[i];
@@ -279,7 +320,7 @@ __global__ void lanczos_beta_kernel(const double* __restrict__ partials, int np,
   if (threadIdx.x == 0) {
     double b = sqrt(acc);
     *beta_out = b;
-    if (b < tol) *done = 1;
+    if (b < tol || b < tol_rel * fabs(*alpha)) *done = 1;
   }
 }
 
@@ -295,13 +336,13 @@ __global__ void scale_into_kernel(const double* __restrict__ w, double* __restri
 }
 
 void launch_lanczos_step(double* w, const double* v, const double* vp, double* vnext, int64_t n, double* alpha,
-                         double* beta_next, const double* beta_prev, double tol, int32_t* done, double* partials,
-                         cudaStream_t st) {
+                         double* beta_next, const double* beta_prev, double tol, double tol_rel, int32_t* done,
+                         double* partials, cudaStream_t st) {
   // alpha = <v, w>
   partial_dot_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(v, w, n, 0, partials, done);
   finish_sum_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, alpha, 0, done);
   lanczos_axpy_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(w, v, vp, n, alpha, beta_prev, partials, done);
-  lanczos_beta_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, beta_next, tol, done);
+  lanczos_beta_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, beta_next, alpha, tol, tol_rel, done);
   if (vnext) scale_into_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(w, vnext, n, beta_next, 1, done);
 }
 

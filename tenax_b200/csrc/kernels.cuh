@@ -22,13 +22,15 @@ int mpo_points_per_cta();
 void launch_dot(const double* x, const double* y, int64_t n, int kind, double* result, double* partials,
                 const int32_t* skip, cudaStream_t st);
 void launch_lanczos_step(double* w, const double* v, const double* vp, double* vnext, int64_t n, double* alpha,
-                         double* beta_next, const double* beta_prev, double tol, int32_t* done, double* partials,
-                         cudaStream_t st);
+                         double* beta_next, const double* beta_prev, double tol, double tol_rel, int32_t* done,
+                         double* partials, cudaStream_t st);
 void launch_scale(const double* w, double* out, int64_t n, const double* s, int mode, const int32_t* skip,
                   cudaStream_t st);
 void launch_combine(const double* const* basis, const double* coefs, int nv, int64_t n, double* out,
                     cudaStream_t st);
 int reduce_partials_count();
+// *result = max |x_i| (partials: reduce_partials_count() doubles)
+void launch_maxabs(const double* x, int64_t n, double* result, double* partials, cudaStream_t st);
 
 // grouped GEMMs: out_tab[g.out_slot][rowoff[g.rowoff0 + row] + col] = sum_k A_g[row,k] B_g[col,k]
 void launch_gemm_f64(const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
