@@ -21,7 +21,10 @@ namespace tnx {
 namespace {
 constexpr int TBM = 128, TBN = 128;
 constexpr int TILE_BYTES = 16384;
-constexpr int THREADS = 192;
+// epilogue warps: one per TMEM lane quarter (8, two per quarter, measured
+// slower on the operand-traffic-bound stage-1 GEMM: 3.55 vs 2.84 ms)
+constexpr int EPI_WARPS = 4;
+constexpr int THREADS = 64 + 32 * EPI_WARPS;
 constexpr int TMEM_COLS = 2 * TBN;
 constexpr uint64_t kTimeoutNs = 2000000000ull;  // 2 s per wait
 
@@ -99,7 +102,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 }
 
 constexpr int kStagePitch = 33;  // fp32 words per staged row (+1 breaks bank conflicts)
-constexpr int kEpiStageBytes = 4 * 32 * kStagePitch * 4;
+constexpr int kEpiStageBytes = EPI_WARPS * 32 * kStagePitch * 4;
 
 template <bool TF32, typename OutT>
 __global__ void __launch_bounds__(THREADS, 1)
@@ -132,7 +135,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(&tfull[a], 1);
-      mbar_init(&tempty[a], 128);
+      mbar_init(&tempty[a], 32 * EPI_WARPS);
     }
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -264,7 +267,10 @@ __global__ void __launch_bounds__(THREADS, 1)
     // ------------------------------------------------------------ epilogue
     const int q = warp & 3;  // TMEM lane quarter this warp may access
     const int r_in_tile = q * 32 + lane;
-    float* stg = epi_stage + (warp - 2) * 32 * kStagePitch;
+    const int e = warp - 2;  // epilogue warp 0..EPI_WARPS-1
+    constexpr int kColsPerWarp = TBN / (EPI_WARPS / 4);
+    const int c_begin = (e / 4) * kColsPerWarp;
+    float* stg = epi_stage + e * 32 * kStagePitch;
     int acc = 0;
     uint32_t aph = 0;
     for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
@@ -280,7 +286,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       // Each lane holds one row; stage 32x32 chunks through shared memory so
       // that every store instruction writes 32 consecutive columns of one row.
 #pragma unroll 1
-      for (int c0 = 0; c0 < TBN; c0 += 32) {
+      for (int c0 = c_begin; c0 < c_begin + kColsPerWarp; c0 += 32) {
         uint32_t v[32];
         tmem_ld32(tbase + c0, v);
 #pragma unroll

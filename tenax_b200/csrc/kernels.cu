@@ -1,5 +1,7 @@
 // HBM-bound kernels: operand-image packing, result scatter, the fused MPO
 // application of the two-site H_eff, and FP64 vector primitives.
+#include <type_traits>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -117,11 +119,33 @@ void launch_zero_ranges(const uint64_t* out_tab, const DevChunk* chunks, int n_c
 constexpr int kMpoThreads = 256;
 constexpr int kMpoLoads = 8;
 
-template <typename TI>
+// compile-time image store: FP64 tiles store the double; the mixed images
+// take an FP32 value (native fp32 -> bf16 / tf32 conversions)
+template <int MODE, typename AccT>
+__device__ __forceinline__ void img_store_t(uint8_t* img, int64_t lo_offset, int nKt, int64_t row, int64_t k, AccT v) {
+  const int64_t off = img_byte_offset(MODE, 0, nKt, row, k);
+  if constexpr (MODE == IMG_F64) {
+    *reinterpret_cast<double*>(img + off) = static_cast<double>(v);
+  } else if constexpr (MODE == IMG_BF16) {
+    const float f = static_cast<float>(v);
+    const __nv_bfloat16 hi = __float2bfloat16_rn(f);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(f - __bfloat162float(hi));
+    *reinterpret_cast<__nv_bfloat16*>(img + off) = hi;
+    *reinterpret_cast<__nv_bfloat16*>(img + lo_offset + off) = lo;
+  } else {
+    uint32_t t;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(static_cast<float>(v)));
+    *reinterpret_cast<uint32_t*>(img + off) = t;
+  }
+}
+
+template <typename TI, int MODE>
 __global__ void __launch_bounds__(kMpoThreads) mpo_apply_kernel(
-    int mode, const DevMpoPair* __restrict__ pairs, const DevMpoSlot* __restrict__ islots,
+    const DevMpoPair* __restrict__ pairs, const DevMpoSlot* __restrict__ islots,
     const DevMpoOutSlot* __restrict__ oslots, const DevMpoTerm* __restrict__ terms,
     const int2* __restrict__ chunks, const int32_t* __restrict__ skip) {
+  // FP64 images accumulate in double; the FP32-input mixed paths in float
+  using AccT = typename std::conditional<MODE == IMG_F64, double, float>::type;
   if (skip && *skip) return;
   extern __shared__ __align__(16) unsigned char mpo_smem[];
   const int2 ch = chunks[blockIdx.x];
@@ -138,7 +162,7 @@ __global__ void __launch_bounds__(kMpoThreads) mpo_apply_kernel(
   if (p >= npts || pr.n_terms == 0) return;
   const int64_t c = p / pr.md;
   const int d = p - static_cast<int>(c) * pr.md;
-  double acc = 0.0;
+  AccT acc = AccT(0);
   int cur = st[0].out_slot;
   for (int t0 = 0; t0 < pr.n_terms; t0 += kMpoLoads) {
     TI xv[kMpoLoads];
@@ -156,19 +180,17 @@ __global__ void __launch_bounds__(kMpoThreads) mpo_apply_kernel(
       const DevMpoTerm tm = st[t0 + u];
       if (tm.out_slot != cur) {
         const DevMpoOutSlot o = so[cur];
-        img_store(mode, reinterpret_cast<uint8_t*>(o.img_addr), o.lo_off, 0, o.nKt,
-                  o.row0 + c * o.rows_per_c + o.row_add, o.k0 + o.k_add + d, acc);
+        img_store_t<MODE>(reinterpret_cast<uint8_t*>(o.img_addr), o.lo_off, o.nKt,
+                          o.row0 + c * o.rows_per_c + o.row_add, o.k0 + o.k_add + d, acc);
         cur = tm.out_slot;
-        acc = 0.0;
+        acc = AccT(0);
       }
-      acc += tm.w * static_cast<double>(xv[u]);
+      acc += static_cast<AccT>(tm.w) * static_cast<AccT>(xv[u]);
     }
   }
-  if (pr.n_terms > 0) {
-    const DevMpoOutSlot o = so[cur];
-    img_store(mode, reinterpret_cast<uint8_t*>(o.img_addr), o.lo_off, 0, o.nKt, o.row0 + c * o.rows_per_c + o.row_add,
-              o.k0 + o.k_add + d, acc);
-  }
+  const DevMpoOutSlot o = so[cur];
+  img_store_t<MODE>(reinterpret_cast<uint8_t*>(o.img_addr), o.lo_off, o.nKt, o.row0 + c * o.rows_per_c + o.row_add,
+                    o.k0 + o.k_add + d, acc);
 }
 
 void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevMpoSlot* islots,
@@ -176,13 +198,16 @@ void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevM
                       size_t smem_bytes, const int32_t* skip, cudaStream_t st) {
   if (n_chunks <= 0) return;
   const int smem = static_cast<int>(smem_bytes);
-  if (x1_f32) {
-    cudaFuncSetAttribute(mpo_apply_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    mpo_apply_kernel<float><<<n_chunks, kMpoThreads, smem, st>>>(mode, pairs, islots, oslots, terms, chunks, skip);
-  } else {
-    cudaFuncSetAttribute(mpo_apply_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    mpo_apply_kernel<double><<<n_chunks, kMpoThreads, smem, st>>>(mode, pairs, islots, oslots, terms, chunks, skip);
-  }
+  auto go = [&](auto kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    kernel<<<n_chunks, kMpoThreads, smem, st>>>(pairs, islots, oslots, terms, chunks, skip);
+  };
+  if (!x1_f32)
+    go(mpo_apply_kernel<double, IMG_F64>);
+  else if (mode == IMG_BF16)
+    go(mpo_apply_kernel<float, IMG_BF16>);
+  else
+    go(mpo_apply_kernel<float, IMG_TF32>);
 }
 
 int mpo_points_per_cta() { return kMpoThreads; }
