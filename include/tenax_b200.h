@@ -152,6 +152,21 @@ int64_t tnx_reduce_scratch_len(void);
 int tnx_dot(const double* x, const double* y, int64_t n, double* result, double* scratch, void* stream);
 int tnx_nrm2(const double* x, int64_t n, double* result, double* scratch, void* stream);
 
+/* Max-abs renormalisation of the CTM environment (tenax
+ * algorithms/ipeps.py:1133-1149, _renormalize_env) for 1..8 tensors per call:
+ *   y_t = x_t / (max|x_t| + eps),  stat[t] = max|x_t|  (device memory).
+ * The adjoint maps gy_t = dL/dy_t to gx_t = dL/dx_t with the derivative of
+ * the max split evenly among the entries attaining it (JAX's rule for
+ * jnp.max): gx = gy/(m+eps) - <gy,x>/(m+eps)^2 * sign(x) [|x| == m] / count.
+ * `stat` is the forward's.  x/y/gy/gx/n are HOST arrays of n_tensors device
+ * pointers / sizes; `scratch` holds tnx_renorm_scratch_len() doubles.
+ * y must not alias x; gx must not alias x or gy. */
+int64_t tnx_renorm_scratch_len(void);
+int tnx_renorm_maxabs(int n_tensors, const double* const* x, double* const* y, const int64_t* n, double eps,
+                      double* stat, double* scratch, void* stream);
+int tnx_renorm_maxabs_adjoint(int n_tensors, const double* const* x, const double* const* gy, double* const* gx,
+                              const int64_t* n, double eps, const double* stat, double* scratch, void* stream);
+
 /* One Lanczos orthogonalisation step (dmrg.py:1005-1019) on device:
  *   alpha[k] = <v, w>;  w -= alpha[k] v  (- beta[k] v_prev if k > 0);
  *   beta[k+1] = ||w||;  if beta[k+1] < tol or beta[k+1] < tol_rel*|alpha[k]|: *done = 1

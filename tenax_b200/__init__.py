@@ -1,9 +1,10 @@
 """tenax_b200: B200-native block-sparse symmetric contraction for tenax.
 
 Drop-in GPU path for tenax's ``SymmetricTensor`` contraction and the
-two-site DMRG H_eff matvec built on it: the same names and argument
-meanings as ``tenax.contract``, ``SymmetricTensor``/``TensorIndex`` and
-``dmrg()``; arithmetic runs in this package's sm_100a kernels through the C
+two-site DMRG H_eff matvec built on it, and the dense CTMRG step with a
+hand-written adjoint: the same names and argument meanings as
+``tenax.contract``, ``SymmetricTensor``/``TensorIndex``, ``dmrg()`` and
+``ctm()``/``compute_energy_ctm()``; arithmetic runs in this package's sm_100a kernels through the C
 ABI in ``include/tenax_b200.h``.
 """
 
@@ -23,6 +24,7 @@ from tenax_b200.contraction import (  # noqa: F401
     contract_with_subscripts,
 )
 from tenax_b200.heff import HeffBatch, HeffOperator  # noqa: F401
+from tenax_b200.ipeps import CTMConfig, CTMEnvironment, compute_energy_ctm, ctm  # noqa: F401
 
 EPS = 1e-15
 LOG_EPS = 1e-250

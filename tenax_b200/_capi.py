@@ -50,7 +50,7 @@ class TensorDesc(C.Structure):
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f"{LIB_PATH} is missing: build it with `python -m tenax_b200.build` "
+            f"{LIB_PATH} is missing: build it with `python tenax_b200/build.py` "
             "(the package has no CPU fallback)"
         )
     lib = C.CDLL(LIB_PATH)
@@ -87,6 +87,9 @@ def _load():
         "tnx_lanczos_step": (C.c_int, [P, P, P, P, i64, P, P, i32, dbl, dbl, P, P, P]),
         "tnx_combine": (C.c_int, [P, P, i32, i64, P, P]),
         "tnx_scale": (C.c_int, [P, P, i64, P, i32, P]),
+        "tnx_renorm_scratch_len": (i64, []),
+        "tnx_renorm_maxabs": (C.c_int, [C.c_int, P, P, P, dbl, P, P, P]),
+        "tnx_renorm_maxabs_adjoint": (C.c_int, [C.c_int, P, P, P, P, dbl, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -104,7 +107,8 @@ EXPORTED = [
     "tnx_heff_batch_create", "tnx_heff_batch_apply", "tnx_heff_batch_apply_stage", "tnx_heff_stage_flops",
     "tnx_heff_batch_launches", "tnx_heff_batch_error",
     "tnx_heff_batch_set_skip_flag", "tnx_heff_batch_destroy", "tnx_reduce_scratch_len", "tnx_dot", "tnx_nrm2",
-    "tnx_lanczos_step", "tnx_combine", "tnx_scale",
+    "tnx_lanczos_step", "tnx_combine", "tnx_scale", "tnx_renorm_scratch_len", "tnx_renorm_maxabs",
+    "tnx_renorm_maxabs_adjoint",
 ]
 
 

@@ -1,6 +1,6 @@
 """Build the in-tree CUDA library ``tenax_b200/libtenax_b200.so`` for sm_100a.
 
-    python -m tenax_b200.build            # or: python tenax_b200/build.py
+    python tenax_b200/build.py   # imports nothing from the package
 
 nvcc cross-compiles without a GPU; the resulting shared object travels with
 the source tree.  Rebuilds only when a source is newer than the library.

@@ -100,7 +100,7 @@ struct PtrTab {
 
 TensorStruct parse_desc(const tnx_tensor_desc* d, const char* default_subs) {
   if (!d) throw PlanError{TNX_ERR_VALUE, "null tensor descriptor"};
-  if (d->n_legs < 0 || d->n_legs > kMaxLegs) throw PlanError{TNX_ERR_UNSUPPORTED, "at most 8 legs per tensor"};
+  if (d->n_legs < 0 || d->n_legs > kMaxLegs) throw PlanError{TNX_ERR_UNSUPPORTED, "at most " + std::to_string(kMaxLegs) + " legs per tensor"};
   TensorStruct t;
   t.nl = d->n_legs;
   if (d->subs)
@@ -1185,6 +1185,49 @@ int64_t tnx_reduce_scratch_len(void) { return reduce_partials_count(); }
 int tnx_dot(const double* x, const double* y, int64_t n, double* result, double* scratch, void* stream) {
   TNX_TRY({
     launch_dot(x, y, n, 0, result, scratch, nullptr, static_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
+
+int64_t tnx_renorm_scratch_len(void) { return 2 * kRenormMax * kRenormBlocks; }
+
+static int renorm_args(int n_tensors, const double* const* x, const double* const* g, double* const* y,
+                       const int64_t* n, RenormArgs& a) {
+  if (n_tensors < 1 || n_tensors > kRenormMax) {
+    return set_err(TNX_ERR_VALUE, "renormalisation takes between 1 and " + std::to_string(kRenormMax) +
+                                      " tensors per call, got " + std::to_string(n_tensors));
+  }
+  a = RenormArgs{};
+  for (int t = 0; t < n_tensors; ++t) {
+    if (n[t] < 0) return set_err(TNX_ERR_VALUE, "renormalisation: negative tensor size");
+    a.x[t] = x[t];
+    a.g[t] = g ? g[t] : nullptr;
+    a.y[t] = y[t];
+    a.n[t] = n[t];
+  }
+  return TNX_OK;
+}
+
+int tnx_renorm_maxabs(int n_tensors, const double* const* x, double* const* y, const int64_t* n, double eps,
+                      double* stat, double* scratch, void* stream) {
+  TNX_TRY({
+    RenormArgs a;
+    int rc = renorm_args(n_tensors, x, nullptr, y, n, a);
+    if (rc != TNX_OK) return rc;
+    launch_renorm(a, n_tensors, eps, stat, scratch, static_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
+
+int tnx_renorm_maxabs_adjoint(int n_tensors, const double* const* x, const double* const* gy, double* const* gx,
+                              const int64_t* n, double eps, const double* stat, double* scratch, void* stream) {
+  TNX_TRY({
+    RenormArgs a;
+    int rc = renorm_args(n_tensors, x, gy, gx, n, a);
+    if (rc != TNX_OK) return rc;
+    launch_renorm_adjoint(a, n_tensors, eps, stat, scratch, static_cast<cudaStream_t>(stream));
     CUDA_OK(cudaGetLastError());
     return TNX_OK;
   })

@@ -54,7 +54,7 @@ __host__ __device__ inline int64_t img_byte_offset(int mode, int64_t tile0, int 
 // ---------------------------------------------------------------------------
 // device tables
 // ---------------------------------------------------------------------------
-constexpr int kMaxLegsDev = 8;
+constexpr int kMaxLegsDev = 12;  // equals kMaxLegs of the planner
 
 struct DevPackSeg {
   int64_t src_off;    // element offset of the block in operand buffer src_tab[src_slot]

@@ -394,4 +394,108 @@ void launch_combine(const double* const* basis, const double* coefs, int nv, int
 
 int reduce_partials_count() { return kRedBlocks; }
 
+// ---------------------------------------------------------------------------
+// Max-abs renormalisation of a batch of tensors and its adjoint.
+// Forward: y_t = x_t / (m_t + eps), m_t = max |x_t|.
+// Adjoint: gx_t = gy_t / (m_t + eps) - <gy_t, x_t> / (m_t + eps)^2 * dm_t/dx_t,
+// where dm/dx puts sign(x_i) / c on each of the c entries with |x_i| == m.
+// Grid (kRenormBlocks, n_tensors); each tensor's reduction is a fixed-order
+// two-pass sum, so results do not depend on scheduling.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int64_t renorm_stride() { return static_cast<int64_t>(kRenormBlocks) * blockDim.x; }
+
+__global__ void renorm_max_partial_kernel(RenormArgs a, double* __restrict__ partials) {
+  const int t = blockIdx.y;
+  const double* __restrict__ x = a.x[t];
+  const int64_t n = a.n[t];
+  double m = 0.0;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += renorm_stride())
+    m = fmax(m, fabs(x[i]));
+  m = block_max(m);
+  if (threadIdx.x == 0) partials[t * kRenormBlocks + blockIdx.x] = m;
+}
+
+// per-tensor total of kRenormBlocks partials in a fixed order (warp 0), broadcast via smem
+__device__ __forceinline__ double renorm_total(const double* __restrict__ p, bool is_max) {
+  __shared__ double tot;
+  if (threadIdx.x < 32) {
+    double v0 = p[threadIdx.x], v1 = p[threadIdx.x + 32];
+    double v = is_max ? fmax(v0, v1) : v0 + v1;
+    v = is_max ? warp_max(v) : warp_sum(v);
+    if (threadIdx.x == 0) tot = v;
+  }
+  __syncthreads();
+  const double r = tot;
+  __syncthreads();
+  return r;
+}
+
+__global__ void renorm_apply_kernel(RenormArgs a, const double* __restrict__ partials, double eps,
+                                    double* __restrict__ stat) {
+  const int t = blockIdx.y;
+  const double m = renorm_total(partials + t * kRenormBlocks, true);
+  if (blockIdx.x == 0 && threadIdx.x == 0) stat[t] = m;
+  const double inv = 1.0 / (m + eps);
+  const double* __restrict__ x = a.x[t];
+  double* __restrict__ y = a.y[t];
+  const int64_t n = a.n[t];
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += renorm_stride())
+    y[i] = x[i] * inv;
+}
+
+__global__ void renorm_adj_partial_kernel(RenormArgs a, const double* __restrict__ stat,
+                                          double* __restrict__ partials) {
+  const int t = blockIdx.y;
+  const double* __restrict__ x = a.x[t];
+  const double* __restrict__ g = a.g[t];
+  const int64_t n = a.n[t];
+  const double m = stat[t];
+  double dot = 0.0, cnt = 0.0;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += renorm_stride()) {
+    const double xi = x[i];
+    dot += g[i] * xi;
+    cnt += fabs(xi) == m ? 1.0 : 0.0;
+  }
+  dot = block_sum(dot);
+  __syncthreads();
+  cnt = block_sum(cnt);
+  if (threadIdx.x == 0) {
+    partials[(2 * t) * kRenormBlocks + blockIdx.x] = dot;
+    partials[(2 * t + 1) * kRenormBlocks + blockIdx.x] = cnt;
+  }
+}
+
+__global__ void renorm_adj_apply_kernel(RenormArgs a, const double* __restrict__ stat,
+                                        const double* __restrict__ partials, double eps) {
+  const int t = blockIdx.y;
+  const double dot = renorm_total(partials + (2 * t) * kRenormBlocks, false);
+  const double cnt = renorm_total(partials + (2 * t + 1) * kRenormBlocks, false);
+  const double m = stat[t];
+  const double inv = 1.0 / (m + eps);
+  const double w = cnt > 0.0 ? dot * inv * inv / cnt : 0.0;
+  const double* __restrict__ x = a.x[t];
+  const double* __restrict__ g = a.g[t];
+  double* __restrict__ gx = a.y[t];
+  const int64_t n = a.n[t];
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += renorm_stride()) {
+    const double xi = x[i];
+    double v = g[i] * inv;
+    if (fabs(xi) == m && xi != 0.0) v -= xi > 0.0 ? w : -w;
+    gx[i] = v;
+  }
+}
+
+void launch_renorm(const RenormArgs& a, int nt, double eps, double* stat, double* partials, cudaStream_t st) {
+  const dim3 grid(kRenormBlocks, nt);
+  renorm_max_partial_kernel<<<grid, kRedThreads, 0, st>>>(a, partials);
+  renorm_apply_kernel<<<grid, kRedThreads, 0, st>>>(a, partials, eps, stat);
+}
+
+void launch_renorm_adjoint(const RenormArgs& a, int nt, double eps, const double* stat, double* partials,
+                           cudaStream_t st) {
+  const dim3 grid(kRenormBlocks, nt);
+  renorm_adj_partial_kernel<<<grid, kRedThreads, 0, st>>>(a, stat, partials);
+  renorm_adj_apply_kernel<<<grid, kRedThreads, 0, st>>>(a, stat, partials, eps);
+}
+
 }  // namespace tnx

@@ -32,6 +32,20 @@ int reduce_partials_count();
 // *result = max |x_i| (partials: reduce_partials_count() doubles)
 void launch_maxabs(const double* x, int64_t n, double* result, double* partials, cudaStream_t st);
 
+// batched max-abs renormalisation (forward: x -> y; adjoint: g = dL/dy, y <- dL/dx)
+constexpr int kRenormMax = 8;
+constexpr int kRenormBlocks = 64;  // per tensor; the per-tensor totals assume exactly 64
+struct RenormArgs {
+  const double* x[kRenormMax];
+  const double* g[kRenormMax];
+  double* y[kRenormMax];
+  int64_t n[kRenormMax];
+};
+// partials: 2 * kRenormMax * kRenormBlocks doubles
+void launch_renorm(const RenormArgs& a, int nt, double eps, double* stat, double* partials, cudaStream_t st);
+void launch_renorm_adjoint(const RenormArgs& a, int nt, double eps, const double* stat, double* partials,
+                           cudaStream_t st);
+
 // grouped GEMMs: out_tab[g.out_slot][rowoff[g.rowoff0 + row] + col] = sum_k A_g[row,k] B_g[col,k]
 void launch_gemm_f64(const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
                      const uint64_t* out_tab, const int32_t* skip, cudaStream_t st);

@@ -192,6 +192,9 @@ PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::stri
   // output legs map to A-free or B-free
   if (out_subs.size() != a_free.size() + b_free.size())
     throw PlanError{1, "output subscripts must list every free index exactly once"};
+  if (static_cast<int>(out_subs.size()) > kMaxLegs)
+    throw PlanError{6, "contraction result has " + std::to_string(out_subs.size()) + " legs; at most " +
+                           std::to_string(kMaxLegs) + " are supported"};
   struct OutLeg {
     bool from_a;
     int pos;  // leg position in A or B

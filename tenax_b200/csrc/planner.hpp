@@ -13,7 +13,7 @@
 
 namespace tnx {
 
-constexpr int kMaxLegs = 8;
+constexpr int kMaxLegs = 12;  // legs per tensor (operands, intermediates and outputs)
 
 using Key = std::vector<int32_t>;
 

@@ -12,7 +12,8 @@ What is emulated:
   * ``jax.random``: a deterministic key -> numpy Generator mapping
     (values differ from real JAX; fixtures store the generated inputs).
   * ``jax.tree_util.register_pytree_node_class``, ``jax.jit``,
-    ``jax.lax.stop_gradient``: identity.
+    ``jax.lax.stop_gradient``: identity (optionally recording its argument,
+    see ``record_stop_gradient``).
   * ``jax.lax.while_loop / fori_loop / cond / scan``: eager Python loops.
   * ``opt_einsum.contract_expression / contract / contract_path``:
     ``np.einsum`` with a path computed once per expression.
@@ -103,11 +104,28 @@ def _array(x, dtype=None, copy=True):
     return np.array(x, dtype=dtype).view(_JArr)
 
 
+_SG_LOG = None
+
+
+def record_stop_gradient(log) -> None:
+    """Append a copy of every array passed to ``jax.lax.stop_gradient`` to
+    ``log`` (a list), or stop recording when ``log`` is None.  The CTM moves
+    of algorithms/ipeps.py pass exactly their projectors through it."""
+    global _SG_LOG
+    _SG_LOG = log
+
+
 def install() -> None:
     """Register the stand-in modules in ``sys.modules``."""
     jnp = _NumpyModule("jax.numpy", np)
     jnp.array = _array
     jnp.asarray = _array
+
+    def einsum(subscripts, *operands, optimize=True, **kwargs):
+        # jnp.einsum contracts pairwise along an optimised path by default
+        return _wrap(np.einsum(subscripts, *operands, optimize=optimize, **kwargs))
+
+    jnp.einsum = einsum
     jnp.float64 = np.float64
     jnp.float32 = np.float32
     jnp.complex128 = np.complex128
@@ -149,7 +167,12 @@ def install() -> None:
     jax.core = core
 
     lax = types.ModuleType("jax.lax")
-    lax.stop_gradient = lambda x: x
+    def stop_gradient(x):
+        if _SG_LOG is not None:
+            _SG_LOG.append(np.array(x, dtype=np.float64, copy=True))
+        return x
+
+    lax.stop_gradient = stop_gradient
 
     def while_loop(cond_fun, body_fun, init_val):
         val = init_val
@@ -259,6 +282,13 @@ def load_reference(src_root: str, modules: list[str]) -> dict[str, types.ModuleT
         m = types.ModuleType(p)
         m.__path__ = [os.path.join(src_root, *p.split("."))]
         sys.modules[p] = m
+    core_pkg = sys.modules["tenax.core"]
+    if not hasattr(core_pkg, "EPS"):
+        # tenax/core/__init__.py only re-exports the core modules and defines
+        # the EPS constants that algorithms/ipeps.py imports from it.
+        path = os.path.join(src_root, "tenax", "core", "__init__.py")
+        with open(path) as fh:
+            exec(compile(fh.read(), path, "exec"), core_pkg.__dict__)
     out = {}
     for name in modules:
         out[name] = importlib.import_module(name)

@@ -306,6 +306,62 @@ def cylinder_bonds(Lx, Ly):
     return bonds
 
 
+def gen_ctm(M):
+    """Dense 1-site CTMRG (algorithms/ipeps.py): environments, corner
+    singular values and NN Heisenberg energies from the reference's own
+    ``ctm`` / ``compute_energy_ctm``.
+
+    The reference's CTM on random site tensors does not converge: its
+    truncation keeps a subspace whose edge is re-chosen every sweep, and a
+    1e-14 change of A moves the 30-sweep energy by ~1e-2.  So the small cases
+    also store every projector the reference computed (recorded at its
+    ``jax.lax.stop_gradient`` call); replaying them makes the rest of the
+    computation a smooth function that other implementations must match to
+    rounding.  The D=4, chi=80, 30-sweep QR case stores the free-running
+    energy and corner spectra only (a statistical reference)."""
+    ip = M["tenax.algorithms.ipeps"]
+    sz = np.array([[0.5, 0.0], [0.0, -0.5]])
+    sp = np.array([[0.0, 1.0], [0.0, 0.0]])
+    H = (np.kron(sz, sz) + 0.5 * np.kron(sp, sp.T) + 0.5 * np.kron(sp.T, sp)).reshape(2, 2, 2, 2)
+    cases = [
+        ("qr_small", 2, 6, 6, "qr", 0, 11),
+        ("eigh_small", 2, 5, 4, "eigh", 0, 12),
+        ("qr_mid", 3, 16, 6, "qr", 0, 13),
+        ("qr_warm", 2, 6, 5, "qr", 2, 14),
+        ("c4", 4, 80, 30, "qr", 0, 2024),
+    ]
+    arrays = {"H": H}
+    meta = {}
+    for name, D, chi, iters, method, warm, seed in cases:
+        rng = np.random.default_rng(seed)
+        A = rng.standard_normal((D, D, D, D, 2)) / np.sqrt(2.0 * D ** 4)
+        cfg = ip.CTMConfig(chi=chi, max_iter=iters, conv_tol=0.0, renormalize=True,
+                           projector_method=method, qr_warmup_steps=warm)
+        t0 = time.time()
+        log: list = []
+        _jax_standin.record_stop_gradient(log)
+        env = ip.ctm(A, cfg)
+        _jax_standin.record_stop_gradient(None)
+        E = float(ip.compute_energy_ctm(A, env, H, 2))
+        assert len(log) == 4 * iters, (name, len(log))
+        arrays[f"{name}.A"] = A
+        if name != "c4":
+            for i, P in enumerate(log):
+                arrays[f"{name}.P{i}"] = P
+        for nm, x in zip(("C1", "C2", "C3", "C4", "T1", "T2", "T3", "T4"), env):
+            x = np.asarray(x, dtype=np.float64)
+            if name != "c4":
+                arrays[f"{name}.{nm}"] = x
+            if nm.startswith("C"):
+                arrays[f"{name}.sv_{nm}"] = np.linalg.svd(x, compute_uv=False)
+        meta[name] = {"D": D, "chi": chi, "iters": iters, "method": method, "warmup": warm, "seed": seed,
+                      "energy": E}
+        print(f"ctm {name}: E={E:.15f} ({time.time() - t0:.1f} s)", flush=True)
+    np.savez_compressed(os.path.join(HERE, "ctm.npz"), **arrays)
+    with open(os.path.join(HERE, "ctm.json"), "w") as fh:
+        json.dump(meta, fh, indent=1)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference/src")
@@ -314,10 +370,10 @@ def main():
     mods = _jax_standin.load_reference(args.ref, [
         "tenax.core.symmetry", "tenax.core.index", "tenax.core.tensor", "tenax.linalg",
         "tenax.contraction.contractor", "tenax.network.network", "tenax.algorithms._tensor_utils",
-        "tenax.algorithms.auto_mpo", "tenax.algorithms.dmrg",
+        "tenax.algorithms.auto_mpo", "tenax.algorithms.dmrg", "tenax.algorithms.ipeps",
     ])
     mods["cfg"] = mods["tenax.algorithms.dmrg"].DMRGConfig
-    todo = args.only.split(",") if args.only else ["valid", "contract", "pieces", "mpo", "c1"]
+    todo = args.only.split(",") if args.only else ["valid", "contract", "pieces", "mpo", "c1", "ctm"]
     if "valid" in todo:
         gen_valid_blocks(mods)
     if "contract" in todo:
@@ -328,6 +384,8 @@ def main():
         gen_mpo(mods)
     if "c1" in todo:
         gen_dmrg_c1(mods)
+    if "ctm" in todo:
+        gen_ctm(mods)
 
 
 if __name__ == "__main__":
