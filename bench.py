@@ -426,7 +426,7 @@ def main():
     ap.add_argument("--cyl-lx", type=int, default=4)
     ap.add_argument("--dmrg-precisions", default="fp64,bf16x3,tf32")
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "tf32"])

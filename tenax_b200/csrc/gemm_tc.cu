@@ -21,9 +21,14 @@ namespace tnx {
 namespace {
 constexpr int TBM = 128, TBN = 128;
 constexpr int TILE_BYTES = 16384;
-// epilogue warps: one per TMEM lane quarter (8, two per quarter, measured
-// slower on the operand-traffic-bound stage-1 GEMM: 3.55 vs 2.84 ms)
-constexpr int EPI_WARPS = 4;
+// epilogue warps: 4 (one per TMEM lane quarter) or 8 (two per quarter,
+// splitting the columns).  Short-K sector GEMMs are epilogue-bound: on the
+// 64-problem H_eff batch stage 1 takes 2.21 ms with 8 warps, 2.96 ms with 4.
+#ifndef TNX_EPI_WARPS
+#define TNX_EPI_WARPS 8
+#endif
+constexpr int EPI_WARPS = TNX_EPI_WARPS;
+static_assert(EPI_WARPS == 4 || EPI_WARPS == 8, "epilogue warps: 4 or 8");
 constexpr int THREADS = 64 + 32 * EPI_WARPS;
 constexpr int TMEM_COLS = 2 * TBN;
 constexpr uint64_t kTimeoutNs = 2000000000ull;  // 2 s per wait
@@ -283,6 +288,10 @@ __global__ void __launch_bounds__(THREADS, 1)
       const int64_t ro = row < g.M ? rowoff[g.rowoff0 + row] : -1;
       OutT* out = reinterpret_cast<OutT*>(out_tab[g.out_slot]);
       const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * TBN);
+      // group scales are powers of two, so the multiply is exact in the
+      // output's own precision (FP32 outputs only ever carry scale 1; a
+      // per-element FP64 round trip there doubled the epilogue's cost)
+      const OutT scale = static_cast<OutT>(g.scale);
       // Each lane holds one row; stage 32x32 chunks through shared memory so
       // that every store instruction writes 32 consecutive columns of one row.
 #pragma unroll 1
@@ -298,7 +307,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         for (int r = 0; r < 32; ++r) {
           const int64_t ro_r = __shfl_sync(0xffffffffu, ro, r);
           if (ro_r >= 0 && col_ok)
-            out[ro_r + col] = static_cast<OutT>(static_cast<double>(stg[r * kStagePitch + lane]) * g.scale);
+            out[ro_r + col] = static_cast<OutT>(stg[r * kStagePitch + lane]) * scale;
         }
         __syncwarp();
       }
