@@ -381,12 +381,15 @@ def run_dmrg_study(args):
     Lx, Ly = args.cyl_lx, 6
     mpo = cylinder_mpo(Lx, Ly)
     out = {"study": "two-site DMRG, width-6 Heisenberg cylinder (U(1), J=1)", "sites": Lx * Ly, "chi": args.chi,
-           "sweeps": args.sweeps, "lanczos_max_iter": args.lanczos, "data": "seeded random initial MPS", "runs": {}}
+           "sweeps": args.sweeps, "lanczos_max_iter": args.lanczos, "data": "seeded random initial MPS",
+           "svd": {"driver": args.svd_driver, "streams": args.svd_streams}, "runs": {}}
     fp64_e = None
     for prec in args.dmrg_precisions.split(","):
         mps = random_symmetric_mps(Lx * Ly, args.chi, seed=args.seed)
         cfg = DMRGConfig(max_bond_dim=args.chi, num_sweeps=args.sweeps, lanczos_max_iter=args.lanczos,
-                         convergence_tol=0.0, precision=prec, check_matvec_residual=prec != "fp64")
+                         convergence_tol=0.0, precision=prec, check_matvec_residual=prec != "fp64",
+                         svd_driver=None if args.svd_driver == "default" else args.svd_driver,
+                         svd_streams=args.svd_streams)
         stats: list = []
         phases: dict = {}
         res = dmrg(mpo, mps, cfg, stats, phases)
@@ -417,6 +420,97 @@ def run_dmrg_study(args):
     print(json.dumps(out), flush=True)
 
 
+def run_ctm_study(args):
+    """Dense 1-site CTMRG (D=4, d=2, chi=80, 30 QR sweeps, square-lattice
+    Heisenberg NN energy): forward and forward+gradient seconds on the GPU,
+    the hand-written adjoint checked against central differences of the
+    fixed-projector energy (h=1e-6, 20 random directions), the free-running
+    energy, and the oracle's CPU forward (the reference's einsum order) on
+    the same site tensor as the CPU baseline.  With --ctm-oracle-grad the
+    oracle's torch-autograd gradient under the GPU's projectors is compared
+    too (tens of seconds of CPU)."""
+    import time
+
+    import torch
+
+    from tenax_b200.ipeps import CTMConfig, compute_energy_ctm, ctm, energy_and_grad, heisenberg_gate
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    D, d, chi, iters = 4, 2, args.ctm_chi, args.ctm_iters
+    rng = np.random.default_rng(args.ctm_seed)
+    A_host = rng.standard_normal((D, D, D, D, d)) / np.sqrt(2.0 * D ** 4)
+    A = torch.from_numpy(A_host).cuda()
+    H = heisenberg_gate()
+    cfg = CTMConfig(chi=chi, max_iter=iters, conv_tol=0.0, projector_method="qr", qr_warmup_steps=0)
+
+    def timed(fn, reps):
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return r, ts
+
+    def forward():
+        with torch.no_grad():
+            env = ctm(A, cfg)
+            return float(compute_energy_ctm(A, env, H, d))
+
+    forward()  # plans, cuSOLVER handles
+    E, t_fwd = timed(forward, args.ctm_reps)
+    (E_g, grad, Ps), t_grad = timed(lambda: energy_and_grad(A, H, cfg), args.ctm_reps)
+    _, t_grad_fixed = timed(lambda: energy_and_grad(A, H, cfg, projectors=Ps), args.ctm_reps)
+
+    def energy_fixed(x):
+        with torch.no_grad():
+            return float(compute_energy_ctm(x, ctm(x, cfg, projectors=Ps), H, d))
+
+    h, worst, dirs = 1e-6, 0.0, []
+    vr = np.random.default_rng(args.ctm_seed + 1)
+    for _ in range(20):
+        v = torch.from_numpy(vr.standard_normal(A.shape)).cuda()
+        fd = (energy_fixed(A + h * v) - energy_fixed(A - h * v)) / (2 * h)
+        ad = float((grad * v).sum())
+        rel = abs(fd - ad) / max(abs(ad), 1e-3 * float(grad.norm() * v.norm()))
+        worst = max(worst, rel)
+        dirs.append(rel)
+    out = {"study": "dense 1-site CTMRG, square-lattice S=1/2 Heisenberg, QR projectors (no warm-up)",
+           "D": D, "d": d, "chi": chi, "sweeps": iters, "seed": args.ctm_seed, "data": "seeded N(0,1)/sqrt(2 D^4)",
+           "energy_free_run": E, "energy_grad_run": E_g,
+           "forward_s": [round(t, 4) for t in t_fwd], "forward_grad_s": [round(t, 4) for t in t_grad],
+           "forward_grad_fixed_projectors_s": [round(t, 4) for t in t_grad_fixed],
+           "grad_norm": float(grad.norm()),
+           "fd_check": {"h": h, "directions": 20, "max_rel_err": worst, "median_rel_err": float(np.median(dirs)),
+                        "projectors": "fixed (those of the gradient run)"}}
+    if not args.no_cpu_baseline:
+        import oracle.ctm as oc
+
+        torch.set_num_threads(os.cpu_count() or 1)
+        At = torch.from_numpy(A_host)
+        t0 = time.perf_counter()
+        with torch.no_grad():
+            env = oc.ctm(At, chi, iters, "qr")
+            E_cpu = float(oc.energy(At, env, oc.heisenberg_gate(), d))
+        t_cpu = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        E_rep = oc.energy_fixed(At, oc.heisenberg_gate(), chi, iters, [p.cpu() for p in Ps])
+        out["cpu_baseline"] = {"value": round(t_cpu, 3), "unit": "s (forward, 30 sweeps + energy)",
+                               "cores": torch.get_num_threads(), "kind": "port",
+                               "sample": "the full forward of this workload, oracle restatement in the "
+                                         "reference's einsum order (torch CPU float64)",
+                               "energy_free_run": E_cpu}
+        out["oracle_replay_of_gpu_projectors"] = {"dE": E_g - E_rep, "seconds": round(time.perf_counter() - t0, 3)}
+        if args.ctm_oracle_grad:
+            t0 = time.perf_counter()
+            _, g_or, _ = oc.energy_and_grad(At, oc.heisenberg_gate(), chi, iters, projectors=[p.cpu() for p in Ps],
+                                            checkpoint=True)
+            out["oracle_autograd"] = {"rel_err": float((grad.cpu() - g_or).abs().max() / g_or.abs().max()),
+                                      "seconds": round(time.perf_counter() - t0, 3)}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--dmrg", action="store_true", help="run the cylinder DMRG precision study instead")
@@ -425,6 +519,14 @@ def main():
     ap.add_argument("--lanczos", type=int, default=20)
     ap.add_argument("--cyl-lx", type=int, default=4)
     ap.add_argument("--dmrg-precisions", default="fp64,bf16x3,tf32")
+    ap.add_argument("--svd-driver", default="gesvdj", help="cuSOLVER SVD driver of the DMRG study (or 'default')")
+    ap.add_argument("--svd-streams", type=int, default=8)
+    ap.add_argument("--ctm", action="store_true", help="run the dense CTMRG forward/gradient study instead")
+    ap.add_argument("--ctm-chi", type=int, default=80)
+    ap.add_argument("--ctm-iters", type=int, default=30)
+    ap.add_argument("--ctm-seed", type=int, default=2024)
+    ap.add_argument("--ctm-reps", type=int, default=3)
+    ap.add_argument("--ctm-oracle-grad", action="store_true")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
@@ -442,6 +544,8 @@ def main():
     sys.path.insert(0, ROOT)
     if args.dmrg:
         run_dmrg_study(args)
+    elif args.ctm:
+        run_ctm_study(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -380,3 +380,67 @@ def blockwise_keys(tensors, subscripts):
 
     rec(0)
     return keys
+
+
+def fused_charges(leg_a: Leg, leg_b: Leg, fused_flow: int, modulus: int | None) -> np.ndarray:
+    """Charges of the fused leg, position i*d_b + j holding
+    fused_flow * (flow_a q_a[i] + flow_b q_b[j]) (mod n)
+    (algorithms/_tensor_utils.py:168-203)."""
+    qa = np.asarray(leg_a.charges, dtype=np.int64)
+    qb = np.asarray(leg_b.charges, dtype=np.int64)
+    raw = int(leg_a.flow) * qa[:, None] + int(leg_b.flow) * qb[None, :]
+    q = raw * int(fused_flow)
+    if modulus is not None:
+        q = np.mod(q, modulus)
+    return q.reshape(-1).astype(np.int32)
+
+
+def fuse_indices(t: OTensor, axis_a: int, axis_b: int, fused_label, fused_flow: int) -> OTensor:
+    """Fuse two legs of a block-sparse tensor (_tensor_utils.py:206-325).
+
+    Charge pairs (q_a, q_b) are enumerated over the sorted unique charges of
+    each leg, q_a outer; each fused charge's sector stacks the pairs mapping
+    to it in that order, a pair occupying d(q_a) * d(q_b) consecutive rows
+    (row-major over the two legs' in-sector positions).  Every input block is
+    permuted so the two legs are adjacent at min(axis_a, axis_b), merged and
+    placed at its pair's offset in a zero-initialised fused block."""
+    a, b = sorted((axis_a, axis_b))
+    leg_a, leg_b = t.legs[a], t.legs[b]
+    fq = fused_charges(leg_a, leg_b, fused_flow, t.modulus)
+    ua, ub = np.unique(leg_a.charges), np.unique(leg_b.charges)
+    da = {int(q): int(np.sum(leg_a.charges == q)) for q in ua}
+    db = {int(q): int(np.sum(leg_b.charges == q)) for q in ub}
+    groups: dict = {}
+    for qa in ua:
+        for qb in ub:
+            qf = int(fused_flow) * (int(leg_a.flow) * int(qa) + int(leg_b.flow) * int(qb))
+            if t.modulus is not None:
+                qf %= t.modulus
+            groups.setdefault(qf, []).append((int(qa), int(qb)))
+    where, fdim = {}, {}
+    for qf, pairs in groups.items():
+        off = 0
+        for p in pairs:
+            where[p] = (qf, off)
+            off += da[p[0]] * db[p[1]]
+        fdim[qf] = off
+    others = [i for i in range(len(t.legs)) if i not in (a, b)]
+    legs = [t.legs[i] for i in others]
+    legs.insert(a, Leg(fq, int(fused_flow), fused_label))
+    perm = others[:a] + [a, b] + others[a:]
+    out: dict = {}
+    for key, blk in t.blocks.items():
+        qf, off = where[(int(key[a]), int(key[b]))]
+        x = np.transpose(blk, perm)
+        shp = list(x.shape)
+        x = x.reshape(shp[:a] + [shp[a] * shp[a + 1]] + shp[a + 2:])
+        ok = [key[i] for i in others]
+        nk = tuple(ok[:a]) + (qf,) + tuple(ok[a:])
+        if nk not in out:
+            full = list(x.shape)
+            full[a] = fdim[qf]
+            out[nk] = np.zeros(full, dtype=x.dtype)
+        sl = [slice(None)] * x.ndim
+        sl[a] = slice(off, off + x.shape[a])
+        out[nk][tuple(sl)] = x
+    return OTensor(tuple(legs), out, t.modulus)

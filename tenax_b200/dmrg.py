@@ -52,9 +52,12 @@ class DMRGConfig:
     # with a mixed precision: FP64 Lanczos steps started from the mixed Ritz
     # vector (0 = report the FP64 Rayleigh quotient only)
     fp64_polish_steps: int = 3
-    # cuSOLVER driver of the per-sector SVD (torch.linalg.svd): "gesvd" is 1.6-1.9x faster than the
-    # Jacobi default for 256..1024-wide sectors on B200 with smaller reconstruction error
-    svd_driver: str | None = "gesvd"
+    # cuSOLVER driver of the per-sector SVD (torch.linalg.svd) and the number
+    # of CUDA streams the sectors of one bond are decomposed on concurrently.
+    # chi=2048 cylinder, 4 sweeps, mixed: SVD phase 9.8 s (gesvd, 1 stream),
+    # 4.7 s (gesvd, 8 streams), 2.9 s (Jacobi gesvdj, 8 streams).
+    svd_driver: str | None = "gesvdj"
+    svd_streams: int = 8
 
 
 NOISE_REL = {"fp64": 0.0, "bf16x3": 1e-5, "tf32": 2e-3}
@@ -215,8 +218,71 @@ def _krylov(op: HeffOperator, x0: torch.Tensor, num_steps: int, tol: float, tol_
 # truncated block SVD and bond scaling
 # ---------------------------------------------------------------------------
 
+_SVD_WORKERS: dict = {}
+
+
+def _svd_workers(device: torch.device, n: int):
+    """A thread pool with one CUDA stream per worker on ``device``."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    key = (device.index, n)
+    w = _SVD_WORKERS.get(key)
+    if w is None:
+        with torch.cuda.device(device):
+            streams = [torch.cuda.Stream() for _ in range(n)]
+        w = (ThreadPoolExecutor(max_workers=n, thread_name_prefix="tnx-svd"), streams)
+        _SVD_WORKERS[key] = w
+    return w
+
+
+def sector_svds(mats, driver: str | None = None, n_streams: int = 1):
+    """``torch.linalg.svd(M, full_matrices=False)`` of every sector matrix.
+
+    With ``n_streams > 1`` the sectors are split into ``n_streams`` lists
+    (longest-first, greedy by m*n*min(m,n)) and each list is decomposed on its
+    own CUDA stream by its own host thread: cuSOLVER's per-call latency and
+    its host synchronisation then overlap across sectors.  The results are
+    identical to the sequential calls (same routine, same inputs); the
+    current stream waits for all of them before this returns."""
+    if n_streams <= 1 or len(mats) <= 1:
+        return [torch.linalg.svd(M, full_matrices=False, driver=driver) for M in mats]
+    dev = mats[0].device
+    pool, streams = _svd_workers(dev, n_streams)
+    main = torch.cuda.current_stream(dev)
+    ready = torch.cuda.Event()
+    ready.record(main)
+    cost = [M.shape[0] * M.shape[1] * min(M.shape) for M in mats]
+    parts: list = [[] for _ in range(n_streams)]
+    load = [0] * n_streams
+    for i in sorted(range(len(mats)), key=lambda j: -cost[j]):
+        k = load.index(min(load))
+        parts[k].append(i)
+        load[k] += cost[i]
+    out: list = [None] * len(mats)
+    done = [torch.cuda.Event() for _ in range(n_streams)]
+
+    def run(k):
+        s = streams[k]
+        with torch.cuda.device(dev), torch.cuda.stream(s):
+            s.wait_event(ready)
+            for i in parts[k]:
+                mats[i].record_stream(s)
+                out[i] = torch.linalg.svd(mats[i], full_matrices=False, driver=driver)
+            done[k].record(s)
+
+    for f in [pool.submit(run, k) for k in range(n_streams) if parts[k]]:
+        f.result()
+    for k in range(n_streams):
+        if parts[k]:
+            main.wait_event(done[k])
+    for r in out:
+        for x in r:
+            x.record_stream(main)
+    return out
+
+
 def truncated_svd(t: SymmetricTensor, left_labels, right_labels, new_bond_label, max_singular_values=None,
-                  max_truncation_err=None, normalize=False, driver: str | None = None):
+                  max_truncation_err=None, normalize=False, driver: str | None = None, n_streams: int = 1):
     """Block-diagonal SVD with global truncation (linalg.py:75-333).
 
     Sectors = fused flow-weighted charge of the left legs; each sector matrix
@@ -239,6 +305,7 @@ def truncated_svd(t: SymmetricTensor, left_labels, right_labels, new_bond_label,
             q %= mod
         grouped.setdefault(q, []).append((tuple(key[i] for i in la), tuple(key[i] for i in ra), key))
     results = {}
+    mats = []
     for q, entries in grouped.items():
         lseen, rseen = {}, {}
         for lk, rk, _ in entries:
@@ -254,9 +321,16 @@ def truncated_svd(t: SymmetricTensor, left_labels, right_labels, new_bond_label,
         for lk, rk, key in entries:
             li, ri = lseen[lk], rseen[rk]
             M[loff[li]:loff[li + 1], roff[ri]:roff[ri + 1]] = blocks[key].reshape(lsz[li], rsz[ri])
-        U, S, Vh = torch.linalg.svd(M, full_matrices=False, driver=driver)
-        results[q] = (U, S, Vh, list(lseen), list(rseen), lsz, rsz, loff, roff)
-    s_host = {q: r[1].cpu().numpy() for q, r in results.items()}
+        mats.append(M)
+        results[q] = [None, None, None, list(lseen), list(rseen), lsz, rsz, loff, roff]
+    for r, usv in zip(results.values(), sector_svds(mats, driver, n_streams)):
+        r[0:3] = usv
+    del mats
+    s_all = torch.cat([r[1] for r in results.values()]).cpu().numpy() if results else np.zeros(0)
+    s_host, o = {}, 0
+    for q, r in results.items():
+        s_host[q] = s_all[o:o + r[1].shape[0]]
+        o += r[1].shape[0]
     pairs = [(float(v), q, i) for q in results for i, v in enumerate(s_host[q])]
     pairs.sort(key=lambda x: -x[0])
     s_full = np.array([v for v, _, _ in pairs])
@@ -334,7 +408,7 @@ def svd_and_truncate_site(theta, site, config, sweep_right=True):
         ll, rl = list(labels[: n // 2]), list(labels[n // 2:])
     bond = f"v{site}_{site + 1}"
     A, s, B, s_full = truncated_svd(theta, ll, rl, bond, config.max_bond_dim, config.svd_trunc_err,
-                                    driver=config.svd_driver)
+                                    driver=config.svd_driver, n_streams=config.svd_streams)
     if len(s_full) > len(s):
         err = float(np.sqrt(np.sum(s_full[len(s):] ** 2) / (np.sum(s_full ** 2) + 1e-15)))
     else:

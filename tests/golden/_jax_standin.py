@@ -189,6 +189,18 @@ def install() -> None:
     def cond(pred, true_fun, false_fun, *operands):
         return true_fun(*operands) if bool(pred) else false_fun(*operands)
 
+    def dynamic_update_slice(operand, update, start_indices):
+        # start indices are clamped so that the update fits, as in XLA
+        out = np.array(operand, copy=True)
+        upd = np.asarray(update)
+        sl = []
+        for s, n, m in zip(start_indices, out.shape, upd.shape):
+            s = min(max(int(s), 0), n - m)
+            sl.append(slice(s, s + m))
+        out[tuple(sl)] = upd
+        return out.view(_JArr)
+
+    lax.dynamic_update_slice = dynamic_update_slice
     lax.while_loop = while_loop
     lax.fori_loop = fori_loop
     lax.cond = cond

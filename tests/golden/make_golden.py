@@ -306,6 +306,40 @@ def cylinder_bonds(Lx, Ly):
     return bonds
 
 
+def gen_fuse(M):
+    """fuse_indices (algorithms/_tensor_utils.py:106-325) on symmetric
+    tensors: the fused leg's charges, the output blocks (pair-grouped in-sector
+    order) and the reference's todense() of the result."""
+    tu = M["tenax.algorithms._tensor_utils"]
+    idx = M["tenax.core.index"]
+    rng = np.random.default_rng(31)
+    cases = [
+        # name, modulus, legs (charges, flow, label), axis_a, axis_b, fused flow
+        ("u1_adjacent", None, [([-1, 0, 1, 0, 1], 1, "a"), ([1, -1, 0], 1, "b"), ([0, 1, -1, 2, 1, 0], -1, "c")],
+         0, 1, 1),
+        ("u1_interleaved", None, [([-2, -1, 0, 1, 2], -1, "c1_d"), ([2, 1, 0, -1, -2, 0], -1, "u"),
+                                  ([0, 1, 2, -1, -2, 0, 1], 1, "I")], 0, 1, 1),
+        ("u1_flow_out", None, [([0, 1, -1], 1, "x"), ([1, 1, -1, 0], -1, "y"), ([1, 0, 2, -1], 1, "z")], 1, 2, -1),
+        ("u1_nonadjacent", None, [([0, 1, -1, 1], 1, "p"), ([1, -1], 1, "q"), ([0, 2, -2, 0, 1], -1, "r"),
+                                  ([1, 0, -1], -1, "s")], 0, 2, 1),
+        ("u1_reversed_axes", None, [([1, -1, 0], 1, "p"), ([0, 1, 2], -1, "q"), ([1, 0, -1, 2], -1, "r")], 2, 1, 1),
+        ("z3", 3, [([0, 1, 2, 1], 1, "a"), ([0, 2, 1], 1, "b"), ([1, 2, 0, 0], -1, "c")], 0, 1, -1),
+    ]
+    arrays, meta = {}, []
+    for name, mod, legs, a, b, ff in cases:
+        T = make_sym_tensor(M, legs, rng, modulus=mod)
+        out = tu.fuse_indices(T, a, b, "fused", idx.FlowDirection(ff))
+        arrays.update(dump_tensor(f"{name}.in", T, mod))
+        arrays.update(dump_tensor(f"{name}.out", out, mod))
+        arrays[f"{name}.out_dense"] = np.asarray(out.todense(), dtype=np.float64)
+        arrays[f"{name}.in_dense"] = np.asarray(T.todense(), dtype=np.float64)
+        meta.append({"name": name, "modulus": mod, "axis_a": a, "axis_b": b, "fused_flow": ff,
+                     "n_out_blocks": len(out.blocks), "out_key_order": [list(map(int, k)) for k in out.blocks]})
+    np.savez_compressed(os.path.join(HERE, "fuse.npz"), **arrays)
+    with open(os.path.join(HERE, "fuse.json"), "w") as fh:
+        json.dump(meta, fh, indent=1)
+
+
 def gen_ctm(M):
     """Dense 1-site CTMRG (algorithms/ipeps.py): environments, corner
     singular values and NN Heisenberg energies from the reference's own
@@ -373,7 +407,7 @@ def main():
         "tenax.algorithms.auto_mpo", "tenax.algorithms.dmrg", "tenax.algorithms.ipeps",
     ])
     mods["cfg"] = mods["tenax.algorithms.dmrg"].DMRGConfig
-    todo = args.only.split(",") if args.only else ["valid", "contract", "pieces", "mpo", "c1", "ctm"]
+    todo = args.only.split(",") if args.only else ["valid", "contract", "pieces", "mpo", "c1", "ctm", "fuse"]
     if "valid" in todo:
         gen_valid_blocks(mods)
     if "contract" in todo:
@@ -386,6 +420,8 @@ def main():
         gen_dmrg_c1(mods)
     if "ctm" in todo:
         gen_ctm(mods)
+    if "fuse" in todo:
+        gen_fuse(mods)
 
 
 if __name__ == "__main__":
