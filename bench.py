@@ -511,6 +511,99 @@ def run_ctm_study(args):
     print(json.dumps(out), flush=True)
 
 
+def run_split_ctm_study(args):
+    """Split CTMRG at the U(1) configuration (D=5, bond charges -2..2,
+    physical {-1,+1}, chi = chi_I = 150, 40 sweeps, gradient with the sweeps
+    recomputed in groups of 5) and, because the reference's re-wrap makes
+    that environment identically zero, the same sizes with trivial charges.
+    Reports forward and forward+gradient seconds (FP64 and split-BF16x3
+    forward), peak device memory, energies, the mixed-vs-FP64 gradient
+    difference, and the oracle's CPU time for one sweep (reference order)."""
+    import time
+
+    import torch
+
+    from tenax_b200 import split_ctm as gs
+    from tenax_b200.core import FlowDirection, TensorIndex, U1Symmetry
+    from tenax_b200.ipeps import heisenberg_gate
+    from tenax_b200.tensor import SymmetricTensor, compute_valid_blocks, block_shape
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    D, chi, iters, ck = 5, args.split_chi, args.split_iters, 5
+    H = heisenberg_gate()
+    u1 = U1Symmetry()
+    out = {"study": "U(1) split CTMRG, square-lattice S=1/2 Heisenberg, ket/bra layers kept apart",
+           "D": D, "chi": chi, "chi_I": chi, "sweeps": iters, "checkpoint_every": ck, "runs": {}}
+
+    def site(trivial, seed):
+        bond = np.zeros(D, np.int32) if trivial else np.arange(-(D // 2), D // 2 + 1, dtype=np.int32)
+        phys = np.zeros(2, np.int32) if trivial else np.array([-1, 1], np.int32)
+        flows = (FlowDirection.OUT, FlowDirection.IN, FlowDirection.OUT, FlowDirection.IN, FlowDirection.IN)
+        idx = tuple(TensorIndex(u1, c, f, lab) for c, f, lab in
+                    zip((bond, bond, bond, bond, phys), flows, ("u", "d", "l", "r", "phys")))
+        rng = np.random.default_rng(seed)
+        keys = sorted(k for k in compute_valid_blocks(idx) if all(s > 0 for s in block_shape(idx, k)))
+        return SymmetricTensor({k: rng.standard_normal(block_shape(idx, k)) for k in keys}, idx)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        torch.cuda.reset_peak_memory_stats()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return r, time.perf_counter() - t0, torch.cuda.max_memory_allocated() / 2 ** 30
+
+    for label, trivial in (("u1_charges_-2..2", False), ("trivial_charges", True)):
+        A = site(trivial, args.seed + 5)
+        Ad = A.todense()
+        run = {}
+        rec: list = []
+        with torch.no_grad():
+            env, t, mem = timed(lambda: gs.ctm_split_tensor(A, chi, iters, conv_tol=0.0, record=rec))
+            E = float(gs.compute_energy_split_ctm_tensor(A, env, H, 2))
+        run["fp64_forward"] = {"s": round(t, 3), "peak_GiB": round(mem, 2), "energy": E,
+                               "env_max_abs": max(float(x.abs().max()) for x in env)}
+        with torch.no_grad():
+            envm, t, mem = timed(lambda: gs.ctm_split_tensor(A, chi, iters, conv_tol=0.0, projectors=rec,
+                                                            precision="bf16x3"))
+            Em = float(gs.compute_energy_split_ctm_tensor(A, envm, H, 2))
+        run["bf16x3_forward"] = {"s": round(t, 3), "peak_GiB": round(mem, 2), "energy": Em, "dE_vs_fp64": Em - E}
+        grads = {}
+        for prec in ("fp64", "bf16x3"):
+            def fg():
+                x = Ad.clone().requires_grad_(True)
+                e = gs.ctm_split_tensor(A, chi, iters, conv_tol=0.0, projectors=rec, A_dense=x, precision=prec,
+                                        checkpoint_every=ck)
+                En = gs.compute_energy_split_ctm_tensor(A, e, H, 2, A_dense=x)
+                (g,) = torch.autograd.grad(En, x)
+                return g
+
+            g, t, mem = timed(fg)
+            grads[prec] = g
+            run[f"{prec}_forward_gradient_checkpointed"] = {"s": round(t, 3), "peak_GiB": round(mem, 2),
+                                                             "grad_finite": bool(torch.isfinite(g).all()),
+                                                             "grad_norm": float(g.norm())}
+        g64, gmx = grads["fp64"], grads["bf16x3"]
+        if torch.isfinite(g64).all() and torch.isfinite(gmx).all() and float(g64.abs().max()) > 0:
+            run["grad_rel_err_bf16x3_vs_fp64"] = float((gmx - g64).abs().max() / g64.abs().max())
+        out["runs"][label] = run
+    if not args.no_cpu_baseline:
+        import oracle.split_ctm as osc
+
+        torch.set_num_threads(os.cpu_count() or 1)
+        A = site(True, args.seed + 5)
+        s = osc.Site(A.todense().cpu(), [i.charges for i in A.indices], [int(i.flow) for i in A.indices])
+        t0 = time.perf_counter()
+        with torch.no_grad():
+            osc.ctm_split(s, chi, 1)
+        t1 = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(t1 * iters, 1), "unit": "s (forward, extrapolated)",
+                               "cores": torch.get_num_threads(), "kind": "port",
+                               "sample": f"one sweep of the oracle restatement in the reference's order "
+                                         f"(dense grown edge), {t1:.2f} s, times {iters} sweeps"}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--dmrg", action="store_true", help="run the cylinder DMRG precision study instead")
@@ -527,6 +620,9 @@ def main():
     ap.add_argument("--ctm-seed", type=int, default=2024)
     ap.add_argument("--ctm-reps", type=int, default=3)
     ap.add_argument("--ctm-oracle-grad", action="store_true")
+    ap.add_argument("--split-ctm", action="store_true", help="run the U(1) split CTMRG study instead")
+    ap.add_argument("--split-chi", type=int, default=150)
+    ap.add_argument("--split-iters", type=int, default=40)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
@@ -546,6 +642,8 @@ def main():
         run_dmrg_study(args)
     elif args.ctm:
         run_ctm_study(args)
+    elif args.split_ctm:
+        run_split_ctm_study(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

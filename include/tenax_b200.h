@@ -152,6 +152,33 @@ int64_t tnx_reduce_scratch_len(void);
 int tnx_dot(const double* x, const double* y, int64_t n, double* result, double* scratch, void* stream);
 int tnx_nrm2(const double* x, int64_t n, double* result, double* scratch, void* stream);
 
+/* Leg fusion of a block-sparse tensor (tenax algorithms/_tensor_utils.py:
+ * 106-325, fuse_indices / _compute_fused_charges / _fuse_indices_symmetric).
+ * Legs axis_a and axis_b become one leg at min(axis_a, axis_b) with flow
+ * fused_flow (+1 IN, -1 OUT); position i*d_b + j of it carries charge
+ * fused_flow*(flow_a q_a[i] + flow_b q_b[j]) (mod n for Z_n, modulus > 0).
+ * Inside a fused sector, charge pairs (q_a, q_b) are stacked in sorted order
+ * (q_a outer), each pair's rows row-major over the two legs' in-sector
+ * positions; pairs without an input block are zero.  Tables are integer-exact
+ * against the reference.  Output blocks are stored in sorted-key order.
+ * `in` blocks must be laid out in the descriptor's key order; subs may be
+ * NULL. tnx_fuse_plan_output: fused_charges holds d_a*d_b entries, keys
+ * n_blocks*(n_legs-1); any pointer may be NULL. */
+typedef struct tnx_fuse_plan tnx_fuse_plan;
+int tnx_fuse_plan_create(const tnx_tensor_desc* in, int32_t modulus, int32_t axis_a, int32_t axis_b,
+                         int32_t fused_flow, tnx_fuse_plan** out);
+int tnx_fuse_plan_output(const tnx_fuse_plan* p, int32_t* fused_charges, int64_t* n_fused, int64_t* n_blocks,
+                         int32_t* keys, int64_t* total);
+int tnx_fuse_execute(tnx_fuse_plan* p, const double* in, double* out, void* stream);
+void tnx_fuse_plan_destroy(tnx_fuse_plan* p);
+/* The dense view of a fused leg (todense() of fuse_indices' result,
+ * core/tensor.py:760-781): natural row i*d_b + j of the pair (leg a, leg b)
+ * is placed at position map[i*d_b + j] of the fused leg.  Used by the
+ * split-CTM moves, which fuse and densify grown corners
+ * (algorithms/_split_ctm_tensor.py:522-541). */
+int tnx_fuse_row_map(const int32_t* charges_a, int64_t d_a, int32_t flow_a, const int32_t* charges_b, int64_t d_b,
+                     int32_t flow_b, int32_t fused_flow, int32_t modulus, int64_t* map);
+
 /* Max-abs renormalisation of the CTM environment (tenax
  * algorithms/ipeps.py:1133-1149, _renormalize_env) for 1..8 tensors per call:
  *   y_t = x_t / (max|x_t| + eps),  stat[t] = max|x_t|  (device memory).

@@ -444,3 +444,36 @@ def fuse_indices(t: OTensor, axis_a: int, axis_b: int, fused_label, fused_flow: 
         sl[a] = slice(off, off + x.shape[a])
         out[nk][tuple(sl)] = x
     return OTensor(tuple(legs), out, t.modulus)
+
+
+def fused_row_map(leg_a: Leg, leg_b: Leg, fused_flow: int, modulus: int | None) -> np.ndarray:
+    """Where todense() of a fused tensor puts each natural row.
+
+    Natural row n = i*d_b + j of the pair (leg a, leg b) is row
+    off(q_a, q_b) + rank_a(i)*d(q_b) + rank_b(j) of its fused sector
+    (fuse_indices above); todense() places a sector's k-th row at the k-th
+    position of the fused leg carrying that sector's charge
+    (core/tensor.py:760-781).  Returns map[n] = that position."""
+    fq = fused_charges(leg_a, leg_b, fused_flow, modulus)
+    qa, qb = np.asarray(leg_a.charges), np.asarray(leg_b.charges)
+    ua, ub = np.unique(qa), np.unique(qb)
+    da = {int(q): int(np.sum(qa == q)) for q in ua}
+    db = {int(q): int(np.sum(qb == q)) for q in ub}
+    off, fill = {}, {}
+    for x in ua:
+        for y in ub:
+            qf = int(fused_flow) * (int(leg_a.flow) * int(x) + int(leg_b.flow) * int(y))
+            if modulus is not None:
+                qf %= modulus
+            off[(int(x), int(y))] = fill.get(qf, 0)
+            fill[qf] = fill.get(qf, 0) + da[int(x)] * db[int(y)]
+    pos = {int(q): np.nonzero(fq == q)[0] for q in np.unique(fq)}
+    rank_a = np.array([int(np.sum(qa[:i] == qa[i])) for i in range(len(qa))])
+    rank_b = np.array([int(np.sum(qb[:j] == qb[j])) for j in range(len(qb))])
+    out = np.empty(len(qa) * len(qb), dtype=np.int64)
+    for i in range(len(qa)):
+        for j in range(len(qb)):
+            n = i * len(qb) + j
+            k = off[(int(qa[i]), int(qb[j]))] + rank_a[i] * db[int(qb[j])] + rank_b[j]
+            out[n] = pos[int(fq[n])][k]
+    return out

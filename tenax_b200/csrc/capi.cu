@@ -576,6 +576,94 @@ int tnx_plan_execute(tnx_plan* plan, const double* const* inputs, double* out, i
 
 void tnx_plan_destroy(tnx_plan* plan) { delete plan; }
 
+// ---------------------------------------------------------------------------
+// leg fusion
+// ---------------------------------------------------------------------------
+struct tnx_fuse_plan {
+  FusePlan F;
+  DevMem segs, chunks;
+  int n_chunks = 0;
+  bool on_device = false;
+};
+
+int tnx_fuse_plan_create(const tnx_tensor_desc* in, int32_t modulus, int32_t axis_a, int32_t axis_b,
+                         int32_t fused_flow, tnx_fuse_plan** out) {
+  TNX_TRY({
+    if (!out) return set_err(TNX_ERR_VALUE, "null output pointer");
+    *out = nullptr;
+    if (!in) return set_err(TNX_ERR_VALUE, "null tensor descriptor");
+    std::string subs(static_cast<size_t>(std::max(0, in->n_legs)), 'a');
+    for (int l = 0; l < in->n_legs; ++l) subs[l] = static_cast<char>('a' + l);
+    TensorStruct T = parse_desc(in, in->subs ? nullptr : subs.c_str());
+    auto p = std::make_unique<tnx_fuse_plan>();
+    p->F = plan_fuse(T, axis_a, axis_b, fused_flow, modulus);
+    *out = p.release();
+    return TNX_OK;
+  })
+}
+
+int tnx_fuse_plan_output(const tnx_fuse_plan* p, int32_t* fused_charges, int64_t* n_fused, int64_t* n_blocks,
+                         int32_t* keys, int64_t* total) {
+  TNX_TRY({
+    if (!p) return set_err(TNX_ERR_VALUE, "null fuse plan");
+    const FusePlan& F = p->F;
+    if (n_fused) *n_fused = static_cast<int64_t>(F.fused_charges.size());
+    if (fused_charges) std::memcpy(fused_charges, F.fused_charges.data(), F.fused_charges.size() * sizeof(int32_t));
+    if (n_blocks) *n_blocks = static_cast<int64_t>(F.out.keys.size());
+    if (keys)
+      for (size_t b = 0; b < F.out.keys.size(); ++b)
+        std::memcpy(keys + b * F.out.nl, F.out.keys[b].data(), F.out.nl * sizeof(int32_t));
+    if (total) *total = F.out.total;
+    return TNX_OK;
+  })
+}
+
+int tnx_fuse_execute(tnx_fuse_plan* p, const double* in, double* out, void* stream) {
+  TNX_TRY({
+    if (!p) return set_err(TNX_ERR_VALUE, "null fuse plan");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!p->on_device) {
+      std::vector<DevCopySeg> segs;
+      std::vector<DevChunk> chunks;
+      for (const CopySeg& c : p->F.segs) {
+        DevCopySeg d{};
+        d.src_off = c.src_off;
+        d.dst_off = c.dst_off;
+        d.nlegs = c.nlegs;
+        for (int l = 0; l < c.nlegs; ++l) {
+          d.dims[l] = c.dims[l];
+          d.dstr[l] = c.dstr[l];
+        }
+        const int id = static_cast<int>(segs.size());
+        segs.push_back(d);
+        for (int64_t s = 0; s < c.count; s += 2048) chunks.push_back({id, 0, s, std::min<int64_t>(2048, c.count - s)});
+      }
+      upload(p->segs, segs);
+      upload(p->chunks, chunks);
+      p->n_chunks = static_cast<int>(chunks.size());
+      CUDA_OK(cudaDeviceSynchronize());
+      p->on_device = true;
+    }
+    if (p->F.out.total > 0) CUDA_OK(cudaMemsetAsync(out, 0, p->F.out.total * sizeof(double), st));
+    launch_strided_copy(in, out, p->segs.as<DevCopySeg>(), p->chunks.as<DevChunk>(), p->n_chunks, st);
+    CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
+
+void tnx_fuse_plan_destroy(tnx_fuse_plan* p) { delete p; }
+
+int tnx_fuse_row_map(const int32_t* charges_a, int64_t d_a, int32_t flow_a, const int32_t* charges_b, int64_t d_b,
+                     int32_t flow_b, int32_t fused_flow, int32_t modulus, int64_t* map) {
+  TNX_TRY({
+    if (d_a < 0 || d_b < 0 || (!map && d_a * d_b > 0)) return set_err(TNX_ERR_VALUE, "fuse_row_map: bad arguments");
+    std::vector<int32_t> qa(charges_a, charges_a + d_a), qb(charges_b, charges_b + d_b);
+    auto m = fuse_row_map(qa, flow_a, qb, flow_b, fused_flow, modulus);
+    if (!m.empty()) std::memcpy(map, m.data(), m.size() * sizeof(int64_t));
+    return TNX_OK;
+  })
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

@@ -78,6 +78,16 @@ struct DevScatSeg {
   int32_t cstr[kMaxLegsDev];
 };
 
+// Copy one block element-for-element: source element e (row-major over
+// dims) lands at dst_off + sum_l idx_l * dstr[l].
+struct DevCopySeg {
+  int64_t src_off;
+  int64_t dst_off;
+  int32_t nlegs, pad;
+  int32_t dims[kMaxLegsDev];
+  int64_t dstr[kMaxLegsDev];
+};
+
 struct DevChunk {  // one CTA's share of a segment list
   int32_t seg;
   int32_t pad;

@@ -90,6 +90,30 @@ void launch_scatter(const void* res, bool res_f32, double* out, const DevScatSeg
 }
 
 // ---------------------------------------------------------------------------
+// strided block copy (leg fusion): reads in source order, writes permuted
+// ---------------------------------------------------------------------------
+__global__ void strided_copy_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                    const DevCopySeg* __restrict__ segs, const DevChunk* __restrict__ chunks) {
+  const DevChunk ch = chunks[blockIdx.x];
+  const DevCopySeg& s = segs[ch.seg];
+  for (int64_t e = ch.start + threadIdx.x; e < ch.start + ch.count; e += blockDim.x) {
+    int64_t rem = e, off = 0;
+    for (int l = s.nlegs - 1; l >= 0; --l) {
+      const int64_t d = s.dims[l];
+      off += (rem % d) * s.dstr[l];
+      rem /= d;
+    }
+    dst[s.dst_off + off] = src[s.src_off + e];
+  }
+}
+
+void launch_strided_copy(const double* src, double* dst, const DevCopySeg* segs, const DevChunk* chunks, int n_chunks,
+                         cudaStream_t st) {
+  if (n_chunks <= 0) return;
+  strided_copy_kernel<<<n_chunks, 256, 0, st>>>(src, dst, segs, chunks);
+}
+
+// ---------------------------------------------------------------------------
 // zero fill of output ranges addressed through a pointer table
 // ---------------------------------------------------------------------------
 __global__ void zero_ranges_kernel(const uint64_t* __restrict__ out_tab, const DevChunk* __restrict__ chunks,

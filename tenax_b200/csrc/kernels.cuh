@@ -19,6 +19,9 @@ void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevM
                       const DevMpoOutSlot* oslots, const DevMpoTerm* terms, const int2* chunks, int n_chunks,
                       size_t smem_bytes, const int32_t* skip, cudaStream_t st);
 int mpo_points_per_cta();
+// dst[seg.dst_off + sum idx_l dstr_l] = src[seg.src_off + e] for each chunk's range of elements e
+void launch_strided_copy(const double* src, double* dst, const DevCopySeg* segs, const DevChunk* chunks, int n_chunks,
+                         cudaStream_t st);
 void launch_dot(const double* x, const double* y, int64_t n, int kind, double* result, double* partials,
                 const int32_t* skip, cudaStream_t st);
 void launch_lanczos_step(double* w, const double* v, const double* vp, double* vnext, int64_t n, double* alpha,

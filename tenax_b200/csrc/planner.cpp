@@ -769,3 +769,158 @@ void heff_mpo_terms(HeffPlan& H, const std::vector<double>& wl, const std::vecto
 }
 
 }  // namespace tnx
+
+namespace tnx {
+
+// ---------------------------------------------------------------------------
+// Leg fusion (algorithms/_tensor_utils.py:106-325).
+//  * fused charge of position i*d_b + j: fused_flow*(flow_a q_a[i] + flow_b q_b[j]), mod n (:168-203);
+//  * pairs (q_a, q_b) over the sorted unique charges of each leg, q_a outer;
+//    a fused sector stacks its pairs in that order, d(q_a)*d(q_b) rows each (:255-270);
+//  * each block is permuted so the legs are adjacent at axis_a, merged, and
+//    placed at its pair's offset in a zero-initialised fused block (:282-320).
+// ---------------------------------------------------------------------------
+static int32_t fuse_mod(int64_t q, int32_t modulus) {
+  if (modulus <= 0) return static_cast<int32_t>(q);
+  int64_t r = q % modulus;
+  return static_cast<int32_t>(r < 0 ? r + modulus : r);
+}
+
+FusePlan plan_fuse(const TensorStruct& T, int axis_a, int axis_b, int32_t fused_flow, int32_t modulus) {
+  if (T.nl < 2) throw PlanError{1, "fuse_indices needs a tensor with at least two legs"};
+  if (axis_a < 0 || axis_a >= T.nl || axis_b < 0 || axis_b >= T.nl || axis_a == axis_b)
+    throw PlanError{1, "fuse_indices: axes must be two distinct legs of the tensor"};
+  if (fused_flow != 1 && fused_flow != -1) throw PlanError{1, "fuse_indices: fused flow must be +1 or -1"};
+  FusePlan F;
+  const int a = std::min(axis_a, axis_b), b = std::max(axis_a, axis_b);
+  F.axis_a = a;
+  F.axis_b = b;
+  const auto& qa = T.charges[a];
+  const auto& qb = T.charges[b];
+  const int64_t fa = T.flows[a], fb = T.flows[b];
+  F.fused_charges.resize(qa.size() * qb.size());
+  for (size_t i = 0; i < qa.size(); ++i)
+    for (size_t j = 0; j < qb.size(); ++j)
+      F.fused_charges[i * qb.size() + j] = fuse_mod(fused_flow * (fa * qa[i] + fb * qb[j]), modulus);
+  std::vector<int32_t> ua(qa.begin(), qa.end()), ub(qb.begin(), qb.end());
+  std::sort(ua.begin(), ua.end());
+  ua.erase(std::unique(ua.begin(), ua.end()), ua.end());
+  std::sort(ub.begin(), ub.end());
+  ub.erase(std::unique(ub.begin(), ub.end()), ub.end());
+  // offset of each pair inside its fused sector
+  std::map<int32_t, int64_t> sector_fill;
+  std::map<std::pair<int32_t, int32_t>, std::pair<int32_t, int64_t>> where;
+  for (int32_t x : ua)
+    for (int32_t y : ub) {
+      const int32_t qf = fuse_mod(fused_flow * (fa * x + fb * y), modulus);
+      int64_t& fill = sector_fill[qf];
+      where[{x, y}] = {qf, fill};
+      fill += T.leg_dim(a, x) * T.leg_dim(b, y);
+    }
+  // output structure
+  std::vector<int> others;
+  for (int i = 0; i < T.nl; ++i)
+    if (i != a && i != b) others.push_back(i);
+  TensorStruct& O = F.out;
+  O.nl = T.nl - 1;
+  O.subs.clear();
+  for (int j = 0; j < static_cast<int>(others.size()); ++j) {
+    if (j == a) {
+      O.flows.push_back(fused_flow);
+      O.charges.push_back(F.fused_charges);
+    }
+    O.flows.push_back(T.flows[others[j]]);
+    O.charges.push_back(T.charges[others[j]]);
+  }
+  if (a == static_cast<int>(others.size())) {
+    O.flows.push_back(fused_flow);
+    O.charges.push_back(F.fused_charges);
+  }
+  O.finalize_leg_maps();
+  auto new_key = [&](const Key& k) {
+    Key nk;
+    for (int j = 0; j < static_cast<int>(others.size()); ++j) {
+      if (j == a) nk.push_back(where.at({k[a], k[b]}).first);
+      nk.push_back(k[others[j]]);
+    }
+    if (a == static_cast<int>(others.size())) nk.push_back(where.at({k[a], k[b]}).first);
+    return nk;
+  };
+  std::set<Key> keyset;
+  for (const auto& k : T.keys) keyset.insert(new_key(k));
+  O.keys.assign(keyset.begin(), keyset.end());
+  O.layout_blocks();
+  std::map<Key, size_t> kidx;
+  for (size_t i = 0; i < O.keys.size(); ++i) kidx[O.keys[i]] = i;
+  // copy segments: source legs -> destination strides
+  for (size_t bi = 0; bi < T.keys.size(); ++bi) {
+    int64_t n = 1;
+    for (int l = 0; l < T.nl; ++l) n *= T.dims[bi][l];
+    if (n == 0) continue;
+    const Key& k = T.keys[bi];
+    const size_t ob = kidx.at(new_key(k));
+    const auto& od = O.dims[ob];
+    std::vector<int64_t> ostr(O.nl);
+    int64_t s = 1;
+    for (int l = O.nl - 1; l >= 0; --l) {
+      ostr[l] = s;
+      s *= od[l];
+    }
+    CopySeg c{};
+    c.src_off = T.offs[bi];
+    c.count = n;
+    c.nlegs = T.nl;
+    c.dst_off = O.offs[ob] + where.at({k[a], k[b]}).second * ostr[a];
+    for (int l = 0; l < T.nl; ++l) c.dims[l] = static_cast<int32_t>(T.dims[bi][l]);
+    c.dstr[a] = ostr[a] * T.dims[bi][b];
+    c.dstr[b] = ostr[a];
+    for (int j = 0; j < static_cast<int>(others.size()); ++j) c.dstr[others[j]] = ostr[j < a ? j : j + 1];
+    F.segs.push_back(c);
+  }
+  return F;
+}
+
+}  // namespace tnx
+
+namespace tnx {
+
+// Where todense() of a fused tensor puts natural row n = i*d_b + j: row
+// off(q_a, q_b) + rank_a(i)*d(q_b) + rank_b(j) of its fused sector (see
+// plan_fuse), which todense() (core/tensor.py:760-781) places at the k-th
+// position of the fused leg carrying that charge.
+std::vector<int64_t> fuse_row_map(const std::vector<int32_t>& qa, int32_t fa, const std::vector<int32_t>& qb,
+                                  int32_t fb, int32_t fused_flow, int32_t modulus) {
+  if (fused_flow != 1 && fused_flow != -1) throw PlanError{1, "fused flow must be +1 or -1"};
+  const size_t na = qa.size(), nb = qb.size();
+  std::map<int32_t, int64_t> da, db;
+  for (int32_t q : qa) da[q] += 1;
+  for (int32_t q : qb) db[q] += 1;
+  auto fq = [&](int32_t x, int32_t y) { return fuse_mod(fused_flow * (int64_t(fa) * x + int64_t(fb) * y), modulus); };
+  std::map<int32_t, int64_t> fill;
+  std::map<std::pair<int32_t, int32_t>, int64_t> off;
+  for (auto& x : da)
+    for (auto& y : db) {
+      const int32_t q = fq(x.first, y.first);
+      off[{x.first, y.first}] = fill[q];
+      fill[q] += x.second * y.second;
+    }
+  std::map<int32_t, std::vector<int64_t>> pos;
+  for (size_t i = 0; i < na; ++i)
+    for (size_t j = 0; j < nb; ++j) pos[fq(qa[i], qb[j])].push_back(static_cast<int64_t>(i * nb + j));
+  std::vector<int64_t> rank_a(na), rank_b(nb);
+  {
+    std::map<int32_t, int64_t> c;
+    for (size_t i = 0; i < na; ++i) rank_a[i] = c[qa[i]]++;
+    c.clear();
+    for (size_t j = 0; j < nb; ++j) rank_b[j] = c[qb[j]]++;
+  }
+  std::vector<int64_t> out(na * nb);
+  for (size_t i = 0; i < na; ++i)
+    for (size_t j = 0; j < nb; ++j) {
+      const int64_t k = off[{qa[i], qb[j]}] + rank_a[i] * db[qb[j]] + rank_b[j];
+      out[i * nb + j] = pos[fq(qa[i], qb[j])][static_cast<size_t>(k)];
+    }
+  return out;
+}
+
+}  // namespace tnx

@@ -171,4 +171,26 @@ HeffPlan plan_heff(const TensorStruct& L, const TensorStruct& th, const TensorSt
 // W_l / W_r block buffers.
 void heff_mpo_terms(HeffPlan& p, const std::vector<double>& wl, const std::vector<double>& wr);
 
+// ---------------------------------------------------------------------------
+// Leg fusion (fuse_indices, algorithms/_tensor_utils.py:106-325).
+// ---------------------------------------------------------------------------
+struct CopySeg {
+  int64_t src_off, dst_off, count;
+  int32_t nlegs;
+  int32_t dims[kMaxLegs];
+  int64_t dstr[kMaxLegs];
+};
+
+struct FusePlan {
+  int axis_a = 0, axis_b = 0;         // sorted: axis_a < axis_b
+  std::vector<int32_t> fused_charges; // position i*d_b + j
+  TensorStruct out;                   // fused leg at axis_a; keys sorted
+  std::vector<CopySeg> segs;          // one per input block with a nonzero size
+};
+
+FusePlan plan_fuse(const TensorStruct& T, int axis_a, int axis_b, int32_t fused_flow, int32_t modulus);
+// todense() position of each natural row i*d_b + j of a fused pair of legs
+std::vector<int64_t> fuse_row_map(const std::vector<int32_t>& qa, int32_t fa, const std::vector<int32_t>& qb,
+                                  int32_t fb, int32_t fused_flow, int32_t modulus);
+
 }  // namespace tnx

@@ -106,31 +106,34 @@ class Contract(torch.autograd.Function):
     """Differentiable pairwise contraction: forward and adjoint on the engine."""
 
     @staticmethod
-    def forward(ctx, subscripts, a, b):
+    def forward(ctx, subscripts, precision, a, b):
         ctx.subscripts = subscripts
+        ctx.precision = precision
         ctx.save_for_backward(a, b)
-        return einsum(subscripts, a, b)
+        return einsum(subscripts, a, b, precision=precision)
 
     @staticmethod
     def backward(ctx, g):
         a, b = ctx.saved_tensors
         lhs, so = ctx.subscripts.split("->")
         sa, sb = lhs.split(",")
-        ga = einsum(f"{so},{sb}->{sa}", g, b) if ctx.needs_input_grad[1] else None
-        gb = einsum(f"{sa},{so}->{sb}", a, g) if ctx.needs_input_grad[2] else None
-        return None, ga, gb
+        p = ctx.precision
+        ga = einsum(f"{so},{sb}->{sa}", g, b, precision=p) if ctx.needs_input_grad[2] else None
+        gb = einsum(f"{sa},{so}->{sb}", a, g, precision=p) if ctx.needs_input_grad[3] else None
+        return None, None, ga, gb
 
 
-def contract(subscripts: str, a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+def contract(subscripts: str, a: torch.Tensor, b: torch.Tensor, precision: str = "fp64") -> torch.Tensor:
     """``einsum`` of two operands that records its adjoint for autograd.
 
     Every subscript of each operand must appear in the other operand or in
     the output (a pure contraction), which is what makes the adjoint two
-    contractions of the same form."""
+    contractions of the same form.  The adjoint runs in the forward's
+    precision."""
     lhs, so = subscripts.split("->")
     sa, sb = lhs.split(",")
     for s, other in ((sa, sb + so), (sb, sa + so)):
         missing = [c for c in s if c not in other]
         if missing:
             raise ValueError(f"'{subscripts}': subscripts {missing} are summed within one operand")
-    return Contract.apply(subscripts, a, b)
+    return Contract.apply(subscripts, precision, a, b)

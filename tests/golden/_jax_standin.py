@@ -115,6 +115,16 @@ def record_stop_gradient(log) -> None:
     _SG_LOG = log
 
 
+_SVD_LOG = None
+
+
+def record_svd(log) -> None:
+    """Append (U, s, Vh) of every ``jnp.linalg.svd(..., compute_uv=True)``
+    call to ``log``, or stop recording when ``log`` is None."""
+    global _SVD_LOG
+    _SVD_LOG = log
+
+
 def install() -> None:
     """Register the stand-in modules in ``sys.modules``."""
     jnp = _NumpyModule("jax.numpy", np)
@@ -133,6 +143,14 @@ def install() -> None:
     jnp.int32 = np.int32
     jnp.ndarray = np.ndarray
     jnp.linalg = _NumpyModule("jax.numpy.linalg", np.linalg)
+
+    def svd(a, full_matrices=True, compute_uv=True, **kw):
+        r = np.linalg.svd(np.asarray(a), full_matrices=full_matrices, compute_uv=compute_uv)
+        if compute_uv and _SVD_LOG is not None:
+            _SVD_LOG.append(tuple(np.array(x, dtype=np.float64, copy=True) for x in r))
+        return _wrap(tuple(r) if compute_uv else r)
+
+    jnp.linalg.svd = svd
 
     jax = types.ModuleType("jax")
     jax.numpy = jnp

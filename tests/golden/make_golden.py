@@ -340,6 +340,64 @@ def gen_fuse(M):
         json.dump(meta, fh, indent=1)
 
 
+def gen_split_ctm(M):
+    """U(1) split-CTMRG (algorithms/_split_ctm_tensor.py) on small symmetric
+    site tensors: every projector (recorded at stop_gradient, ket/bra per
+    move in call order) and every edge-split SVD (U, s, Vh) the reference
+    computed, the final environments (dense) and the energy from
+    compute_energy_split_ctm_tensor.  Site legs (u, d, l, r, phys) with flows
+    (OUT, IN, OUT, IN, IN), N(0,1) blocks in sorted-key order.
+
+    Trivial-charge cases (all charges 0, the only setting in which the
+    reference's own tests check values) and U(1) cases with bond charges
+    -k..k of multiplicity 1 and physical charges {-1, +1}.  On the U(1) cases
+    the reference's environment becomes exactly zero within the first sweep
+    (its charge-tiled re-wrapping of the rotated corners and edges keeps no
+    entry), and the fixture records that."""
+    sc = M["tenax.algorithms._split_ctm_tensor"]
+    sz = np.array([[0.5, 0.0], [0.0, -0.5]])
+    sp = np.array([[0.0, 1.0], [0.0, 0.0]])
+    H = (np.kron(sz, sz) + 0.5 * np.kron(sp, sp.T) + 0.5 * np.kron(sp.T, sp)).reshape(2, 2, 2, 2)
+    # (name, D, bond charges (None: -k..k), chi, sweeps, seed)
+    cases = [("triv_d2_chi6", 2, [0, 0], 6, 3, 44), ("triv_d3_chi8", 3, [0, 0, 0], 8, 3, 45),
+             ("u1_d3_chi6", 3, None, 6, 2, 41), ("u1_d3_chi9", 3, None, 9, 2, 42)]
+    arrays, meta = {"H": H}, {}
+    names = ("C1", "C2", "C3", "C4", "T1_ket", "T1_bra", "T2_ket", "T2_bra", "T3_ket", "T3_bra", "T4_ket",
+             "T4_bra")
+    for name, D, bond, chi, iters, seed in cases:
+        rng = np.random.default_rng(seed)
+        trivial = bond is not None
+        if bond is None:
+            bond = list(range(-(D // 2), D // 2 + 1))
+        phys = [0, 0] if trivial else [-1, 1]
+        legs = [(bond, -1, "u"), (bond, 1, "d"), (bond, -1, "l"), (bond, 1, "r"), (phys, 1, "phys")]
+        A = make_sym_tensor(M, legs, rng)
+        sg, sv = [], []
+        _jax_standin.record_stop_gradient(sg)
+        _jax_standin.record_svd(sv)
+        t0 = time.time()
+        env = sc.ctm_split_tensor(A, chi, max_iter=iters, conv_tol=0.0)
+        _jax_standin.record_stop_gradient(None)
+        _jax_standin.record_svd(None)
+        E = float(sc.compute_energy_split_ctm_tensor(A, env, H, 2))
+        assert len(sg) == 8 * iters and len(sv) == 4 * iters, (name, len(sg), len(sv))
+        arrays.update(dump_tensor(f"{name}.A", A))
+        for i, P in enumerate(sg):
+            arrays[f"{name}.P{i}"] = P
+        for i, (U, s, Vh) in enumerate(sv):
+            arrays[f"{name}.svdU{i}"] = U
+            arrays[f"{name}.svds{i}"] = s
+            arrays[f"{name}.svdVh{i}"] = Vh
+        for nm, x in zip(names, env):
+            arrays[f"{name}.{nm}"] = np.asarray(x.todense(), dtype=np.float64)
+        meta[name] = {"D": D, "bond_charges": [int(q) for q in bond], "phys_charges": phys, "chi": chi,
+                      "chi_I": chi, "iters": iters, "seed": seed, "energy": E}
+        print(f"split ctm {name}: E={E:.15f} ({time.time() - t0:.1f} s)", flush=True)
+    np.savez_compressed(os.path.join(HERE, "split_ctm.npz"), **arrays)
+    with open(os.path.join(HERE, "split_ctm.json"), "w") as fh:
+        json.dump(meta, fh, indent=1)
+
+
 def gen_ctm(M):
     """Dense 1-site CTMRG (algorithms/ipeps.py): environments, corner
     singular values and NN Heisenberg energies from the reference's own
@@ -405,9 +463,10 @@ def main():
         "tenax.core.symmetry", "tenax.core.index", "tenax.core.tensor", "tenax.linalg",
         "tenax.contraction.contractor", "tenax.network.network", "tenax.algorithms._tensor_utils",
         "tenax.algorithms.auto_mpo", "tenax.algorithms.dmrg", "tenax.algorithms.ipeps",
+        "tenax.algorithms._split_ctm_tensor",
     ])
     mods["cfg"] = mods["tenax.algorithms.dmrg"].DMRGConfig
-    todo = args.only.split(",") if args.only else ["valid", "contract", "pieces", "mpo", "c1", "ctm", "fuse"]
+    todo = args.only.split(",") if args.only else ["valid", "contract", "pieces", "mpo", "c1", "ctm", "fuse", "split"]
     if "valid" in todo:
         gen_valid_blocks(mods)
     if "contract" in todo:
@@ -422,6 +481,8 @@ def main():
         gen_ctm(mods)
     if "fuse" in todo:
         gen_fuse(mods)
+    if "split" in todo:
+        gen_split_ctm(mods)
 
 
 if __name__ == "__main__":
