@@ -21,6 +21,7 @@ from tenax_b200.tensor import SymmetricTensor, compute_valid_blocks, inner  # no
 from tenax_b200.contraction import (  # noqa: F401
     blockwise_contract,
     contract,
+    contract_ad,
     contract_with_subscripts,
 )
 from tenax_b200.heff import HeffBatch, HeffOperator  # noqa: F401

@@ -183,3 +183,75 @@ def contract(*tensors, output_labels=None, optimize="auto", precision=None):
         if lhs == rhs:
             return tensors[0]
     return contract_with_subscripts(tensors, subscripts, output_indices, optimize, precision)
+
+
+# ---------------------------------------------------------------------------
+# differentiable block-sparse contraction
+# ---------------------------------------------------------------------------
+
+def _onto_keys(t: SymmetricTensor, keys) -> torch.Tensor:
+    """Flat data of ``t`` laid out over ``keys``: blocks ``t`` has are copied,
+    the others are zero, blocks of ``t`` outside ``keys`` are dropped."""
+    from tenax_b200.tensor import embed_in_keys, restrict_to_keys
+
+    keys = sorted(keys)
+    common = sorted(set(t.keys) & set(keys))
+    return embed_in_keys(restrict_to_keys(t, common), keys).data
+
+
+class _SymContract(torch.autograd.Function):
+    """C = A (x) B over shared subscripts on the block-sparse engine, with
+    the adjoint written out: dA = dC (x) B and dB = A (x) dC, each another
+    contraction of the same engine (unfiltered matching), laid out on the
+    operand's own key set (blocks an operand does not store get no gradient:
+    they are structurally zero)."""
+
+    @staticmethod
+    def forward(ctx, spec, a_data, b_data):
+        a_idx, a_keys, b_idx, b_keys, subs, out_idx, filtered, precision = spec
+        a = SymmetricTensor.from_flat(a_idx, a_keys, a_data)
+        b = SymmetricTensor.from_flat(b_idx, b_keys, b_data)
+        if filtered:
+            out = _contract_symmetric([a, b], subs, out_idx, precision)
+        else:
+            out = blockwise_contract([a, b], subs, out_idx, precision)
+        ctx.spec = spec
+        ctx.out_keys = out.keys
+        ctx.save_for_backward(a_data, b_data)
+        return out.data
+
+    @staticmethod
+    def backward(ctx, g):
+        a_idx, a_keys, b_idx, b_keys, subs, out_idx, _, precision = ctx.spec
+        a_data, b_data = ctx.saved_tensors
+        lhs, so = subs.split("->")
+        sa, sb = lhs.split(",")
+        gc = SymmetricTensor.from_flat(out_idx, ctx.out_keys, g.contiguous())
+        ga = gb = None
+        if ctx.needs_input_grad[1]:
+            b = SymmetricTensor.from_flat(b_idx, b_keys, b_data)
+            ga = _onto_keys(blockwise_contract([gc, b], f"{so},{sb}->{sa}", a_idx, precision), a_keys)
+        if ctx.needs_input_grad[2]:
+            a = SymmetricTensor.from_flat(a_idx, a_keys, a_data)
+            gb = _onto_keys(blockwise_contract([a, gc], f"{sa},{so}->{sb}", b_idx, precision), b_keys)
+        return None, ga, gb
+
+
+def contract_ad(a: SymmetricTensor, b: SymmetricTensor, output_labels=None, precision=None) -> SymmetricTensor:
+    """``contract(a, b)`` (contractor.py:490-531, filtered semantics) whose
+    result's flat ``data`` carries autograd history: gradients flow to
+    ``a.data`` / ``b.data`` through the hand-written block-sparse adjoint."""
+    subscripts, out_idx = _labels_to_subscripts((a, b), output_labels)
+    lhs, so = subscripts.split("->")
+    sa, sb = lhs.split(",")
+    for s, other in ((sa, sb + so), (sb, sa + so)):
+        if any(c not in other for c in s):
+            raise TnxUnsupportedAD(f"'{subscripts}': a leg summed within one operand has no adjoint here")
+    spec = (a.indices, a.keys, b.indices, b.keys, subscripts, tuple(out_idx), True, precision)
+    data = _SymContract.apply(spec, a.data, b.data)
+    probe = get_plan([a, b], [sa, sb], so, _capi.MATCH_FILTERED, tuple(out_idx))
+    return SymmetricTensor.from_flat(tuple(out_idx), probe.out_keys, data)
+
+
+class TnxUnsupportedAD(NotImplementedError):
+    """A contraction form whose adjoint is not a contraction of the same kind."""
