@@ -175,6 +175,7 @@ void build_pack(const std::vector<PackSeg>& segs, const PairGeom& G, bool a_side
       d.dims[l] = s.dims[l];
       d.rstr[l] = s.rstr[l];
       d.kstr[l] = s.kstr[l];
+      d.kdstr[l] = s.kdstr[l];
       if (s.kstr[l]) d.kcount *= s.dims[l];
     }
     int seg_id = static_cast<int>(out.size());
@@ -1109,6 +1110,8 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
                 MI.push_back(sl);
               }
         }
+        // stage-4 K places each f block's d range at a multiple of kMpoKAlign
+        const int32_t md_pad = (mp.md + kMpoKAlign - 1) / kMpoKAlign * kMpoKAlign;
         for (size_t k = 0; k < mp.outs.size(); ++k) {
           const MpoOut& o = mp.outs[k];
           for (int s = 0; s < o.ms; ++s)
@@ -1122,7 +1125,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
                 os.k0 = o.k0;
                 os.rows_per_c = o.ms * o.mt;
                 os.row_add = s * o.mt + t;
-                os.k_add = f * mp.md;
+                os.k_add = f * md_pad;
                 MO.push_back(os);
               }
         }
@@ -1130,7 +1133,9 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         const int pair_id = static_cast<int>(MP.size());
         MP.push_back(dp);
         const int ppc = mpo_points_per_cta();
-        for (int p0 = 0; p0 < mp.mc * mp.md; p0 += ppc) MC.push_back(make_int2(pair_id, p0));
+        const int dpt = mpo_d_per_thread(b->mode);
+        const int npts = mp.mc * ((mp.md + dpt - 1) / dpt);
+        for (int p0 = 0; p0 < npts; p0 += ppc) MC.push_back(make_int2(pair_id, p0));
       }
     }
     if (b->mpo_smem > 200 * 1024)

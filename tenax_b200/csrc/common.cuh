@@ -55,6 +55,7 @@ __host__ __device__ inline int64_t img_byte_offset(int mode, int64_t tile0, int 
 // device tables
 // ---------------------------------------------------------------------------
 constexpr int kMaxLegsDev = 12;  // equals kMaxLegs of the planner
+constexpr int kMpoKAlignDev = 8;  // equals kMpoKAlign of the planner (stage-4 d padding)
 
 struct DevPackSeg {
   int64_t src_off;    // element offset of the block in operand buffer src_tab[src_slot]
@@ -65,7 +66,8 @@ struct DevPackSeg {
   double scale;              // multiplies every packed value (an exact power of two)
   int32_t dims[kMaxLegsDev];
   int32_t rstr[kMaxLegsDev];
-  int32_t kstr[kMaxLegsDev];
+  int32_t kstr[kMaxLegsDev];   // contracted-leg strides of the element order (k fastest)
+  int32_t kdstr[kMaxLegsDev];  // contracted-leg strides in the image's K coordinate
 };
 
 struct DevScatSeg {

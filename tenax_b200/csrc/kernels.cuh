@@ -19,6 +19,8 @@ void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevM
                       const DevMpoOutSlot* oslots, const DevMpoTerm* terms, const int2* chunks, int n_chunks,
                       size_t smem_bytes, const int32_t* skip, cudaStream_t st);
 int mpo_points_per_cta();
+// consecutive d one MPO thread produces: the stage-4 d padding for the mixed images, 1 for FP64
+int mpo_d_per_thread(int mode);
 // dst[seg.dst_off + sum idx_l dstr_l] = src[seg.src_off + e] for each chunk's range of elements e
 void launch_strided_copy(const double* src, double* dst, const DevCopySeg* segs, const DevChunk* chunks, int n_chunks,
                          cudaStream_t st);

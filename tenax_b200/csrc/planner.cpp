@@ -164,7 +164,8 @@ struct NodeTable {
 
 PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::string& out_subs,
                    const KeyFilter& filter, const std::vector<std::vector<int32_t>>* out_charges,
-                   const std::vector<int32_t>* out_flows) {
+                   const std::vector<int32_t>* out_flows, int k_align) {
+  if (k_align < 1) k_align = 1;
   PairPlan P;
   P.a_subs = A.subs;
   P.b_subs = B.subs;
@@ -217,6 +218,7 @@ PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::stri
 
   DSU dsu;
   NodeTable rn, kn, cn;
+  std::vector<int64_t> k_real;  // unpadded K extent of each kappa node (FLOP count)
   struct Edge {
     int block, r_or_c, k;
   };
@@ -229,15 +231,21 @@ PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::stri
       rk.push_back(A.keys[b][p]);
       rs *= A.dims[b][p];
     }
-    for (int p : a_con) {
+    int64_t ks_img = 1;  // K extent in the image (innermost contracted leg padded)
+    for (size_t i = 0; i < a_con.size(); ++i) {
+      const int p = a_con[i];
       kk.push_back(A.keys[b][p]);
       ks *= A.dims[b][p];
+      const int64_t d = A.dims[b][p];
+      ks_img *= (i + 1 == a_con.size()) ? (d + k_align - 1) / k_align * k_align : d;
     }
     // kappa identity includes the contracted dims (mismatched dims never pair)
     for (int p : a_con) kk.push_back(static_cast<int32_t>(A.dims[b][p]));
     if (rs == 0 || ks == 0) empty = true;
     if (empty) continue;
-    int r = rn.get(rk, rs, dsu), k = kn.get(kk, ks, dsu);
+    int r = rn.get(rk, rs, dsu), k = kn.get(kk, ks_img, dsu);
+    if (static_cast<size_t>(k) >= k_real.size()) k_real.resize(k + 1, 0);
+    k_real[k] = ks;
     dsu.unite(rn.dsu_id[r], kn.dsu_id[k]);
     ea.push_back({static_cast<int>(b), r, k});
   }
@@ -330,13 +338,15 @@ PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::stri
   }
   // pack segments
   auto fill_strides = [](const std::vector<int64_t>& dims, const std::vector<int>& legs_in_order,
-                         int32_t* out_str, int nl) {
+                         int32_t* out_str, int nl, int align = 1) {
     // stride of each leg in the row-major flattening over legs_in_order
+    // (the innermost extent rounded up to a multiple of align)
     for (int l = 0; l < nl; ++l) out_str[l] = 0;
     int64_t s = 1;
     for (int i = static_cast<int>(legs_in_order.size()) - 1; i >= 0; --i) {
       out_str[legs_in_order[i]] = static_cast<int32_t>(s);
-      s *= dims[legs_in_order[i]];
+      const int64_t d = dims[legs_in_order[i]];
+      s *= (i + 1 == static_cast<int>(legs_in_order.size())) ? (d + align - 1) / align * align : d;
     }
   };
   for (auto& e : ea) {
@@ -353,6 +363,7 @@ PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::stri
     for (int l = 0; l < A.nl; ++l) s.dims[l] = static_cast<int32_t>(A.dims[b][l]);
     fill_strides(A.dims[b], a_free, s.rstr, A.nl);
     fill_strides(A.dims[b], a_con, s.kstr, A.nl);
+    fill_strides(A.dims[b], a_con, s.kdstr, A.nl, k_align);
     P.packA.push_back(s);
   }
   for (auto& e : eb) {
@@ -369,6 +380,7 @@ PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::stri
     for (int l = 0; l < B.nl; ++l) s.dims[l] = static_cast<int32_t>(B.dims[b][l]);
     fill_strides(B.dims[b], b_free, s.rstr, B.nl);
     fill_strides(B.dims[b], b_con, s.kstr, B.nl);
+    fill_strides(B.dims[b], b_con, s.kdstr, B.nl, k_align);
     P.packB.push_back(s);
   }
   // contributing (r, c) pairs and flops
@@ -380,7 +392,7 @@ PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::stri
         int r = ea[ia].r_or_c, c = eb[ib].r_or_c;
         present[{r, c}] = static_cast<int>(k_group[k]);
         P.flops += 2.0 * static_cast<double>(rn.size[r]) * static_cast<double>(cn.size[c]) *
-                   static_cast<double>(kn.size[k]);
+                   static_cast<double>(k_real[k]);
       }
   }
   // output blocks
@@ -578,7 +590,10 @@ HeffPlan plan_heff(const TensorStruct& L, const TensorStruct& th, const TensorSt
     for (int l = 0; l < 5; ++l) X3.cdim[l][X3.keys[i][l]] = X3.dims[i][l];
   H.x3 = X3;
   // stage 4: Y[c,s,t,g] = X3[c,s,t,f,d] R[d,f,g]
-  H.s4 = plan_pair(X3, H.R, "cstg", none, nullptr, nullptr);
+  // K = (f, d) with the d extent padded to a multiple of 8: the fused MPO
+  // kernel writes X3 in whole 8-wide K chunks (one 16-byte swizzle unit of a
+  // BF16 image row)
+  H.s4 = plan_pair(X3, H.R, "cstg", none, nullptr, nullptr, kMpoKAlign);
   H.flops_s4 = H.s4.flops;
   H.flops = H.flops_s1 + H.flops_mpo + H.flops_s4;
   // output keys vs theta keys

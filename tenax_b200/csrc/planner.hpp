@@ -14,6 +14,7 @@
 namespace tnx {
 
 constexpr int kMaxLegs = 12;  // legs per tensor (operands, intermediates and outputs)
+constexpr int kMpoKAlign = 8;  // d-extent padding of the H_eff stage-4 K blocks
 
 using Key = std::vector<int32_t>;
 
@@ -71,7 +72,8 @@ struct PackSeg {
   int32_t nlegs;
   int32_t dims[kMaxLegs];
   int32_t rstr[kMaxLegs];
-  int32_t kstr[kMaxLegs];
+  int32_t kstr[kMaxLegs];   // K strides of the contracted legs (unpadded: element order)
+  int32_t kdstr[kMaxLegs];  // K strides in the operand image (the innermost may be padded)
 };
 
 // Copy one output block out of a group's result matrix (M x N, row-major).
@@ -113,9 +115,12 @@ struct KeyFilter {
   std::unordered_map<Key, int, KeyHash> allowed;
 };
 
+// k_align > 1 pads the innermost contracted leg of every K block to a
+// multiple of k_align in the GEMM's K coordinate (zero rows of K), so that a
+// producer can write whole aligned K chunks; FLOP counts stay unpadded.
 PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::string& out_subs,
                    const KeyFilter& filter, const std::vector<std::vector<int32_t>>* out_charges,
-                   const std::vector<int32_t>* out_flows);
+                   const std::vector<int32_t>* out_flows, int k_align = 1);
 
 // ---------------------------------------------------------------------------
 // Two-site H_eff plan: Y[c,s,t,g] = L[a,b,c] th[a,p,q,d] Wl[b,p,s,e] Wr[e,q,t,f] R[d,f,g]
