@@ -131,6 +131,10 @@ int img_mode_of(int precision) {
 
 int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// row length of an H_eff stage-1 result matrix: N rounded up to 4 elements so
+// every row starts 16-byte aligned (FP32) and the epilogue stores float4s
+int64_t x1_ld(int64_t n) { return (n + 3) / 4 * 4; }
+
 // image geometry of one pair plan for one mode
 struct PairGeom {
   std::vector<int64_t> a_tile0, b_tile0;  // per group, in tiles
@@ -998,7 +1002,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
       x1_0[i] = x1_elems;
       th_tiles += hs[i]->g1.b_tiles;
       x3_tiles += hs[i]->g4.a_tiles;
-      for (auto& g : H.s1.groups) x1_elems += g.M * g.N;
+      for (auto& g : H.s1.groups) x1_elems += g.M * x1_ld(g.N);
     }
     b->th_img.alloc(std::max<int64_t>(1, th_tiles) * ig.tile_bytes * split);
     b->x3_img.alloc(std::max<int64_t>(1, x3_tiles) * ig.tile_bytes * split);
@@ -1045,8 +1049,10 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         x.nKt = h->g1.nKt[g];
         x.out_slot = 0;
         x.scale = 1.0;
-        for (int64_t r = 0; r < H.s1.groups[g].M; ++r) R1.push_back(xo + r * H.s1.groups[g].N);
-        xo += H.s1.groups[g].M * H.s1.groups[g].N;
+        const int64_t ld = x1_ld(H.s1.groups[g].N);
+        x.vec_ld = static_cast<int32_t>(ld);
+        for (int64_t r = 0; r < H.s1.groups[g].M; ++r) R1.push_back(xo + r * ld);
+        xo += H.s1.groups[g].M * ld;
         G1.push_back(x);
       }
       std::vector<std::pair<int64_t, DevTile>> tl;
@@ -1097,7 +1103,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         for (size_t k = 0; k < mp.ins.size(); ++k) {
           // one record per input slot (b,p,q): address of its point (c=0, d=0)
           const MpoIn& in = mp.ins[k];
-          const int64_t ld = H.s1.groups[in.g1].N;
+          const int64_t ld = x1_ld(H.s1.groups[in.g1].N);
           const int64_t blk = x1_goff[in.g1] + static_cast<int64_t>(in.row0) * ld + in.col0;
           for (int bb = 0; bb < in.mb; ++bb)
             for (int pp = 0; pp < in.mp; ++pp)

@@ -103,6 +103,9 @@ struct DevGroup {
   int64_t rowoff0;          // index of row 0 in the row-offset table
   int32_t M, N, nKt, out_slot;  // result rows go to out_tab[out_slot] + rowoff[.] + col
   double scale;             // result = scale * sum_k A B (undoes operand range scaling)
+  int32_t vec_ld;           // > 0: every row offset is a multiple of 4 elements and the first
+                            // vec_ld (a multiple of 4, >= N) columns may be written: 16-byte stores
+  int32_t pad;
 };
 
 struct DevTile {

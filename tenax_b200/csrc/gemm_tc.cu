@@ -8,7 +8,7 @@
 //           acc += A_hi B_hi + A_hi B_lo + A_lo B_hi, FP32 accumulation in TMEM.
 //   TF32:   acc += A B with kind::tf32.
 // Warp roles: warp 0 = copy producer, warp 1 = TMEM owner + single-thread MMA
-// issuer, warps 2..5 = epilogue (TMEM -> registers -> global through a
+// issuer, warps 2.. = epilogue warps (TMEM -> registers -> global through a
 // per-row offset table).  Two TMEM accumulators let the epilogue of tile i
 // overlap the MMAs of tile i+1.  Every wait is bounded by a globaltimer
 // deadline; on expiry the kernel raises *err_flag, drains its own copies and
@@ -298,18 +298,52 @@ __global__ void __launch_bounds__(THREADS, 1)
       for (int c0 = c_begin; c0 < c_begin + kColsPerWarp; c0 += 32) {
         uint32_t v[32];
         tmem_ld32(tbase + c0, v);
+        bool done = false;
+        if constexpr (sizeof(OutT) == 4) {
+          if (g.vec_ld > 0) {
+            // 16-byte path: rows of 32 floats, 16-byte chunks XOR-swizzled by
+            // row (conflict-free STS.128 / LDS.128); each lane then stores 4
+            // consecutive columns of row it*4 + lane/8
 #pragma unroll
-        for (int j = 0; j < 32; ++j) stg[lane * kStagePitch + j] = __uint_as_float(v[j]);
-        __syncwarp();
-        const int col = tl.nt * TBN + c0 + lane;
-        const bool col_ok = col < g.N;
-#pragma unroll 4
-        for (int r = 0; r < 32; ++r) {
-          const int64_t ro_r = __shfl_sync(0xffffffffu, ro, r);
-          if (ro_r >= 0 && col_ok)
-            out[ro_r + col] = static_cast<OutT>(stg[r * kStagePitch + lane]) * scale;
+            for (int q = 0; q < 8; ++q)
+              *reinterpret_cast<float4*>(stg + lane * 32 + ((q ^ (lane & 7)) << 2)) =
+                  make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                              __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+            __syncwarp();
+            const int cq = lane & 7;
+            const int col = tl.nt * TBN + c0 + cq * 4;
+            const float fs = static_cast<float>(scale);
+#pragma unroll 2
+            for (int it = 0; it < 8; ++it) {
+              const int r = it * 4 + (lane >> 3);
+              const int64_t ro_r = __shfl_sync(0xffffffffu, ro, r);
+              float4 x = *reinterpret_cast<const float4*>(stg + r * 32 + ((cq ^ (r & 7)) << 2));
+              if (ro_r >= 0 && col < g.vec_ld) {
+                x.x *= fs;
+                x.y *= fs;
+                x.z *= fs;
+                x.w *= fs;
+                *reinterpret_cast<float4*>(reinterpret_cast<float*>(out) + ro_r + col) = x;
+              }
+            }
+            __syncwarp();
+            done = true;
+          }
         }
-        __syncwarp();
+        if (!done) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) stg[lane * kStagePitch + j] = __uint_as_float(v[j]);
+          __syncwarp();
+          const int col = tl.nt * TBN + c0 + lane;
+          const bool col_ok = col < g.N;
+#pragma unroll 4
+          for (int r = 0; r < 32; ++r) {
+            const int64_t ro_r = __shfl_sync(0xffffffffu, ro, r);
+            if (ro_r >= 0 && col_ok)
+              out[ro_r + col] = static_cast<OutT>(stg[r * kStagePitch + lane]) * scale;
+          }
+          __syncwarp();
+        }
       }
       tc_fence_before();
       mbar_arrive(&tempty[acc]);
