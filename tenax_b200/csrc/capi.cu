@@ -965,6 +965,10 @@ struct tnx_heff_batch {
   int64_t th_lo = 0, x3_lo = 0;
   DevMem th_pack, th_chunks;
   int n_th_chunks = 0;
+  // theta by rows (k-major blocks, 8 consecutive k per thread) when every segment qualifies
+  DevMem th_rows, th_row_chunks;
+  int n_th_row_chunks = 0;
+  bool th_by_rows = false;
   DevMem g1, t1, ro1, g4, t4, ro4;
   int n_t1 = 0, n_t4 = 0;
   DevMem mpo_pairs, mpo_slots, mpo_oslots, mpo_terms, mpo_chunks;
@@ -1017,6 +1021,9 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     const int esz = f32 ? 4 : 8;
     std::vector<DevPackSeg> tp;
     std::vector<DevChunk> tc;
+    std::vector<DevRowPackSeg> trs;
+    std::vector<int2> trc;
+    bool rows_ok = true;
     std::vector<DevGroup> G1, G4;
     std::vector<int64_t> R1, R4;
     std::vector<std::pair<int64_t, DevTile>> T1, T4;
@@ -1033,6 +1040,31 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
       PairGeom gth = h->g1;  // b_tile0 relative to this problem
       for (auto& t : gth.b_tile0) t += th_t0[i];
       build_pack(H.s1.packB, gth, false, th_base, b->th_lo, ig.tile_bytes, i, tp, tc);
+      for (const PackSeg& ps : H.s1.packB) {
+        bool ok = ps.nlegs >= 2 && ps.kstr[0] == 1 && ps.rstr[ps.nlegs - 1] == 1 && ps.k0 % kMpoKAlign == 0;
+        for (int l = 1; l < ps.nlegs && ok; ++l) {
+          ok = ps.kstr[l] == 0;
+          if (l + 1 < ps.nlegs) ok = ok && ps.rstr[l] == ps.rstr[l + 1] * ps.dims[l + 1];
+        }
+        if (!ok) {
+          rows_ok = false;
+          continue;
+        }
+        DevRowPackSeg rs{};
+        rs.src_off = ps.src_off;
+        rs.img_addr = th_base + static_cast<uint64_t>(gth.b_tile0[ps.group]) * ig.tile_bytes;
+        rs.lo_off = b->th_lo;
+        rs.row0 = ps.row0;
+        rs.k0 = ps.k0;
+        rs.nKt = gth.nKt[ps.group];
+        rs.kval = ps.dims[0];
+        rs.rows = static_cast<int32_t>(ps.count / ps.dims[0]);
+        rs.src_slot = i;
+        rs.scale = 1.0;
+        const int id = static_cast<int>(trs.size());
+        trs.push_back(rs);
+        for (int r0 = 0; r0 < rs.rows; r0 += 256) trc.push_back(make_int2(id, r0));
+      }
       // stage-1 groups
       std::vector<int64_t> x1_goff;
       int64_t xo = x1_0[i];
@@ -1149,6 +1181,12 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     upload(b->th_pack, tp);
     upload(b->th_chunks, tc);
     b->n_th_chunks = static_cast<int>(tc.size());
+    b->th_by_rows = rows_ok;
+    if (rows_ok) {
+      upload(b->th_rows, trs);
+      upload(b->th_row_chunks, trc);
+      b->n_th_row_chunks = static_cast<int>(trc.size());
+    }
     upload(b->g1, G1);
     upload(b->ro1, R1);
     auto t1 = sorted_tiles(T1);
@@ -1198,8 +1236,12 @@ static void heff_batch_stage(tnx_heff_batch* b, int stage, cudaStream_t st) {
   const bool f32 = b->mode != IMG_F64;
   switch (stage) {
     case 0:
-      launch_pack(b->src_tab.as<uint64_t>(), b->th_pack.as<DevPackSeg>(), b->th_chunks.as<DevChunk>(),
-                  b->n_th_chunks, b->mode, b->skip, st);
+      if (b->th_by_rows)
+        launch_pack_rows(b->src_tab.as<uint64_t>(), b->th_rows.as<DevRowPackSeg>(), b->th_row_chunks.as<int2>(),
+                         b->n_th_row_chunks, b->mode, b->skip, st);
+      else
+        launch_pack(b->src_tab.as<uint64_t>(), b->th_pack.as<DevPackSeg>(), b->th_chunks.as<DevChunk>(),
+                    b->n_th_chunks, b->mode, b->skip, st);
       break;
     case 1:
       if (b->mode == IMG_F64)

@@ -70,6 +70,18 @@ struct DevPackSeg {
   int32_t kdstr[kMaxLegsDev];  // contracted-leg strides in the image's K coordinate
 };
 
+// A block stored k-major with contiguous rows (source offset = k * rows + r,
+// one contracted leg first, free legs after it in row-major order), packed
+// into an image whose K blocks start at multiples of 8: one thread per row
+// writes 8 consecutive k at a time.
+struct DevRowPackSeg {
+  int64_t src_off;    // element offset of the block in src_tab[src_slot]
+  uint64_t img_addr;  // destination group image (tile 0)
+  int64_t lo_off;     // byte offset of the low-part image (BF16 split)
+  int32_t row0, k0, nKt, rows, kval, src_slot;
+  double scale;
+};
+
 struct DevScatSeg {
   int64_t dst_off;
   int64_t src_base;  // element offset of (row0, col0) in the result scratch

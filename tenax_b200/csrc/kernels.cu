@@ -309,6 +309,46 @@ __global__ void __launch_bounds__(kMpoThreads) mpo_apply_point_kernel(
                                              o.k0 + o.k_add + d)) = acc;
 }
 
+// ---------------------------------------------------------------------------
+// row pack: k-major blocks with contiguous rows (theta of the H_eff stage 1)
+// -> operand image, 8 consecutive k per thread and store (see DevRowPackSeg)
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void __launch_bounds__(256) pack_rows_kernel(const uint64_t* __restrict__ src_tab,
+                                                        const DevRowPackSeg* __restrict__ segs,
+                                                        const int2* __restrict__ chunks,
+                                                        const int32_t* __restrict__ skip) {
+  using ValT = typename std::conditional<MODE == IMG_F64, double, float>::type;
+  if (skip && *skip) return;
+  const int2 ch = chunks[blockIdx.x];
+  const DevRowPackSeg s = segs[ch.x];
+  const int r = ch.y + static_cast<int>(threadIdx.x);
+  if (r >= s.rows) return;
+  const double* src = reinterpret_cast<const double*>(src_tab[s.src_slot]) + s.src_off + r;
+  uint8_t* img = reinterpret_cast<uint8_t*>(s.img_addr);
+  const int nkc = (s.kval + kMpoVec - 1) / kMpoVec;
+  for (int kc = 0; kc < nkc; ++kc) {
+    ValT v[kMpoVec];
+#pragma unroll
+    for (int u = 0; u < kMpoVec; ++u) {
+      const int a = kc * kMpoVec + u;
+      v[u] = a < s.kval ? static_cast<ValT>(src[static_cast<int64_t>(a) * s.rows] * s.scale) : ValT(0);
+    }
+    img_store_chunk<MODE>(img, s.lo_off, s.nKt, s.row0 + r, s.k0 + kc * kMpoVec, v);
+  }
+}
+
+void launch_pack_rows(const uint64_t* src_tab, const DevRowPackSeg* segs, const int2* chunks, int n_chunks, int mode,
+                      const int32_t* skip, cudaStream_t st) {
+  if (n_chunks <= 0) return;
+  if (mode == IMG_F64)
+    pack_rows_kernel<IMG_F64><<<n_chunks, 256, 0, st>>>(src_tab, segs, chunks, skip);
+  else if (mode == IMG_BF16)
+    pack_rows_kernel<IMG_BF16><<<n_chunks, 256, 0, st>>>(src_tab, segs, chunks, skip);
+  else
+    pack_rows_kernel<IMG_TF32><<<n_chunks, 256, 0, st>>>(src_tab, segs, chunks, skip);
+}
+
 void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevMpoSlot* islots,
                       const DevMpoOutSlot* oslots, const DevMpoTerm* terms, const int2* chunks, int n_chunks,
                       size_t smem_bytes, const int32_t* skip, cudaStream_t st) {

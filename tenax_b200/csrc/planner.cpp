@@ -507,7 +507,9 @@ HeffPlan plan_heff(const TensorStruct& L, const TensorStruct& th, const TensorSt
     throw PlanError{1, "H_eff operands must have 3,4,4,4,3 legs"};
   KeyFilter none;
   // stage 1: X1[b,c,p,q,d] = L[a,b,c] th[a,p,q,d]
-  H.s1 = plan_pair(H.L, H.th, "bcpqd", none, nullptr, nullptr);
+  // K = a padded to a multiple of 8 per sector: theta is packed by whole
+  // 8-wide K chunks (pack_rows_kernel)
+  H.s1 = plan_pair(H.L, H.th, "bcpqd", none, nullptr, nullptr, kMpoKAlign);
   H.flops_s1 = H.s1.flops;
   // X1 blocks (present (r,c) pairs): r = (qb,qc), c = (qp,qq,qd)
   // stage 2 structure/flops: X2[c,s,e,q,d] = X1[b,c,p,q,d] Wl[b,p,s,e]
