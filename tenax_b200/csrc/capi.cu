@@ -1022,7 +1022,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     std::vector<DevPackSeg> tp;
     std::vector<DevChunk> tc;
     std::vector<DevRowPackSeg> trs;
-    std::vector<int2> trc;
+    std::vector<int4> trc;
     bool rows_ok = true;
     std::vector<DevGroup> G1, G4;
     std::vector<int64_t> R1, R4;
@@ -1063,7 +1063,9 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         rs.scale = 1.0;
         const int id = static_cast<int>(trs.size());
         trs.push_back(rs);
-        for (int r0 = 0; r0 < rs.rows; r0 += 256) trc.push_back(make_int2(id, r0));
+        const int nkc = (rs.kval + kMpoKAlign - 1) / kMpoKAlign, cpt = pack_rows_chunks_per_thread();
+        for (int r0 = 0; r0 < rs.rows; r0 += 256)
+          for (int kc = 0; kc < nkc; kc += cpt) trc.push_back(make_int4(id, r0, kc, 0));
       }
       // stage-1 groups
       std::vector<int64_t> x1_goff;
@@ -1237,7 +1239,7 @@ static void heff_batch_stage(tnx_heff_batch* b, int stage, cudaStream_t st) {
   switch (stage) {
     case 0:
       if (b->th_by_rows)
-        launch_pack_rows(b->src_tab.as<uint64_t>(), b->th_rows.as<DevRowPackSeg>(), b->th_row_chunks.as<int2>(),
+        launch_pack_rows(b->src_tab.as<uint64_t>(), b->th_rows.as<DevRowPackSeg>(), b->th_row_chunks.as<int4>(),
                          b->n_th_row_chunks, b->mode, b->skip, st);
       else
         launch_pack(b->src_tab.as<uint64_t>(), b->th_pack.as<DevPackSeg>(), b->th_chunks.as<DevChunk>(),

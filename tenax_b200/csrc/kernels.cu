@@ -316,29 +316,32 @@ __global__ void __launch_bounds__(kMpoThreads) mpo_apply_point_kernel(
 template <int MODE>
 __global__ void __launch_bounds__(256) pack_rows_kernel(const uint64_t* __restrict__ src_tab,
                                                         const DevRowPackSeg* __restrict__ segs,
-                                                        const int2* __restrict__ chunks,
+                                                        const int4* __restrict__ chunks,
                                                         const int32_t* __restrict__ skip) {
   using ValT = typename std::conditional<MODE == IMG_F64, double, float>::type;
+  constexpr int kChunks = 4;  // K chunks of 8 per thread, all loads issued before the stores
   if (skip && *skip) return;
-  const int2 ch = chunks[blockIdx.x];
+  const int4 ch = chunks[blockIdx.x];  // (segment, first row, first K chunk, -)
   const DevRowPackSeg s = segs[ch.x];
   const int r = ch.y + static_cast<int>(threadIdx.x);
   if (r >= s.rows) return;
   const double* src = reinterpret_cast<const double*>(src_tab[s.src_slot]) + s.src_off + r;
   uint8_t* img = reinterpret_cast<uint8_t*>(s.img_addr);
   const int nkc = (s.kval + kMpoVec - 1) / kMpoVec;
-  for (int kc = 0; kc < nkc; ++kc) {
-    ValT v[kMpoVec];
+  ValT v[kChunks][kMpoVec];
+#pragma unroll
+  for (int j = 0; j < kChunks; ++j)
 #pragma unroll
     for (int u = 0; u < kMpoVec; ++u) {
-      const int a = kc * kMpoVec + u;
-      v[u] = a < s.kval ? static_cast<ValT>(src[static_cast<int64_t>(a) * s.rows] * s.scale) : ValT(0);
+      const int a = (ch.z + j) * kMpoVec + u;
+      v[j][u] = a < s.kval ? static_cast<ValT>(src[static_cast<int64_t>(a) * s.rows] * s.scale) : ValT(0);
     }
-    img_store_chunk<MODE>(img, s.lo_off, s.nKt, s.row0 + r, s.k0 + kc * kMpoVec, v);
-  }
+#pragma unroll
+  for (int j = 0; j < kChunks; ++j)
+    if (ch.z + j < nkc) img_store_chunk<MODE>(img, s.lo_off, s.nKt, s.row0 + r, s.k0 + (ch.z + j) * kMpoVec, v[j]);
 }
 
-void launch_pack_rows(const uint64_t* src_tab, const DevRowPackSeg* segs, const int2* chunks, int n_chunks, int mode,
+void launch_pack_rows(const uint64_t* src_tab, const DevRowPackSeg* segs, const int4* chunks, int n_chunks, int mode,
                       const int32_t* skip, cudaStream_t st) {
   if (n_chunks <= 0) return;
   if (mode == IMG_F64)
@@ -367,6 +370,7 @@ void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevM
 }
 
 int mpo_points_per_cta() { return kMpoThreads; }
+int pack_rows_chunks_per_thread() { return 4; }
 int mpo_d_per_thread(int mode) { return mode == IMG_F64 ? 1 : kMpoVec; }
 
 // ---------------------------------------------------------------------------
