@@ -289,6 +289,49 @@ def energy(A, env, H, d):
     return eh + ev
 
 
+def rdm2x1_2site(A, B, env_A, env_B, d):
+    """Horizontal RDM of a checkerboard cell, A left and B right, left half
+    from A's environment and right half from B's (ipeps.py:1552-1594)."""
+    C1, _, _, C4, T1, _, T3, T4 = env_A
+    _, C2, C3, _, T1b, T2, T3b, _ = env_B
+    ao_A, ao_B = build_double_layer_open(A), build_double_layer_open(B)
+    UL = torch.einsum("ab,buc->auc", C1, T1)
+    LL = torch.einsum("gi,idj->gdj", C4, T3)
+    Lenv = torch.einsum("auc,axg,gdj->ucxdj", UL, T4, LL)
+    UR = torch.einsum("cuf,fg->cug", T1b, C2)
+    LR = torch.einsum("jdk,mk->jdm", T3b, C3)
+    Renv = torch.einsum("cuf,frm,jdm->curjd", UR, T2, LR)
+    L1 = torch.einsum("ucxdj,udxrst->crjst", Lenv, ao_A)
+    R2 = torch.einsum("curjd,udlrtv->cjltv", Renv, ao_B)
+    rdm = torch.einsum("crjst,cjruv->stuv", L1, R2).permute(0, 2, 1, 3)
+    return _finish_rdm(rdm, d)
+
+
+def rdm1x2_2site(A, B, env_A, env_B, d):
+    """Vertical RDM of a checkerboard cell, A top and B bottom
+    (ipeps.py:1597-1642)."""
+    C1, C2, _, _, T1, T2, _, T4 = env_A
+    _, _, C3b, C4b, _, T2b, T3b, T4b = env_B
+    ao_A, ao_B = build_double_layer_open(A), build_double_layer_open(B)
+    top = torch.einsum("ab,buc,ce->aue", C1, T1, C2)
+    row1 = torch.einsum("aue,alf,erg->ulfrg", top, T4, T2)
+    site1 = torch.einsum("ulfrg,udlrst->dfgst", row1, ao_A)
+    T4ao = torch.einsum("fmh,pqmnwx->fhpqnwx", T4b, ao_B)
+    s12 = torch.einsum("abcst,bhaqnwx->chqnstwx", site1, T4ao)
+    s12r = torch.einsum("chqnstwx,cni->hqistwx", s12, T2b)
+    bot = torch.einsum("hj,jqk,ik->hqi", C4b, T3b, C3b)
+    rdm = torch.einsum("hqistwx,hqi->stwx", s12r, bot).permute(0, 2, 1, 3)
+    return _finish_rdm(rdm, d)
+
+
+def energy_2site(A, B, env_A, env_B, H, d):
+    """E_h + E_v of a checkerboard cell (ipeps.py:1645-1662)."""
+    Hr = H.reshape(d, d, d, d)
+    eh = torch.einsum("ijkl,ijkl->", rdm2x1_2site(A, B, env_A, env_B, d), Hr)
+    ev = torch.einsum("ijkl,ijkl->", rdm1x2_2site(A, B, env_A, env_B, d), Hr)
+    return eh + ev
+
+
 def energy_and_grad(A, H, chi, iters, method="qr", warmup=0, projectors=None, checkpoint=False):
     """Energy after ``iters`` CTM sweeps and its gradient in A with the
     projectors held fixed (the stop-gradient semantics of the reference).

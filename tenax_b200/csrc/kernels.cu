@@ -596,12 +596,12 @@ __global__ void renorm_apply_kernel(RenormArgs a, const double* __restrict__ par
   const int t = blockIdx.y;
   const double m = renorm_total(partials + t * kRenormBlocks, true);
   if (blockIdx.x == 0 && threadIdx.x == 0) stat[t] = m;
-  const double inv = 1.0 / (m + eps);
+  const double den = m + eps;  // a true division per element, as x / (max|x| + eps) is written
   const double* __restrict__ x = a.x[t];
   double* __restrict__ y = a.y[t];
   const int64_t n = a.n[t];
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += renorm_stride())
-    y[i] = x[i] * inv;
+    y[i] = x[i] / den;
 }
 
 __global__ void renorm_adj_partial_kernel(RenormArgs a, const double* __restrict__ stat,
@@ -632,15 +632,15 @@ __global__ void renorm_adj_apply_kernel(RenormArgs a, const double* __restrict__
   const double dot = renorm_total(partials + (2 * t) * kRenormBlocks, false);
   const double cnt = renorm_total(partials + (2 * t + 1) * kRenormBlocks, false);
   const double m = stat[t];
-  const double inv = 1.0 / (m + eps);
-  const double w = cnt > 0.0 ? dot * inv * inv / cnt : 0.0;
+  const double den = m + eps;
+  const double w = cnt > 0.0 ? dot / (den * den) / cnt : 0.0;
   const double* __restrict__ x = a.x[t];
   const double* __restrict__ g = a.g[t];
   double* __restrict__ gx = a.y[t];
   const int64_t n = a.n[t];
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n; i += renorm_stride()) {
     const double xi = x[i];
-    double v = g[i] * inv;
+    double v = g[i] / den;
     if (fabs(xi) == m && xi != 0.0) v -= xi > 0.0 ? w : -w;
     gx[i] = v;
   }

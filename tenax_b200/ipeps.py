@@ -379,6 +379,57 @@ def compute_energy_ctm(A, env: CTMEnvironment, hamiltonian_gate, d: int) -> torc
     return eh + ev
 
 
+def rdm2x1_2site(A, B, env_A: CTMEnvironment, env_B: CTMEnvironment, d: int, ao_A=None, ao_B=None):
+    """Horizontal RDM of a checkerboard cell, A left and B right
+    (ipeps.py:1552-1594): the left half from A's corners and edges with A's
+    open double layer, the right half from B's with B's."""
+    C1, _, _, C4, T1, _, T3, T4 = env_A
+    _, C2, C3, _, T1b, T2, T3b, _ = env_B
+    ao_A = build_double_layer_open(A) if ao_A is None else ao_A
+    ao_B = build_double_layer_open(B) if ao_B is None else ao_B
+    UL = contract("ab,buc->auc", C1, T1)
+    LL = contract("gi,idj->gdj", C4, T3)
+    X = contract("auc,axg->ucxg", UL, T4)
+    X = contract("ucxg,udxrst->cgdrst", X, ao_A)
+    L1 = contract("cgdrst,gdj->crjst", X, LL)
+    UR = contract("cuf,fg->cug", T1b, C2)
+    LR = contract("jdk,mk->jdm", T3b, C3)
+    Y = contract("cuf,frm->curm", UR, T2)
+    Y = contract("curm,udlrtv->cmdltv", Y, ao_B)
+    R2 = contract("cmdltv,jdm->cjltv", Y, LR)
+    return _finish_rdm(contract("crjst,cjruv->stuv", L1, R2), d)
+
+
+def rdm1x2_2site(A, B, env_A: CTMEnvironment, env_B: CTMEnvironment, d: int, ao_A=None, ao_B=None):
+    """Vertical RDM of a checkerboard cell, A top and B bottom
+    (ipeps.py:1597-1642)."""
+    C1, C2, _, _, T1, T2, _, T4 = env_A
+    _, _, C3b, C4b, _, T2b, T3b, T4b = env_B
+    ao_A = build_double_layer_open(A) if ao_A is None else ao_A
+    ao_B = build_double_layer_open(B) if ao_B is None else ao_B
+    top = contract("auc,ce->aue", contract("ab,buc->auc", C1, T1), C2)
+    Z = contract("aue,alf->uelf", top, T4)
+    Z = contract("uelf,udlrst->efdrst", Z, ao_A)
+    site1 = contract("efdrst,erg->dfgst", Z, T2)
+    bot = contract("hqk,ik->hqi", contract("hj,jqk->hqk", C4b, T3b), C3b)
+    W = contract("fmh,hqi->fmqi", T4b, bot)
+    W = contract("fmqi,pqmnwx->fipnwx", W, ao_B)
+    site2 = contract("fipnwx,gni->fgpwx", W, T2b)
+    return _finish_rdm(contract("dfgst,fgdwx->stwx", site1, site2), d)
+
+
+def compute_energy_ctm_2site(A, B, env_A: CTMEnvironment, env_B: CTMEnvironment, hamiltonian_gate,
+                             d: int) -> torch.Tensor:
+    """Energy per site of a checkerboard cell, one horizontal and one
+    vertical bond (ipeps.py:1645-1662)."""
+    A, B = _as_site_tensor(A), _as_site_tensor(B)
+    H = torch.as_tensor(hamiltonian_gate, dtype=torch.float64, device=A.device).reshape(d, d, d, d)
+    ao_A, ao_B = build_double_layer_open(A), build_double_layer_open(B)
+    eh = (rdm2x1_2site(A, B, env_A, env_B, d, ao_A, ao_B) * H).sum()
+    ev = (rdm1x2_2site(A, B, env_A, env_B, d, ao_A, ao_B) * H).sum()
+    return eh + ev
+
+
 def energy_and_grad(A, hamiltonian_gate, config: CTMConfig, projectors=None):
     """Energy after ``config`` CTM sweeps and its gradient in A through the
     hand-written adjoint, projectors held fixed (stop-gradient semantics).

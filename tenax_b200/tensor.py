@@ -126,7 +126,13 @@ class SymmetricTensor:
 
     @classmethod
     def from_dense(cls, data, indices, tol: float = 1e-12) -> "SymmetricTensor":
-        """Extract the valid sectors of a dense array (core/tensor.py:670-732)."""
+        """Extract the valid sectors of a dense array (core/tensor.py:670-732).
+
+        Every valid key whose legs all have basis states gets a block (zero
+        blocks included).  A CUDA tensor is cut on the device by index
+        gathers; host arrays are cut on the host and copied once."""
+        if isinstance(data, torch.Tensor) and data.is_cuda:
+            return cls._from_dense_device(data, tuple(indices), tol)
         arr = data.detach().cpu().numpy() if isinstance(data, torch.Tensor) else np.asarray(data)
         if arr.shape != tuple(i.dim for i in indices):
             raise ValueError(f"data.shape {arr.shape} does not match index dims {tuple(i.dim for i in indices)}")
@@ -146,6 +152,31 @@ class SymmetricTensor:
                 raise ValueError(f"data has {int(np.sum(np.abs(outside) > tol))} non-zero elements outside "
                                  f"symmetry-allowed sectors (max abs value: {np.max(np.abs(outside)):.3e})")
         return cls(blocks, indices)
+
+    @classmethod
+    def _from_dense_device(cls, x: torch.Tensor, indices, tol: float) -> "SymmetricTensor":
+        if tuple(x.shape) != tuple(i.dim for i in indices):
+            raise ValueError(f"data.shape {tuple(x.shape)} does not match index dims {tuple(i.dim for i in indices)}")
+        x = x.detach().to(dtype=torch.float64)
+        keys, parts = [], []
+        mask = torch.zeros(x.shape, dtype=torch.bool, device=x.device) if tol != float("inf") else None
+        for k in sorted(compute_valid_blocks(indices)):
+            pos = [np.flatnonzero(i.charges == q) for i, q in zip(indices, k)]
+            if not all(len(p) for p in pos):
+                continue
+            grid = torch.meshgrid(*[torch.as_tensor(p, device=x.device) for p in pos], indexing="ij")
+            parts.append(x[grid].reshape(-1))
+            keys.append(tuple(int(q) for q in k))
+            if mask is not None:
+                mask[grid] = True
+        if mask is not None:
+            outside = x[~mask].abs()
+            n_bad = int((outside > tol).sum())
+            if n_bad:
+                raise ValueError(f"data has {n_bad} non-zero elements outside symmetry-allowed sectors "
+                                 f"(max abs value: {float(outside.max()):.3e})")
+        data = torch.cat(parts) if parts else torch.zeros(0, dtype=torch.float64, device=x.device)
+        return cls.from_flat(indices, keys, data)
 
     # ------------------------------------------------------------ accessors
     @property

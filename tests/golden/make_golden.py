@@ -398,6 +398,98 @@ def gen_split_ctm(M):
         json.dump(meta, fh, indent=1)
 
 
+def gen_ctm_tensor(M):
+    """Block-sparse standard CTMRG (algorithms/_ctm_tensor.py): every
+    projector the reference computed (the dense P recorded at its
+    stop_gradient call, in call order), the final environments as
+    block-sparse tensors (keys + data) and the energy from
+    compute_energy_ctm_tensor; one checkerboard (2-site) case with
+    compute_energy_ctm_tensor_2site.
+
+    Site legs (u, d, l, r, phys) with flows (OUT, IN, OUT, IN, IN), N(0,1)
+    blocks in sorted-key order.  Trivial-charge cases carry values; on the
+    U(1) and Z2 cases the reference's trivial chi_new charges keep only the
+    fused charge-0 rows of each projector and the environment is exactly
+    zero after the first sweep (the fixture records its block structure).
+    Charges whose grown corners differ in sector height make the
+    reference's per-sector reshape fail; that case records the error."""
+    ct = M["tenax.algorithms._ctm_tensor"]
+    core = M["tenax.core.tensor"]
+    sz = np.array([[0.5, 0.0], [0.0, -0.5]])
+    sp = np.array([[0.0, 1.0], [0.0, 0.0]])
+    H = (np.kron(sz, sz) + 0.5 * np.kron(sp, sp.T) + 0.5 * np.kron(sp.T, sp)).reshape(2, 2, 2, 2)
+    # (name, bond charges, phys charges, modulus, chi, sweeps, method, warm-up, seed, DenseTensor input)
+    cases = [("triv_d2_chi6", [0, 0], [0, 0], None, 6, 3, "eigh", 0, 44, False),
+             ("triv_d3_chi10", [0, 0, 0], [0, 0], None, 10, 2, "eigh", 0, 45, False),
+             ("triv_d2_chi5_qr", [0, 0], [0, 0], None, 5, 4, "qr", 2, 46, False),
+             ("dense_d2_chi6", [0, 0], [0, 0], None, 6, 3, "eigh", 0, 47, True),
+             ("dense_d2_chi4_qr", [0, 0], [0, 0], None, 4, 3, "qr", 1, 48, True),
+             ("u1_d3_chi8", [-1, 0, 1], [-1, 1], None, 8, 2, "eigh", 0, 41, False),
+             ("z2_d3_chi6", [0, 0, 1], [0, 1], 2, 6, 2, "eigh", 0, 7, False),
+             ("u1_d2_chi6_err", [0, 1], [0, 1], None, 6, 1, "eigh", 0, 7, False)]
+    arrays, meta = {"H": H}, {}
+    for name, bond, phys, mod, chi, iters, method, warm, seed, dense in cases:
+        rng = np.random.default_rng(seed)
+        legs = [(bond, -1, "u"), (bond, 1, "d"), (bond, -1, "l"), (bond, 1, "r"), (phys, 1, "phys")]
+        A = make_sym_tensor(M, legs, rng, modulus=mod)
+        arrays.update(dump_tensor(f"{name}.A", A, mod))
+        A_in = core.DenseTensor(A.todense(), A.indices) if dense else A
+        sg = []
+        _jax_standin.record_stop_gradient(sg)
+        t0 = time.time()
+        entry = {"bond_charges": bond, "phys_charges": phys, "modulus": mod, "chi": chi, "iters": iters,
+                 "method": method, "warmup": warm, "seed": seed, "dense": dense}
+        try:
+            env = ct.ctm_tensor(A_in, chi, max_iter=iters, conv_tol=0.0, projector_method=method,
+                                qr_warmup_steps=warm)
+        except ValueError as e:
+            _jax_standin.record_stop_gradient(None)
+            entry["error"] = str(e)
+            entry["n_projectors_before_error"] = len(sg)
+            meta[name] = entry
+            print(f"ctm_tensor {name}: ValueError {e}", flush=True)
+            continue
+        _jax_standin.record_stop_gradient(None)
+        E = float(ct.compute_energy_ctm_tensor(A_in, env, H, 2))
+        assert len(sg) == 4 * iters, (name, len(sg))
+        for i, P in enumerate(sg):
+            arrays[f"{name}.P{i}"] = np.asarray(P, dtype=np.float64)
+        for f in env._fields:
+            x = getattr(env, f)
+            if dense:
+                arrays[f"{name}.{f}"] = np.asarray(x.todense(), dtype=np.float64)
+            else:
+                arrays.update(dump_tensor(f"{name}.{f}", x, mod))
+        entry["energy"] = E
+        meta[name] = entry
+        print(f"ctm_tensor {name}: E={E:.15f} ({time.time() - t0:.1f} s)", flush=True)
+
+    # checkerboard cell, trivial charges
+    name, chi, iters = "cb_d2_chi6", 6, 2
+    sites = []
+    for s, seed in (("A", 99), ("B", 200)):
+        rng = np.random.default_rng(seed)
+        legs = [([0, 0], -1, "u"), ([0, 0], 1, "d"), ([0, 0], -1, "l"), ([0, 0], 1, "r"), ([0, 0], 1, "phys")]
+        sites.append(make_sym_tensor(M, legs, rng))
+        arrays.update(dump_tensor(f"{name}.{s}", sites[-1]))
+    sg = []
+    _jax_standin.record_stop_gradient(sg)
+    env_A, env_B = ct.ctm_tensor_2site(sites[0], sites[1], chi, max_iter=iters, conv_tol=0.0)
+    _jax_standin.record_stop_gradient(None)
+    E = float(ct.compute_energy_ctm_tensor_2site(sites[0], sites[1], env_A, env_B, H, 2))
+    assert len(sg) == 8 * iters, len(sg)
+    for i, P in enumerate(sg):
+        arrays[f"{name}.P{i}"] = np.asarray(P, dtype=np.float64)
+    for s, env in (("A", env_A), ("B", env_B)):
+        for f in env._fields:
+            arrays.update(dump_tensor(f"{name}.env{s}.{f}", getattr(env, f)))
+    meta[name] = {"chi": chi, "iters": iters, "seeds": [99, 200], "energy": E}
+    print(f"ctm_tensor {name}: E={E:.15f}", flush=True)
+    np.savez_compressed(os.path.join(HERE, "ctm_tensor.npz"), **arrays)
+    with open(os.path.join(HERE, "ctm_tensor.json"), "w") as fh:
+        json.dump(meta, fh, indent=1)
+
+
 def gen_ctm(M):
     """Dense 1-site CTMRG (algorithms/ipeps.py): environments, corner
     singular values and NN Heisenberg energies from the reference's own
@@ -463,10 +555,11 @@ def main():
         "tenax.core.symmetry", "tenax.core.index", "tenax.core.tensor", "tenax.linalg",
         "tenax.contraction.contractor", "tenax.network.network", "tenax.algorithms._tensor_utils",
         "tenax.algorithms.auto_mpo", "tenax.algorithms.dmrg", "tenax.algorithms.ipeps",
-        "tenax.algorithms._split_ctm_tensor",
+        "tenax.algorithms._split_ctm_tensor", "tenax.algorithms._ctm_tensor",
     ])
     mods["cfg"] = mods["tenax.algorithms.dmrg"].DMRGConfig
-    todo = args.only.split(",") if args.only else ["valid", "contract", "pieces", "mpo", "c1", "ctm", "fuse", "split"]
+    todo = args.only.split(",") if args.only else ["valid", "contract", "pieces", "mpo", "c1", "ctm", "fuse", "split",
+                                                       "ctm_tensor"]
     if "valid" in todo:
         gen_valid_blocks(mods)
     if "contract" in todo:
@@ -483,6 +576,8 @@ def main():
         gen_fuse(mods)
     if "split" in todo:
         gen_split_ctm(mods)
+    if "ctm_tensor" in todo:
+        gen_ctm_tensor(mods)
 
 
 if __name__ == "__main__":
