@@ -898,6 +898,13 @@ int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const
     const int mode = img_mode_of(precision);
     const ImgGeom ig = img_geom(mode);
     const int split = mode == IMG_BF16 ? 2 : 1;
+    // the mixed paths read X1 in FP32 with 32-byte vector loads: every d range
+    // of the stage-1 result starts on a multiple of 8 columns
+    const int want_align = mode == IMG_F64 ? 1 : kMpoKAlign;
+    if (H.x1_align != want_align) {
+      const TensorStruct tL = H.L, tT = H.th, tWl = H.Wl, tWr = H.Wr, tR = H.R;
+      H = plan_heff(tL, tT, tWl, tWr, tR, want_align);
+    }
     // W data to host for the fused MPO terms
     std::vector<double> wl(H.Wl.total), wr(H.Wr.total);
     if (H.Wl.total) CUDA_OK(cudaMemcpyAsync(wl.data(), Wl, H.Wl.total * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1041,10 +1048,13 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
       for (auto& t : gth.b_tile0) t += th_t0[i];
       build_pack(H.s1.packB, gth, false, th_base, b->th_lo, ig.tile_bytes, i, tp, tc);
       for (const PackSeg& ps : H.s1.packB) {
-        bool ok = ps.nlegs >= 2 && ps.kstr[0] == 1 && ps.rstr[ps.nlegs - 1] == 1 && ps.k0 % kMpoKAlign == 0;
-        for (int l = 1; l < ps.nlegs && ok; ++l) {
-          ok = ps.kstr[l] == 0;
-          if (l + 1 < ps.nlegs) ok = ok && ps.rstr[l] == ps.rstr[l + 1] * ps.dims[l + 1];
+        // eligible: leg 0 is the only contracted leg and the free legs (1..)
+        // map to consecutive image rows (legs of extent 1 carry no stride)
+        bool ok = ps.nlegs >= 2 && ps.kstr[0] == 1 && ps.k0 % kMpoKAlign == 0;
+        int64_t expect = 1;
+        for (int l = ps.nlegs - 1; l >= 1 && ok; --l) {
+          ok = ps.kstr[l] == 0 && (ps.dims[l] == 1 || ps.rstr[l] == expect);
+          expect *= ps.dims[l];
         }
         if (!ok) {
           rows_ok = false;
@@ -1134,6 +1144,8 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         b->mpo_smem = std::max<size_t>(b->mpo_smem, mp.terms.size() * sizeof(DevMpoTerm) +
                                                        mp.n_in_slots * sizeof(DevMpoSlot) +
                                                        mp.n_out_slots * sizeof(DevMpoOutSlot));
+        // X1 columns of one (p,q) slot: its d range padded to H.x1_align
+        const int64_t md_x1 = (mp.md + H.x1_align - 1) / H.x1_align * H.x1_align;
         for (size_t k = 0; k < mp.ins.size(); ++k) {
           // one record per input slot (b,p,q): address of its point (c=0, d=0)
           const MpoIn& in = mp.ins[k];
@@ -1144,9 +1156,12 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
               for (int qq = 0; qq < in.mq; ++qq) {
                 DevMpoSlot sl{};
                 sl.base = x1_base + static_cast<uint64_t>(blk + static_cast<int64_t>(bb) * mp.mc * ld +
-                                                          static_cast<int64_t>(pp * in.mq + qq) * mp.md) *
+                                                          static_cast<int64_t>(pp * in.mq + qq) * md_x1) *
                                         esz;
                 sl.ld = ld;
+                // the FP32 MPO kernel loads 8 consecutive d (padding included) with 16-byte loads
+                if (f32 && (H.x1_align != kMpoKAlign || sl.base % 32 != 0 || ld % 8 != 0))
+                  return set_err(TNX_ERR_RUNTIME, "internal: X1 slot not aligned for the vector MPO loads");
                 MI.push_back(sl);
               }
         }

@@ -142,13 +142,14 @@ void launch_zero_ranges(const uint64_t* out_tab, const DevChunk* chunks, int n_c
 // Wlr is very sparse (an MPO is mostly pass-through states), so each output
 // slot (s,t,f) is a short sum of scaled input slots (b,p,q): the kernel walks
 // the pair's terms, sorted by output slot and staged in shared memory with the
-// input- and output-slot tables.  One thread owns kMpoVec consecutive d of one
-// point row c: the stage-4 K layout pads every d range to a multiple of
-// kMpoVec, so the thread's outputs of one slot form one aligned K chunk -- a
-// single 16-byte swizzle unit of a BF16 image row (two for TF32, four double2
-// stores for FP64) -- and the table reads and image addressing are paid once
-// per chunk instead of once per element.  kMpoTerms terms' loads are kept in
-// flight per thread.
+// input- and output-slot tables.  Mixed paths (FP32 stage-1 results): one
+// thread owns kMpoVec consecutive d of one point row c; the stage-1 N layout
+// and the stage-4 K layout both pad every d range to a multiple of kMpoVec, so
+// the thread reads each term's 8 values with two aligned 16-byte loads and its
+// outputs of one slot form one aligned K chunk -- a single 16-byte swizzle
+// unit of a BF16 image row (two for TF32) -- and the table reads and image
+// addressing are paid once per chunk instead of once per element.  kMpoTerms
+// terms' loads are kept in flight per thread.  FP64 uses the per-point kernel.
 // ---------------------------------------------------------------------------
 constexpr int kMpoThreads = 256;
 constexpr int kMpoVec = 8;
@@ -191,13 +192,15 @@ __device__ __forceinline__ void img_store_chunk(uint8_t* img, int64_t lo_offset,
   }
 }
 
-template <typename TI, int MODE>
+template <int MODE>
 __global__ void __launch_bounds__(kMpoThreads) mpo_apply_kernel(
     const DevMpoPair* __restrict__ pairs, const DevMpoSlot* __restrict__ islots,
     const DevMpoOutSlot* __restrict__ oslots, const DevMpoTerm* __restrict__ terms,
     const int2* __restrict__ chunks, const int32_t* __restrict__ skip) {
-  // FP64 images accumulate in double; the FP32-input mixed paths in float
-  using AccT = typename std::conditional<MODE == IMG_F64, double, float>::type;
+  // FP32 stage-1 results: every input slot's d range starts on a 32-byte
+  // boundary and is padded to a multiple of kMpoVec with zero columns (the
+  // planner's N padding), so a thread's 8 d of one term are two aligned
+  // 16-byte loads and need no bounds mask
   if (skip && *skip) return;
   extern __shared__ __align__(16) unsigned char mpo_smem[];
   const int2 ch = chunks[blockIdx.x];
@@ -214,25 +217,25 @@ __global__ void __launch_bounds__(kMpoThreads) mpo_apply_kernel(
   if (p >= pr.mc * nchunk || pr.n_terms == 0) return;
   const int64_t c = p / nchunk;
   const int d0 = (p - static_cast<int>(c) * nchunk) * kMpoVec;
-  const int dn = min(kMpoVec, pr.md - d0);  // valid d of this chunk; the rest are padding zeros
-  AccT acc[kMpoVec];
+  float acc[kMpoVec];
 #pragma unroll
-  for (int u = 0; u < kMpoVec; ++u) acc[u] = AccT(0);
-  // FP64 chunks hold twice the registers: fewer terms in flight keeps occupancy
-  constexpr int kTerms = MODE == IMG_F64 ? 2 : kMpoTerms;
+  for (int u = 0; u < kMpoVec; ++u) acc[u] = 0.0f;
   int cur = st[0].out_slot;
-  for (int t0 = 0; t0 < pr.n_terms; t0 += kTerms) {
-    TI xv[kTerms][kMpoVec];
+  for (int t0 = 0; t0 < pr.n_terms; t0 += kMpoTerms) {
+    float4 xv[kMpoTerms][2];
 #pragma unroll
-    for (int j = 0; j < kTerms; ++j) {
-      const bool live = t0 + j < pr.n_terms;
-      const DevMpoSlot sl = si[live ? st[t0 + j].in_slot : 0];
-      const TI* src = reinterpret_cast<const TI*>(sl.base) + c * sl.ld + d0;
-#pragma unroll
-      for (int u = 0; u < kMpoVec; ++u) xv[j][u] = (live && u < dn) ? src[u] : TI(0);
+    for (int j = 0; j < kMpoTerms; ++j) {
+      if (t0 + j < pr.n_terms) {
+        const DevMpoSlot sl = si[st[t0 + j].in_slot];
+        const float4* src = reinterpret_cast<const float4*>(reinterpret_cast<const float*>(sl.base) + c * sl.ld + d0);
+        xv[j][0] = __ldg(src);
+        xv[j][1] = __ldg(src + 1);
+      } else {
+        xv[j][0] = xv[j][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
     }
 #pragma unroll
-    for (int j = 0; j < kTerms; ++j) {
+    for (int j = 0; j < kMpoTerms; ++j) {
       if (t0 + j >= pr.n_terms) break;
       const DevMpoTerm tm = st[t0 + j];
       if (tm.out_slot != cur) {
@@ -241,11 +244,17 @@ __global__ void __launch_bounds__(kMpoThreads) mpo_apply_kernel(
                               o.row0 + c * o.rows_per_c + o.row_add, o.k0 + o.k_add + d0, acc);
         cur = tm.out_slot;
 #pragma unroll
-        for (int u = 0; u < kMpoVec; ++u) acc[u] = AccT(0);
+        for (int u = 0; u < kMpoVec; ++u) acc[u] = 0.0f;
       }
-      const AccT w = static_cast<AccT>(tm.w);
-#pragma unroll
-      for (int u = 0; u < kMpoVec; ++u) acc[u] += w * static_cast<AccT>(xv[j][u]);
+      const float w = static_cast<float>(tm.w);
+      acc[0] += w * xv[j][0].x;
+      acc[1] += w * xv[j][0].y;
+      acc[2] += w * xv[j][0].z;
+      acc[3] += w * xv[j][0].w;
+      acc[4] += w * xv[j][1].x;
+      acc[5] += w * xv[j][1].y;
+      acc[6] += w * xv[j][1].z;
+      acc[7] += w * xv[j][1].w;
     }
   }
   const DevMpoOutSlot o = so[cur];
@@ -364,9 +373,9 @@ void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevM
   if (!x1_f32)
     go(mpo_apply_point_kernel);
   else if (mode == IMG_BF16)
-    go(mpo_apply_kernel<float, IMG_BF16>);
+    go(mpo_apply_kernel<IMG_BF16>);
   else
-    go(mpo_apply_kernel<float, IMG_TF32>);
+    go(mpo_apply_kernel<IMG_TF32>);
 }
 
 int mpo_points_per_cta() { return kMpoThreads; }

@@ -164,8 +164,9 @@ struct NodeTable {
 
 PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::string& out_subs,
                    const KeyFilter& filter, const std::vector<std::vector<int32_t>>* out_charges,
-                   const std::vector<int32_t>* out_flows, int k_align) {
+                   const std::vector<int32_t>* out_flows, int k_align, int n_align) {
   if (k_align < 1) k_align = 1;
+  if (n_align < 1) n_align = 1;
   PairPlan P;
   P.a_subs = A.subs;
   P.b_subs = B.subs;
@@ -218,7 +219,7 @@ PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::stri
 
   DSU dsu;
   NodeTable rn, kn, cn;
-  std::vector<int64_t> k_real;  // unpadded K extent of each kappa node (FLOP count)
+  std::vector<int64_t> k_real, c_real;  // unpadded K / column extents of each node (FLOP count)
   struct Edge {
     int block, r_or_c, k;
   };
@@ -251,10 +252,13 @@ PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::stri
   }
   for (size_t b = 0; b < B.keys.size(); ++b) {
     Key ck, kk;
-    int64_t cs = 1, ks = 1;
-    for (int p : b_free) {
+    int64_t cs = 1, ks = 1, cs_img = 1;  // cs_img: column extent with the innermost free leg padded
+    for (size_t i = 0; i < b_free.size(); ++i) {
+      const int p = b_free[i];
       ck.push_back(B.keys[b][p]);
       cs *= B.dims[b][p];
+      const int64_t d = B.dims[b][p];
+      cs_img *= (i + 1 == b_free.size()) ? (d + n_align - 1) / n_align * n_align : d;
     }
     for (int p : b_con) {
       kk.push_back(B.keys[b][p]);
@@ -264,7 +268,9 @@ PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::stri
     if (cs == 0 || ks == 0) continue;
     auto it = kn.idx.find(kk);
     if (it == kn.idx.end()) continue;  // no A block shares this contracted tuple
-    int c = cn.get(ck, cs, dsu);
+    int c = cn.get(ck, cs_img, dsu);
+    if (static_cast<size_t>(c) >= c_real.size()) c_real.resize(c + 1, 0);
+    c_real[c] = cs;
     dsu.unite(cn.dsu_id[c], kn.dsu_id[it->second]);
     eb.push_back({static_cast<int>(b), c, it->second});
   }
@@ -378,7 +384,7 @@ PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::stri
     s.k0 = static_cast<int32_t>(k_start[e.k]);
     s.nlegs = B.nl;
     for (int l = 0; l < B.nl; ++l) s.dims[l] = static_cast<int32_t>(B.dims[b][l]);
-    fill_strides(B.dims[b], b_free, s.rstr, B.nl);
+    fill_strides(B.dims[b], b_free, s.rstr, B.nl, n_align);
     fill_strides(B.dims[b], b_con, s.kstr, B.nl);
     fill_strides(B.dims[b], b_con, s.kdstr, B.nl, k_align);
     P.packB.push_back(s);
@@ -391,7 +397,7 @@ PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::stri
       for (int ib : b_by_k[k]) {
         int r = ea[ia].r_or_c, c = eb[ib].r_or_c;
         present[{r, c}] = static_cast<int>(k_group[k]);
-        P.flops += 2.0 * static_cast<double>(rn.size[r]) * static_cast<double>(cn.size[c]) *
+        P.flops += 2.0 * static_cast<double>(rn.size[r]) * static_cast<double>(c_real[c]) *
                    static_cast<double>(k_real[k]);
       }
   }
@@ -464,7 +470,7 @@ PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::stri
     acc = 1;
     for (int i = static_cast<int>(fb.size()) - 1; i >= 0; --i) {
       sb[i] = acc;
-      acc *= fb[i];
+      acc *= (i + 1 == static_cast<int>(fb.size())) ? (fb[i] + n_align - 1) / n_align * n_align : fb[i];
     }
     for (size_t i = 0; i < olegs.size(); ++i) {
       s.dims[i] = static_cast<int32_t>(d[i]);
@@ -491,8 +497,9 @@ static TensorStruct sub_struct(const std::string& subs, int nl) {
 }
 
 HeffPlan plan_heff(const TensorStruct& L, const TensorStruct& th, const TensorStruct& Wl, const TensorStruct& Wr,
-                   const TensorStruct& R) {
+                   const TensorStruct& R, int x1_align) {
   HeffPlan H;
+  H.x1_align = x1_align < 1 ? 1 : x1_align;
   H.L = L;
   H.th = th;
   H.Wl = Wl;
@@ -509,7 +516,9 @@ HeffPlan plan_heff(const TensorStruct& L, const TensorStruct& th, const TensorSt
   // stage 1: X1[b,c,p,q,d] = L[a,b,c] th[a,p,q,d]
   // K = a padded to a multiple of 8 per sector: theta is packed by whole
   // 8-wide K chunks (pack_rows_kernel)
-  H.s1 = plan_pair(H.L, H.th, "bcpqd", none, nullptr, nullptr, kMpoKAlign);
+  // N = (p,q,d) with d padded to a multiple of x1_align: every MPO input
+  // slot of X1 starts on an aligned column (vector loads in the MPO kernel)
+  H.s1 = plan_pair(H.L, H.th, "bcpqd", none, nullptr, nullptr, kMpoKAlign, H.x1_align);
   H.flops_s1 = H.s1.flops;
   // X1 blocks (present (r,c) pairs): r = (qb,qc), c = (qp,qq,qd)
   // stage 2 structure/flops: X2[c,s,e,q,d] = X1[b,c,p,q,d] Wl[b,p,s,e]

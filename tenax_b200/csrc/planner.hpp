@@ -117,10 +117,13 @@ struct KeyFilter {
 
 // k_align > 1 pads the innermost contracted leg of every K block to a
 // multiple of k_align in the GEMM's K coordinate (zero rows of K), so that a
-// producer can write whole aligned K chunks; FLOP counts stay unpadded.
+// producer can write whole aligned K chunks.  n_align > 1 pads the innermost
+// free leg of B in the GEMM's N coordinate the same way (zero rows of the B
+// image, zero result columns), so that every result slot starts on an
+// aligned column.  FLOP counts stay unpadded.
 PairPlan plan_pair(const TensorStruct& A, const TensorStruct& B, const std::string& out_subs,
                    const KeyFilter& filter, const std::vector<std::vector<int32_t>>* out_charges,
-                   const std::vector<int32_t>* out_flows, int k_align = 1);
+                   const std::vector<int32_t>* out_flows, int k_align = 1, int n_align = 1);
 
 // ---------------------------------------------------------------------------
 // Two-site H_eff plan: Y[c,s,t,g] = L[a,b,c] th[a,p,q,d] Wl[b,p,s,e] Wr[e,q,t,f] R[d,f,g]
@@ -153,6 +156,7 @@ struct MpoPair {
 
 struct HeffPlan {
   TensorStruct L, th, Wl, Wr, R;
+  int x1_align = 1;             // stage-1 result columns: each d range padded to a multiple of this
   PairPlan s1;                  // L (x) theta over a -> X1 group matrices
   PairPlan s4;                  // X3 (x) R over (f,d) -> Y
   TensorStruct x3;              // structure of X3[c,s,t,f,d]
@@ -171,7 +175,7 @@ struct HeffPlan {
 };
 
 HeffPlan plan_heff(const TensorStruct& L, const TensorStruct& th, const TensorStruct& Wl, const TensorStruct& Wr,
-                   const TensorStruct& R);
+                   const TensorStruct& R, int x1_align = 1);
 // Fill the MPO terms (W_l W_r contracted over e) from host copies of the
 // W_l / W_r block buffers.
 void heff_mpo_terms(HeffPlan& p, const std::vector<double>& wl, const std::vector<double>& wr);
