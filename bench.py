@@ -183,24 +183,28 @@ def run_ours(args):
         res = {"ms": ms, "flops": flops, "stage_ms": stage_ms, "stage_flops": tot_sf.tolist(), "err": err,
                "per_problem_flops": [o.flops for o in ops], "launches": batch.launches_per_apply}
         if with_e2e:
-            host_in = torch.empty(int(offs[-1]), dtype=torch.float64, pin_memory=True)
-            host_out = torch.empty(int(offs[-1]), dtype=torch.float64, pin_memory=True)
-            host_in.copy_(x_all.cpu())
-            for _ in range(args.warmup):
-                x_all.copy_(host_in, non_blocking=True)
-                batch.apply(xs, ys)
-                host_out.copy_(y_all, non_blocking=True)
+            # end to end through HeffBatch.apply_host: every step copies its
+            # inputs in from pinned host memory and its outputs back; step
+            # s+1's copy in and step s-1's copy out overlap step s's compute
+            assert batch.total == int(offs[-1])
+            host_in = [torch.empty(batch.total, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+            host_out = [torch.empty(batch.total, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+            for h in host_in:
+                h.copy_(x_all.cpu())
+            batch.apply_host([host_in[i % 2] for i in range(args.warmup)],
+                             [host_out[i % 2] for i in range(args.warmup)])
             barrier()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(st)
-            for _ in range(args.steps):
-                x_all.copy_(host_in, non_blocking=True)
-                batch.apply(xs, ys)
-                host_out.copy_(y_all, non_blocking=True)
+            batch.apply_host([host_in[i % 2] for i in range(args.steps)],
+                             [host_out[i % 2] for i in range(args.steps)])
             b.record(st)
             barrier()
             res["e2e_ms"] = max_over_ranks(a.elapsed_time(b) / args.steps)
             res["e2e_bytes"] = int(offs[-1]) * 8
+            batch.apply(xs, ys)
+            torch.cuda.synchronize()
+            res["e2e_max_abs_diff_vs_device"] = float((host_out[(args.steps - 1) % 2] - y_all.cpu()).abs().max())
         del batch, ops, x_all, y_all, xs, ys
         torch.cuda.empty_cache()
         return res
@@ -239,12 +243,15 @@ def run_ours(args):
             "mixed_over_fp64": round(value / fp64_value, 3),
             "stage_ms": [round(x, 4) for x in st_ms],
             "stage_names": ["pack theta", "stage-1 GEMM L.theta", "fused MPO (W_l W_r)", "stage-4 GEMM .R"],
-            "roofline": {"bound": "tensor", "kernel": f"stage{dom} tcgen05 grouped GEMM", "achieved":
+            "roofline": {"bound": "tensor", "kernel": f"{STAGE_GEMM[dom]} tcgen05 grouped GEMM", "achieved":
                          round(achieved, 2), "peak": round(peak, 1), "unit": "TFLOP/s",
                          "frac": round(achieved / peak, 4), "peak_source": f"{peak_src} bf16 burst"
                          + (" / 3 (three products)" if split == 3 else " / 2 (tf32)"), "traffic": traffic},
             "e2e": {"value": round(flops_all / (rmx["e2e_ms"] * 1e-3) / 1e12, 3), "unit": "TFLOP/s",
-                    "h2d_bytes_per_step": rmx["e2e_bytes"], "d2h_bytes_per_step": rmx["e2e_bytes"]},
+                    "h2d_bytes_per_step": rmx["e2e_bytes"], "d2h_bytes_per_step": rmx["e2e_bytes"],
+                    "ms_per_step": round(rmx["e2e_ms"], 4), "api": "HeffBatch.apply_host (pinned host buffers; "
+                    "step s+1 copied in and step s-1 copied out while step s computes)",
+                    "max_abs_diff_vs_device_apply": rmx["e2e_max_abs_diff_vs_device"]},
             "gpu_launches": rmx["launches"] * args.steps,
             "device_error_flag": rmx["err"],
             "clocks": clocks,
@@ -265,6 +272,9 @@ def _host_problem(p):
         return OTensor(tuple(Leg(i.charges, int(i.flow), i.label) for i in t.indices), t.numpy_blocks())
 
     return [h(t) for t in (p.L, p.theta, p.Wl, p.Wr, p.R)]
+
+
+STAGE_GEMM = {1: "stage-1 (L.theta)", 3: "stage-4 (.R)"}
 
 
 def cpu_baseline(problems, flops, budget_s=15.0):

@@ -129,6 +129,18 @@ void tnx_heff_destroy(tnx_heff* h);
  * (persistent grouped GEMMs over all sectors of all problems). */
 int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx_heff_batch** b);
 int tnx_heff_batch_apply(tnx_heff_batch* b, const double* const* thetas, double* const* outs, void* stream);
+/* Host-resident streaming: n_steps independent applications whose inputs and
+ * outputs live in host memory (pinned for overlap).  host_in[s] / host_out[s]
+ * hold all problems' theta buffers concatenated in batch order (offsets from
+ * tnx_heff_batch_size).  Step s+1's copy in and step s-1's copy out run on
+ * their own streams while step s computes; the call's work on `stream`
+ * completes after the last copy out.  Device staging (two copies of inputs
+ * and outputs) is allocated on the first call and kept with the batch. */
+int tnx_heff_batch_apply_host(tnx_heff_batch* b, const double* const* host_in, double* const* host_out,
+                              int32_t n_steps, void* stream);
+/* Elements of the concatenated theta buffer and each problem's offset in it
+ * (offsets: n doubles' worth of int64, or NULL). */
+int tnx_heff_batch_size(const tnx_heff_batch* b, int64_t* total, int64_t* offsets);
 /* Re-run one stage of the last apply (0 pack theta, 1 stage-1 GEMM, 2 fused
  * MPO, 3 stage-4 GEMM) with the same buffers -- per-kernel timing. */
 int tnx_heff_batch_apply_stage(tnx_heff_batch* b, int32_t stage, void* stream);

@@ -75,6 +75,8 @@ def _load():
         "tnx_heff_destroy": (None, [P]),
         "tnx_heff_batch_create": (C.c_int, [P, i32, i32, P]),
         "tnx_heff_batch_apply": (C.c_int, [P, P, P, P]),
+        "tnx_heff_batch_apply_host": (C.c_int, [P, P, P, i32, P]),
+        "tnx_heff_batch_size": (C.c_int, [P, P, P]),
         "tnx_heff_batch_launches": (C.c_int, [P, P]),
         "tnx_heff_batch_apply_stage": (C.c_int, [P, i32, P]),
         "tnx_heff_stage_flops": (C.c_int, [P, P]),
@@ -109,7 +111,8 @@ EXPORTED = [
     "tnx_plan_workspace", "tnx_plan_flops", "tnx_plan_execute", "tnx_plan_destroy", "tnx_plan_execute_static",
     "tnx_heff_create",
     "tnx_heff_closed", "tnx_heff_out_keys", "tnx_heff_flops", "tnx_heff_set_operators", "tnx_heff_destroy",
-    "tnx_heff_batch_create", "tnx_heff_batch_apply", "tnx_heff_batch_apply_stage", "tnx_heff_stage_flops",
+    "tnx_heff_batch_create", "tnx_heff_batch_apply", "tnx_heff_batch_apply_host", "tnx_heff_batch_size",
+    "tnx_heff_batch_apply_stage", "tnx_heff_stage_flops",
     "tnx_heff_batch_launches", "tnx_heff_batch_error",
     "tnx_heff_batch_set_skip_flag", "tnx_heff_batch_destroy", "tnx_reduce_scratch_len", "tnx_dot", "tnx_nrm2",
     "tnx_lanczos_step", "tnx_combine", "tnx_scale", "tnx_fuse_plan_create", "tnx_fuse_plan_output",

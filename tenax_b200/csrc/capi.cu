@@ -987,6 +987,29 @@ struct tnx_heff_batch {
   const int32_t* skip = nullptr;
   int n_launches = 0;
   std::vector<uint64_t> last_src, last_out;
+  // host-resident streaming (tnx_heff_batch_apply_host): each problem's theta
+  // at th_off[i] of one concatenated buffer; two device copies of the inputs
+  // and outputs with their pointer tables, two copy streams and the events
+  // that order them against the compute stream
+  std::vector<int64_t> th_off;
+  int64_t th_total = 0;
+  DevMem pipe_in[2], pipe_out[2], pipe_src_tab[2], pipe_out_tab[2];
+  cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_in_ready[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr},
+              ev_out_free[2] = {nullptr, nullptr};
+  tnx_heff_batch() = default;
+  tnx_heff_batch(const tnx_heff_batch&) = delete;
+  tnx_heff_batch& operator=(const tnx_heff_batch&) = delete;
+  ~tnx_heff_batch() {
+    // copies still in flight must land before the buffers are released
+    if (s_h2d) cudaStreamSynchronize(s_h2d);
+    if (s_d2h) cudaStreamSynchronize(s_d2h);
+    if (s_h2d) cudaStreamDestroy(s_h2d);
+    if (s_d2h) cudaStreamDestroy(s_d2h);
+    for (cudaEvent_t e : {ev_start, ev_in_ready[0], ev_in_ready[1], ev_done[0], ev_done[1], ev_out_free[0],
+                          ev_out_free[1]})
+      if (e) cudaEventDestroy(e);
+  }
 };
 
 int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx_heff_batch** out) {
@@ -1002,6 +1025,10 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     for (int i = 0; i < n; ++i) {
       if (hs[i]->prec != precision) return set_err(TNX_ERR_VALUE, "operators were packed for another precision");
       b->hs.push_back(hs[i]);
+    }
+    for (int i = 0; i < n; ++i) {
+      b->th_off.push_back(b->th_total);
+      b->th_total += hs[i]->H.th.total;
     }
     // sizes: theta images (stage-1 B), X1 results, X3 images (stage-4 A)
     int64_t th_tiles = 0, x3_tiles = 0, x1_elems = 0;
@@ -1248,16 +1275,18 @@ int tnx_heff_batch_launches(const tnx_heff_batch* b, int32_t* n_launches) {
   return TNX_OK;
 }
 
-// stage 0: pack theta; 1: stage-1 GEMM; 2: fused MPO; 3: stage-4 GEMM into theta layout
-static void heff_batch_stage(tnx_heff_batch* b, int stage, cudaStream_t st) {
+// stage 0: pack theta; 1: stage-1 GEMM; 2: fused MPO; 3: stage-4 GEMM into theta layout.
+// src_tab / out_tab4: device pointer tables of the inputs (problem i) and outputs (slot 1 + i)
+static void heff_batch_stage(tnx_heff_batch* b, int stage, cudaStream_t st, const uint64_t* src_tab,
+                             const uint64_t* out_tab4) {
   const bool f32 = b->mode != IMG_F64;
   switch (stage) {
     case 0:
       if (b->th_by_rows)
-        launch_pack_rows(b->src_tab.as<uint64_t>(), b->th_rows.as<DevRowPackSeg>(), b->th_row_chunks.as<int4>(),
+        launch_pack_rows(src_tab, b->th_rows.as<DevRowPackSeg>(), b->th_row_chunks.as<int4>(),
                          b->n_th_row_chunks, b->mode, b->skip, st);
       else
-        launch_pack(b->src_tab.as<uint64_t>(), b->th_pack.as<DevPackSeg>(), b->th_chunks.as<DevChunk>(),
+        launch_pack(src_tab, b->th_pack.as<DevPackSeg>(), b->th_chunks.as<DevChunk>(),
                     b->n_th_chunks, b->mode, b->skip, st);
       break;
     case 1:
@@ -1274,13 +1303,13 @@ static void heff_batch_stage(tnx_heff_batch* b, int stage, cudaStream_t st) {
                        b->n_mpo_chunks, b->mpo_smem, b->skip, st);
       break;
     default:
-      launch_zero_ranges(b->out_tab4.as<uint64_t>(), b->zero_chunks.as<DevChunk>(), b->n_zero_chunks, b->skip, st);
+      launch_zero_ranges(out_tab4, b->zero_chunks.as<DevChunk>(), b->n_zero_chunks, b->skip, st);
       if (b->mode == IMG_F64)
         launch_gemm_f64(b->g4.as<DevGroup>(), b->t4.as<DevTile>(), b->n_t4, b->ro4.as<int64_t>(),
-                        b->out_tab4.as<uint64_t>(), b->skip, st);
+                        out_tab4, b->skip, st);
       else
         launch_gemm_tc(b->mode, b->g4.as<DevGroup>(), b->t4.as<DevTile>(), b->n_t4, b->ro4.as<int64_t>(),
-                       b->out_tab4.as<uint64_t>(), true, b->err.as<int32_t>(), b->skip, st);
+                       out_tab4, true, b->err.as<int32_t>(), b->skip, st);
   }
 }
 
@@ -1303,17 +1332,80 @@ int tnx_heff_batch_apply(tnx_heff_batch* b, const double* const* thetas, double*
       CUDA_OK(cudaMemcpyAsync(b->out_tab4.p, o4.data(), (n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
       b->last_out = o4;
     }
-    for (int stage = 0; stage < 4; ++stage) heff_batch_stage(b, stage, st);
+    for (int stage = 0; stage < 4; ++stage)
+      heff_batch_stage(b, stage, st, b->src_tab.as<uint64_t>(), b->out_tab4.as<uint64_t>());
     CUDA_OK(cudaGetLastError());
     return TNX_OK;
   })
+}
+
+int tnx_heff_batch_apply_host(tnx_heff_batch* b, const double* const* host_in, double* const* host_out,
+                              int32_t n_steps, void* stream) {
+  TNX_TRY({
+    if (n_steps < 0) return set_err(TNX_ERR_VALUE, "n_steps must be >= 0");
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    const int n = static_cast<int>(b->hs.size());
+    const size_t bytes = static_cast<size_t>(b->th_total) * sizeof(double);
+    if (!b->s_h2d) {
+      CUDA_OK(cudaStreamCreateWithFlags(&b->s_h2d, cudaStreamNonBlocking));
+      CUDA_OK(cudaStreamCreateWithFlags(&b->s_d2h, cudaStreamNonBlocking));
+      CUDA_OK(cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming));
+      for (int k = 0; k < 2; ++k) {
+        CUDA_OK(cudaEventCreateWithFlags(&b->ev_in_ready[k], cudaEventDisableTiming));
+        CUDA_OK(cudaEventCreateWithFlags(&b->ev_done[k], cudaEventDisableTiming));
+        CUDA_OK(cudaEventCreateWithFlags(&b->ev_out_free[k], cudaEventDisableTiming));
+        b->pipe_in[k].alloc(std::max<size_t>(8, bytes));
+        b->pipe_out[k].alloc(std::max<size_t>(8, bytes));
+        std::vector<uint64_t> src(n), o4(n + 1, 0);
+        for (int i = 0; i < n; ++i) {
+          src[i] = reinterpret_cast<uint64_t>(b->pipe_in[k].as<double>() + b->th_off[i]);
+          o4[1 + i] = reinterpret_cast<uint64_t>(b->pipe_out[k].as<double>() + b->th_off[i]);
+        }
+        upload(b->pipe_src_tab[k], src);
+        upload(b->pipe_out_tab[k], o4);
+      }
+      CUDA_OK(cudaDeviceSynchronize());
+    }
+    if (n_steps == 0) return TNX_OK;
+    // the copy streams start after the work already queued on the caller's stream
+    CUDA_OK(cudaEventRecord(b->ev_start, cs));
+    CUDA_OK(cudaStreamWaitEvent(b->s_h2d, b->ev_start, 0));
+    CUDA_OK(cudaStreamWaitEvent(b->s_d2h, b->ev_start, 0));
+    for (int i = 0; i < n_steps; ++i) {
+      const int k = i & 1;
+      // in[k] is free once step i-2 has computed; out[k] once its copy-out ended
+      if (i >= 2) CUDA_OK(cudaStreamWaitEvent(b->s_h2d, b->ev_done[k], 0));
+      if (bytes) CUDA_OK(cudaMemcpyAsync(b->pipe_in[k].p, host_in[i], bytes, cudaMemcpyHostToDevice, b->s_h2d));
+      CUDA_OK(cudaEventRecord(b->ev_in_ready[k], b->s_h2d));
+      CUDA_OK(cudaStreamWaitEvent(cs, b->ev_in_ready[k], 0));
+      if (i >= 2) CUDA_OK(cudaStreamWaitEvent(cs, b->ev_out_free[k], 0));
+      for (int stage = 0; stage < 4; ++stage)
+        heff_batch_stage(b, stage, cs, b->pipe_src_tab[k].as<uint64_t>(), b->pipe_out_tab[k].as<uint64_t>());
+      CUDA_OK(cudaEventRecord(b->ev_done[k], cs));
+      CUDA_OK(cudaStreamWaitEvent(b->s_d2h, b->ev_done[k], 0));
+      if (bytes) CUDA_OK(cudaMemcpyAsync(host_out[i], b->pipe_out[k].p, bytes, cudaMemcpyDeviceToHost, b->s_d2h));
+      CUDA_OK(cudaEventRecord(b->ev_out_free[k], b->s_d2h));
+    }
+    // the caller's stream completes after the last copy-out
+    CUDA_OK(cudaStreamWaitEvent(cs, b->ev_out_free[(n_steps - 1) & 1], 0));
+    CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
+
+int tnx_heff_batch_size(const tnx_heff_batch* b, int64_t* total, int64_t* offsets) {
+  *total = b->th_total;
+  if (offsets)
+    for (size_t i = 0; i < b->th_off.size(); ++i) offsets[i] = b->th_off[i];
+  return TNX_OK;
 }
 
 int tnx_heff_batch_apply_stage(tnx_heff_batch* b, int32_t stage, void* stream) {
   TNX_TRY({
     if (stage < 0 || stage > 3) return set_err(TNX_ERR_VALUE, "stage must be 0..3");
     if (b->last_src.empty()) return set_err(TNX_ERR_VALUE, "call tnx_heff_batch_apply once first");
-    heff_batch_stage(b, stage, static_cast<cudaStream_t>(stream));
+    heff_batch_stage(b, stage, static_cast<cudaStream_t>(stream), b->src_tab.as<uint64_t>(),
+                     b->out_tab4.as<uint64_t>());
     CUDA_OK(cudaGetLastError());
     return TNX_OK;
   })

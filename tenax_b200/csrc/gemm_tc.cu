@@ -30,7 +30,15 @@ constexpr int TILE_BYTES = 16384;
 constexpr int EPI_WARPS = TNX_EPI_WARPS;
 static_assert(EPI_WARPS == 4 || EPI_WARPS == 8, "epilogue warps: 4 or 8");
 constexpr int THREADS = 64 + 32 * EPI_WARPS;
-constexpr int TMEM_COLS = 2 * TBN;
+// TMEM accumulators: the MMAs may run NACC - 1 tiles ahead of the epilogue.
+// Four (all 512 columns) measured the same as two on the 64-problem H_eff
+// batch (stage 1: 1.84-1.88 vs 1.84-1.86 ms).
+#ifndef TNX_TMEM_ACC
+#define TNX_TMEM_ACC 2
+#endif
+constexpr int NACC = TNX_TMEM_ACC;
+static_assert(NACC == 2 || NACC == 4, "TMEM accumulators: 2 or 4 (512 columns)");
+constexpr int TMEM_COLS = NACC * TBN;
 constexpr uint64_t kTimeoutNs = 2000000000ull;  // 2 s per wait
 
 __device__ __forceinline__ uint64_t gtimer() {
@@ -106,6 +114,18 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// 16 lanes x 4 chunks of 8 consecutive 32-bit columns (no wait): in each
+// chunk j, thread t holds row t/4 in v[4j], v[4j+1] and row t/4 + 8 in
+// v[4j+2], v[4j+3], columns 8j + 2(t%4) and 8j + 2(t%4) + 1
+__device__ __forceinline__ void tmem_ld16x256b_x4(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 constexpr int kStagePitch = 33;  // fp32 words per staged row (+1 breaks bank conflicts)
 constexpr int kEpiStageBytes = EPI_WARPS * 32 * kStagePitch * 4;
 
@@ -125,8 +145,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * NT * TILE_BYTES);
   uint64_t* empty = full + STAGES;
   uint64_t* tfull = empty + STAGES;
-  uint64_t* tempty = tfull + 2;
-  uint64_t* drain = tempty + 2;
+  uint64_t* tempty = tfull + NACC;
+  uint64_t* drain = tempty + NACC;
   uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
   // epilogue staging: one 32 x 33 fp32 buffer per epilogue warp, after 256 B of barriers
@@ -138,7 +158,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    for (int a = 0; a < 2; ++a) {
+    for (int a = 0; a < NACC; ++a) {
       mbar_init(&tfull[a], 1);
       mbar_init(&tempty[a], 32 * EPI_WARPS);
     }
@@ -255,7 +275,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         if (!ok) break;
         mma_commit(&tfull[acc]);
-        if (++acc == 2) {
+        if (++acc == NACC) {
           acc = 0;
           aph ^= 1u;
         }
@@ -292,45 +312,50 @@ __global__ void __launch_bounds__(THREADS, 1)
       // output's own precision (FP32 outputs only ever carry scale 1; a
       // per-element FP64 round trip there doubled the epilogue's cost)
       const OutT scale = static_cast<OutT>(g.scale);
-      // Each lane holds one row; stage 32x32 chunks through shared memory so
-      // that every store instruction writes 32 consecutive columns of one row.
+      // FP32 results with aligned rows store straight from the 16x256b
+      // fragments; otherwise each lane holds one row (32x32b) and 32x32
+      // chunks are staged through shared memory so that every store
+      // instruction writes 32 consecutive columns of one row.
 #pragma unroll 1
       for (int c0 = c_begin; c0 < c_begin + kColsPerWarp; c0 += 32) {
-        uint32_t v[32];
-        tmem_ld32(tbase + c0, v);
         bool done = false;
         if constexpr (sizeof(OutT) == 4) {
           if (g.vec_ld > 0) {
-            // 16-byte path: rows of 32 floats, 16-byte chunks XOR-swizzled by
-            // row (conflict-free STS.128 / LDS.128); each lane then stores 4
-            // consecutive columns of row it*4 + lane/8
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-              *reinterpret_cast<float4*>(stg + lane * 32 + ((q ^ (lane & 7)) << 2)) =
-                  make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
-                              __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
-            __syncwarp();
-            const int cq = lane & 7;
-            const int col = tl.nt * TBN + c0 + cq * 4;
+            // register-direct path (no staging): two 16-row slabs in the
+            // 16x256b fragment layout; four lanes hold 8 consecutive columns
+            // of one row, so every 8-byte store instruction fills whole
+            // 32-byte sectors of 8 rows
+            uint32_t v0[16], v1[16];
+            tmem_ld16x256b_x4(tbase + c0, v0);
+            tmem_ld16x256b_x4(tbase + (16u << 16) + c0, v1);
+            tmem_wait_ld();
             const float fs = static_cast<float>(scale);
-#pragma unroll 2
-            for (int it = 0; it < 8; ++it) {
-              const int r = it * 4 + (lane >> 3);
-              const int64_t ro_r = __shfl_sync(0xffffffffu, ro, r);
-              float4 x = *reinterpret_cast<const float4*>(stg + r * 32 + ((cq ^ (r & 7)) << 2));
-              if (ro_r >= 0 && col < g.vec_ld) {
-                x.x *= fs;
-                x.y *= fs;
-                x.z *= fs;
-                x.w *= fs;
-                *reinterpret_cast<float4*>(reinterpret_cast<float*>(out) + ro_r + col) = x;
+            const int cl = tl.nt * TBN + c0 + 2 * (lane & 3);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const uint32_t(&v)[16] = h ? v1 : v0;
+              const int r = 16 * h + (lane >> 2);
+              const int64_t ro_a = __shfl_sync(0xffffffffu, ro, r);
+              const int64_t ro_b = __shfl_sync(0xffffffffu, ro, r + 8);
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {
+                const int col = cl + 8 * j;  // even; vec_ld is a multiple of 4
+                if (col < g.vec_ld) {
+                  if (ro_a >= 0)
+                    *reinterpret_cast<float2*>(reinterpret_cast<float*>(out) + ro_a + col) =
+                        make_float2(__uint_as_float(v[4 * j]) * fs, __uint_as_float(v[4 * j + 1]) * fs);
+                  if (ro_b >= 0)
+                    *reinterpret_cast<float2*>(reinterpret_cast<float*>(out) + ro_b + col) =
+                        make_float2(__uint_as_float(v[4 * j + 2]) * fs, __uint_as_float(v[4 * j + 3]) * fs);
+                }
               }
             }
-            __syncwarp();
             done = true;
           }
         }
         if (!done) {
+          uint32_t v[32];
+          tmem_ld32(tbase + c0, v);
 #pragma unroll
           for (int j = 0; j < 32; ++j) stg[lane * kStagePitch + j] = __uint_as_float(v[j]);
           __syncwarp();
@@ -347,7 +372,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       }
       tc_fence_before();
       mbar_arrive(&tempty[acc]);
-      if (++acc == 2) {
+      if (++acc == NACC) {
         acc = 0;
         aph ^= 1u;
       }

@@ -130,11 +130,34 @@ class HeffBatch:
         _capi.check(_capi.LIB.tnx_heff_batch_launches(h, C.byref(n)))
         self.launches_per_apply = n.value
         self.flops = sum(o.flops for o in self.ops)
+        tot = C.c_int64()
+        offs = np.zeros(len(self.ops), dtype=np.int64)
+        _capi.check(_capi.LIB.tnx_heff_batch_size(h, C.byref(tot), offs.ctypes.data))
+        self.total = tot.value  # elements of the concatenated theta buffer (problems in batch order)
+        self.offsets = offs
 
     def apply(self, thetas, outs):
         tp = (C.c_void_p * len(thetas))(*[t.data_ptr() for t in thetas])
         op = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
         _capi.check(_capi.LIB.tnx_heff_batch_apply(self.handle, tp, op, torch.cuda.current_stream().cuda_stream))
+
+    def apply_host(self, host_inputs, host_outputs):
+        """Stream independent applications from host memory: host_inputs[s]
+        and host_outputs[s] are CPU float64 tensors of ``total`` elements
+        (every problem's theta concatenated in batch order, at ``offsets``).
+        Step s+1's copy in and step s-1's copy out overlap step s's compute;
+        pinned buffers make the copies asynchronous.  Work is queued on the
+        current stream and complete when it is."""
+        if len(host_inputs) != len(host_outputs):
+            raise ValueError("host_inputs and host_outputs must have the same length")
+        for t in list(host_inputs) + list(host_outputs):
+            if t.device.type != "cpu" or t.dtype != torch.float64 or not t.is_contiguous() or t.numel() != self.total:
+                raise ValueError(f"host buffers must be contiguous CPU float64 tensors of {self.total} elements")
+        n = len(host_inputs)
+        ip = (C.c_void_p * max(1, n))(*[t.data_ptr() for t in host_inputs])
+        op = (C.c_void_p * max(1, n))(*[t.data_ptr() for t in host_outputs])
+        _capi.check(_capi.LIB.tnx_heff_batch_apply_host(self.handle, ip, op, n,
+                                                        torch.cuda.current_stream().cuda_stream))
 
     def device_error(self) -> int:
         e = C.c_int32()

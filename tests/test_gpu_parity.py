@@ -138,6 +138,35 @@ def test_batch_equals_individual():
         torch.testing.assert_close(a, b, rtol=0, atol=0)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+def test_batch_host_streaming_equals_device_apply(precision):
+    """tnx_heff_batch_apply_host: five independent steps streamed from pinned
+    host memory (copies overlapped with compute on their own streams) give
+    bit-for-bit the outputs of device-resident applies of the same inputs."""
+    probs = [_random_problem(c, s, n_sectors=10, hi=48) for c, s in ((120, 1), (200, 2), (160, 3))]
+    ops = [tb.HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, precision) for p in probs]
+    batch = tb.HeffBatch(ops)
+    assert batch.total == sum(o.size for o in ops)
+    assert list(batch.offsets) == list(np.cumsum([0] + [o.size for o in ops])[:-1])
+    rng = np.random.default_rng(7)
+    steps = 5
+    h_in = [torch.from_numpy(rng.standard_normal(batch.total)).pin_memory() for _ in range(steps)]
+    h_out = [torch.full((batch.total,), np.nan, dtype=torch.float64).pin_memory() for _ in range(steps)]
+    batch.apply_host(h_in, h_out)
+    torch.cuda.synchronize()
+    for s in range(steps):
+        x = h_in[s].cuda()
+        y = torch.empty_like(x)
+        xs = [x[o:o + op.size] for o, op in zip(batch.offsets, ops)]
+        ys = [y[o:o + op.size] for o, op in zip(batch.offsets, ops)]
+        batch.apply(xs, ys)
+        torch.cuda.synchronize()
+        torch.testing.assert_close(h_out[s], y.cpu(), rtol=0, atol=0)
+    assert batch.device_error() == 0
+    with pytest.raises(ValueError):
+        batch.apply_host(h_in[:1], [torch.empty(3, dtype=torch.float64)])
+
+
 def test_vector_primitives():
     from tenax_b200 import vector
 
