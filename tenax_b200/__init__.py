@@ -26,6 +26,7 @@ from tenax_b200.contraction import (  # noqa: F401
     contract_with_subscripts,
 )
 from tenax_b200.heff import HeffBatch, HeffOperator  # noqa: F401
+from tenax_b200.netfile import NetworkBlueprint, from_netfile, parse_netfile  # noqa: F401
 from tenax_b200.ipeps import (  # noqa: F401
     CTMConfig,
     CTMEnvironment,

@@ -310,7 +310,8 @@ int tnx_plan_create(const tnx_tensor_desc* ops, int32_t n_ops, const char* out_s
       if (kv.second > 2) return set_err(TNX_ERR_VALUE, std::string("subscript '") + kv.first + "' used more than twice");
     KeyFilter filt;
     if (mode == TNX_MATCH_FILTERED) {
-      if (och.empty()) return set_err(TNX_ERR_VALUE, "filtered plans need the output leg charges");
+      if (och.empty() && !osubs.empty())
+        return set_err(TNX_ERR_VALUE, "filtered plans need the output leg charges");
       // output target inference (contractor.py:344-355): plain integer sum
       int64_t total = 0;
       for (auto& t : p->ins) {

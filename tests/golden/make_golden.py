@@ -490,6 +490,83 @@ def gen_ctm_tensor(M):
         json.dump(meta, fh, indent=1)
 
 
+NETFILE_SOURCES = [
+    ("pair", "# a pair\nA: i, j\nB: j, k\nTOUT: k, i\n"),
+    ("chain3", "A: i, j\nB: j, k\nC: k, l\n"),
+    ("chain3_order", "A: i, j\nB: j, k\nC: k, l\nTOUT: l, i\nORDER: ((A, B), C)\n"),
+    ("chain3_order_right", "A: i, j\nB: j, k\nC: k, l\nORDER: (A,(B,C))\n"),
+    ("ring_scalar", "A: i, j\nB: j, i\nTOUT:\n"),
+    ("no_tout", "X: a, b, c\nY: c, d\n"),
+    ("err_no_colon", "A i j\n"),
+    ("err_dup_tout", "A: i\nTOUT: i\nTOUT: i\n"),
+    ("err_dup_order", "A: i, j\nB: j\nORDER: (A,B)\nORDER: (A,B)\n"),
+    ("err_dup_name", "A: i\nA: j\n"),
+    ("err_no_labels", "A:\n"),
+    ("err_empty", "# nothing\n\n"),
+    ("err_label3", "A: i\nB: i\nC: i\n"),
+    ("err_order_unknown", "A: i, j\nB: j\nORDER: (A, Z)\n"),
+    ("err_order_syntax", "A: i, j\nB: j\nORDER: (A B)\n"),
+    ("err_order_trailing", "A: i, j\nB: j\nORDER: (A,B) C\n"),
+    ("err_order_close", "A: i, j\nB: j\nORDER: (A,B\n"),
+    ("err_tout_not_free", "A: i, j\nB: j, k\nTOUT: j\n"),
+]
+
+
+def gen_netfile(M):
+    """Network files (network/netfile.py): the reference's parse result,
+    pairwise ORDER steps, precomputed subscripts or its error text for each
+    source above, and NetworkBlueprint.launch() on U(1) tensors: a pair with
+    a TOUT permutation, a 3-chain without ORDER (the reference's filtered
+    N-operand contraction returns no blocks), the same chain with ORDER
+    left and right nested, a closed ring contracted to a scalar, and slots
+    filled through label_order and through a transpose."""
+    nf = M["tenax.network.netfile"]
+    out = {"parse": {}, "launch": {}}
+    for name, src in NETFILE_SOURCES:
+        try:
+            bp = nf.NetworkBlueprint(src)
+            spec = nf.parse_netfile(src)
+            steps = nf._parse_order(spec["order"], set(spec["tensors"])) if spec["order"] is not None else None
+            out["parse"][name] = {"source": src, "tensors": spec["tensors"], "tout": spec["tout"],
+                                  "order": spec["order"], "steps": steps, "subscripts": bp.subscripts,
+                                  "tensor_names": bp.tensor_names, "output_labels": bp.output_labels}
+        except ValueError as e:
+            out["parse"][name] = {"source": src, "error": str(e)}
+    rng = np.random.default_rng(31)
+    bond = [-1, 0, 1, 0]
+    arrays = {}
+
+    def t(labels, flows):
+        return make_sym_tensor(M, [(bond, f, lab) for lab, f in zip(labels, flows)], rng)
+
+    A = t("ij", (1, -1))
+    B = t("jk", (1, -1))
+    Cc = t("kl", (1, -1))
+    Bring = t("ji", (1, -1))
+    for nm, x in (("A", A), ("B", B), ("C", Cc), ("Bring", Bring)):
+        arrays.update(dump_tensor(f"in.{nm}", x))
+    runs = [("pair", {"A": A, "B": B}), ("chain3", {"A": A, "B": B, "C": Cc}),
+            ("chain3_order", {"A": A, "B": B, "C": Cc}), ("chain3_order_right", {"A": A, "B": B, "C": Cc}),
+            ("ring_scalar", {"A": A, "B": Bring})]
+    for name, slots in runs:
+        bp = nf.NetworkBlueprint(dict(NETFILE_SOURCES)[name])
+        bp.put_tensors(slots)
+        res = bp.launch()
+        arrays.update(dump_tensor(f"out.{name}", res))
+        out["launch"][name] = {"n_blocks": len(res.blocks), "labels": [str(x) for x in res.labels()]}
+    # slots filled through label_order (relabel) and through a transpose
+    bp = nf.NetworkBlueprint(dict(NETFILE_SOURCES)["pair"])
+    bp.put_tensor("A", A.relabels({"i": "x", "j": "y"}), label_order=["x", "y"])
+    bp.put_tensor("B", B.transpose((1, 0)))
+    res = bp.launch()
+    arrays.update(dump_tensor("out.pair_label_order", res))
+    out["launch"]["pair_label_order"] = {"n_blocks": len(res.blocks), "labels": [str(x) for x in res.labels()]}
+    np.savez_compressed(os.path.join(HERE, "netfile.npz"), **arrays)
+    with open(os.path.join(HERE, "netfile.json"), "w") as fh:
+        json.dump(out, fh, indent=1)
+    print(f"netfile: {len(out['parse'])} parse cases, {len(out['launch'])} launches", flush=True)
+
+
 def gen_ctm(M):
     """Dense 1-site CTMRG (algorithms/ipeps.py): environments, corner
     singular values and NN Heisenberg energies from the reference's own
@@ -555,11 +632,11 @@ def main():
         "tenax.core.symmetry", "tenax.core.index", "tenax.core.tensor", "tenax.linalg",
         "tenax.contraction.contractor", "tenax.network.network", "tenax.algorithms._tensor_utils",
         "tenax.algorithms.auto_mpo", "tenax.algorithms.dmrg", "tenax.algorithms.ipeps",
-        "tenax.algorithms._split_ctm_tensor", "tenax.algorithms._ctm_tensor",
+        "tenax.algorithms._split_ctm_tensor", "tenax.algorithms._ctm_tensor", "tenax.network.netfile",
     ])
     mods["cfg"] = mods["tenax.algorithms.dmrg"].DMRGConfig
     todo = args.only.split(",") if args.only else ["valid", "contract", "pieces", "mpo", "c1", "ctm", "fuse", "split",
-                                                       "ctm_tensor"]
+                                                       "ctm_tensor", "netfile"]
     if "valid" in todo:
         gen_valid_blocks(mods)
     if "contract" in todo:
@@ -578,6 +655,8 @@ def main():
         gen_split_ctm(mods)
     if "ctm_tensor" in todo:
         gen_ctm_tensor(mods)
+    if "netfile" in todo:
+        gen_netfile(mods)
 
 
 if __name__ == "__main__":
