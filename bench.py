@@ -116,10 +116,11 @@ def run_ours(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from tenax_b200 import HeffBatch, HeffOperator, _capi
+    from tenax_b200 import replicas
     from tenax_b200.tensor import embed_in_keys
     from tenax_b200.workloads import batched_problems
 
-    problems = batched_problems(args.problems, CHIS, seed=args.seed + 1000 * rank)
+    problems = batched_problems(args.problems, CHIS, seed=replicas.rank_seed(args.seed, rank))
     chi_counts = {int(c): sum(1 for p in problems if p.chi == c) for c in CHIS}
     dev = torch.device("cuda", local)
 
@@ -129,11 +130,7 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, dist, dev)
 
     def run_precision(prec, with_e2e=False, sampler=None):
         ops = [HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, prec) for p in problems]
@@ -214,9 +211,11 @@ def run_ours(args):
     rmx = run_precision(args.precision, with_e2e=True, sampler=sampler)
     clocks = sampler.summary()
 
-    flops_all = rmx["flops"] * world
+    # ranks draw different problems: the job's work is the sum over ranks, its
+    # time the slowest rank's (the ms values above are already maxima)
+    flops_all = replicas.sum_over_ranks(rmx["flops"], dist, dev)
     value = flops_all / (rmx["ms"] * 1e-3) / 1e12
-    fp64_value = r64["flops"] * world / (r64["ms"] * 1e-3) / 1e12
+    fp64_value = replicas.sum_over_ranks(r64["flops"], dist, dev) / (r64["ms"] * 1e-3) / 1e12
     peaks, peak_src = _peaks()
     # dominant GEMM stage of the mixed step
     st_ms = rmx["stage_ms"]

@@ -219,13 +219,17 @@ def cylinder_mpo(Lx: int = 4, Ly: int = 6):
     return net
 
 
+def draw_chis(n: int, chis=(256, 512, 1024, 2048), seed: int = 0) -> np.ndarray:
+    """The bond dimensions of a batch: n draws, uniform over ``chis``, from a seeded generator."""
+    return np.random.default_rng(seed).choice(np.asarray(chis), size=n)
+
+
 def batched_problems(n: int = 64, chis=(256, 512, 1024, 2048), seed: int = 0, gen_backend: str = "torch",
                      **kw) -> list:
     """The batched grouped-sector workload: n independent two-site problems,
     chi drawn uniformly from ``chis`` with a seeded generator."""
     Wl, Wr = cylinder_bulk_w()
-    rng = np.random.default_rng(seed)
-    draw = rng.choice(np.asarray(chis), size=n)
+    draw = draw_chis(n, chis, seed)
     if gen_backend == "torch":
         gen = torch.Generator(device=_device())
         gen.manual_seed(seed)
