@@ -393,7 +393,12 @@ def run_dmrg_study(args):
            "sweeps": args.sweeps, "lanczos_max_iter": args.lanczos, "data": "seeded random initial MPS",
            "svd": {"driver": args.svd_driver, "streams": args.svd_streams}, "runs": {}}
     fp64_e = None
+    out["plans"] = "contraction plan caches cleared before every run: each arm plans its own contractions"
+    from tenax_b200 import contraction as _contraction, dense as _dense
+
     for prec in args.dmrg_precisions.split(","):
+        _contraction._PLANS.clear()
+        _dense._PLANS.clear()
         mps = random_symmetric_mps(Lx * Ly, args.chi, seed=args.seed)
         cfg = DMRGConfig(max_bond_dim=args.chi, num_sweeps=args.sweeps, lanczos_max_iter=args.lanczos,
                          convergence_tol=0.0, precision=prec, check_matvec_residual=prec != "fp64",

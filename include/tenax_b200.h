@@ -114,6 +114,12 @@ int tnx_plan_execute_static(const tnx_plan* plan, const double* const* inputs, d
  * set until it is -- the key-union growth of the reference's Lanczos). */
 int tnx_heff_create(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, const tnx_tensor_desc* Wl,
                     const tnx_tensor_desc* Wr, const tnx_tensor_desc* R, tnx_heff** h);
+/* The same, planned for the precision the operator will be packed in
+ * (TNX_PREC_*): the mixed precisions lay the stage-1 result out for the fused
+ * MPO kernel's aligned loads.  tnx_heff_set_operators with another
+ * precision re-plans, so either create works with any precision. */
+int tnx_heff_create_for(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, const tnx_tensor_desc* Wl,
+                        const tnx_tensor_desc* Wr, const tnx_tensor_desc* R, int32_t precision, tnx_heff** h);
 int tnx_heff_closed(const tnx_heff* h, int32_t* closed);
 /* Output keys of H_eff applied to theta's key set (structure only). */
 int tnx_heff_out_keys(const tnx_heff* h, int64_t* n_keys, int32_t* keys);

@@ -68,6 +68,7 @@ def _load():
         "tnx_plan_destroy": (None, [P]),
         "tnx_plan_execute_static": (C.c_int, [P, P, P, P]),
         "tnx_heff_create": (C.c_int, [P, P, P, P, P, P]),
+        "tnx_heff_create_for": (C.c_int, [P, P, P, P, P, i32, P]),
         "tnx_heff_closed": (C.c_int, [P, P]),
         "tnx_heff_out_keys": (C.c_int, [P, P, P]),
         "tnx_heff_flops": (dbl, [P]),
@@ -109,7 +110,7 @@ LIB = _load()
 EXPORTED = [
     "tnx_last_error", "tnx_version", "tnx_valid_blocks", "tnx_plan_create", "tnx_plan_output",
     "tnx_plan_workspace", "tnx_plan_flops", "tnx_plan_execute", "tnx_plan_destroy", "tnx_plan_execute_static",
-    "tnx_heff_create",
+    "tnx_heff_create", "tnx_heff_create_for",
     "tnx_heff_closed", "tnx_heff_out_keys", "tnx_heff_flops", "tnx_heff_set_operators", "tnx_heff_destroy",
     "tnx_heff_batch_create", "tnx_heff_batch_apply", "tnx_heff_batch_apply_host", "tnx_heff_batch_size",
     "tnx_heff_batch_apply_stage", "tnx_heff_stage_flops",

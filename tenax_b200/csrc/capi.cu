@@ -859,6 +859,11 @@ struct tnx_heff {
 
 int tnx_heff_create(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, const tnx_tensor_desc* Wl,
                     const tnx_tensor_desc* Wr, const tnx_tensor_desc* R, tnx_heff** h) {
+  return tnx_heff_create_for(L, theta, Wl, Wr, R, TNX_PREC_FP64, h);
+}
+
+int tnx_heff_create_for(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, const tnx_tensor_desc* Wl,
+                        const tnx_tensor_desc* Wr, const tnx_tensor_desc* R, int32_t precision, tnx_heff** h) {
   TNX_TRY({
     auto x = std::make_unique<tnx_heff>();
     TensorStruct tL = parse_desc(L, "abc"), tT = parse_desc(theta, "apqd"), tWl = parse_desc(Wl, "bpse"),
@@ -868,7 +873,8 @@ int tnx_heff_create(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, cons
     tWl.subs = "bpse";
     tWr.subs = "eqtf";
     tR.subs = "dfg";
-    x->H = plan_heff(tL, tT, tWl, tWr, tR);
+    // the mixed precisions read X1 with aligned 32-byte loads (see tnx_heff_set_operators)
+    x->H = plan_heff(tL, tT, tWl, tWr, tR, img_mode_of(precision) == IMG_F64 ? 1 : kMpoKAlign);
     *h = x.release();
     return TNX_OK;
   })

@@ -31,11 +31,12 @@ def _desc(t_indices, keys):
     return _capi.DescHolder([i.charges for i in t_indices], [int(i.flow) for i in t_indices], keys, None)
 
 
-def _create(L, th_indices, th_keys, Wl, Wr, R):
+def _create(L, th_indices, th_keys, Wl, Wr, R, precision: str = "fp64"):
     hold = [_desc(L.indices, L.keys), _desc(th_indices, th_keys), _desc(Wl.indices, Wl.keys),
             _desc(Wr.indices, Wr.keys), _desc(R.indices, R.keys)]
     h = C.c_void_p()
-    _capi.check(_capi.LIB.tnx_heff_create(*[C.byref(x.desc) for x in hold], C.byref(h)))
+    _capi.check(_capi.LIB.tnx_heff_create_for(*[C.byref(x.desc) for x in hold], _capi.PRECISIONS[precision],
+                                              C.byref(h)))
     return h, hold
 
 
@@ -54,14 +55,22 @@ def heff_key_closure(L, th_indices, th_keys, Wl, Wr, R, max_iter: int = 64):
     this way (key-union addition, core/tensor.py:933-952, of matvec outputs
     whose keys are never filtered, dmrg.py:1097).
     """
+    seq, h, _hold = _closure(L, th_indices, th_keys, Wl, Wr, R, "fp64", max_iter)
+    _capi.LIB.tnx_heff_destroy(h)
+    return seq
+
+
+def _closure(L, th_indices, th_keys, Wl, Wr, R, precision, max_iter: int = 64):
+    """heff_key_closure, also returning the plan of the fixed point (created
+    for ``precision``) and the descriptors it points into."""
     seq = [sorted(th_keys)]
     for _ in range(max_iter):
-        h, _hold = _create(L, th_indices, seq[-1], Wl, Wr, R)
+        h, hold = _create(L, th_indices, seq[-1], Wl, Wr, R, precision)
         out = _out_keys(h)
-        _capi.LIB.tnx_heff_destroy(h)
         nxt = sorted(set(seq[-1]) | set(out))
         if nxt == seq[-1]:
-            return seq
+            return seq, h, hold
+        _capi.LIB.tnx_heff_destroy(h)
         seq.append(nxt)
     raise RuntimeError("H_eff key closure did not converge")
 
@@ -72,9 +81,9 @@ class HeffOperator:
     def __init__(self, L: SymmetricTensor, Wl: SymmetricTensor, Wr: SymmetricTensor, R: SymmetricTensor,
                  theta_indices, theta_keys, precision: str = "fp64"):
         self.theta_indices = tuple(theta_indices)
-        self.key_seq = heff_key_closure(L, theta_indices, theta_keys, Wl, Wr, R)
+        # the closure's last plan is the operator's plan (created for its precision)
+        self.key_seq, self.handle, self._hold = _closure(L, theta_indices, theta_keys, Wl, Wr, R, precision)
         self.keys = self.key_seq[-1]
-        self.handle, self._hold = _create(L, theta_indices, self.keys, Wl, Wr, R)
         closed = C.c_int32()
         _capi.check(_capi.LIB.tnx_heff_closed(self.handle, C.byref(closed)))
         if not closed.value:
