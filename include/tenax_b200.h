@@ -135,8 +135,9 @@ void tnx_heff_destroy(tnx_heff* h);
  * (persistent grouped GEMMs over all sectors of all problems). */
 int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx_heff_batch** b);
 int tnx_heff_batch_apply(tnx_heff_batch* b, const double* const* thetas, double* const* outs, void* stream);
-/* Host-resident streaming: n_steps independent applications whose inputs and
- * outputs live in host memory (pinned for overlap).  host_in[s] / host_out[s]
+/* Host-resident streaming (no counterpart in the reference, which applies one
+ * matvec at a time from device arrays): n_steps independent applications
+ * whose inputs and outputs live in host memory (pinned for overlap).  host_in[s] / host_out[s]
  * hold all problems' theta buffers concatenated in batch order (offsets from
  * tnx_heff_batch_size).  Step s+1's copy in and step s-1's copy out run on
  * their own streams while step s computes; the call's work on `stream`
