@@ -171,6 +171,14 @@ int64_t tnx_reduce_scratch_len(void);
 int tnx_dot(const double* x, const double* y, int64_t n, double* result, double* scratch, void* stream);
 int tnx_nrm2(const double* x, int64_t n, double* result, double* scratch, void* stream);
 
+/* Bounded wait on a device flag (no counterpart in the reference): one
+ * thread polls *flag until it equals `expected` or `timeout_ns` (at most
+ * 10 s) has passed on the GPU timer, then writes *status (device memory):
+ * 0, or TNX_ERR_TIMEOUT.  The kernel always returns, so the context stays
+ * usable; it is the same deadline discipline as every wait inside the GEMM
+ * kernels, exposed so callers (and tests) can exercise the timeout path. */
+int tnx_wait_flag(const int32_t* flag, int32_t expected, int64_t timeout_ns, int32_t* status, void* stream);
+
 /* Leg fusion of a block-sparse tensor (tenax algorithms/_tensor_utils.py:
  * 106-325, fuse_indices / _compute_fused_charges / _fuse_indices_symmetric).
  * Legs axis_a and axis_b become one leg at min(axis_a, axis_b) with flow

@@ -1490,6 +1490,17 @@ int tnx_renorm_maxabs_adjoint(int n_tensors, const double* const* x, const doubl
   })
 }
 
+int tnx_wait_flag(const int32_t* flag, int32_t expected, int64_t timeout_ns, int32_t* status, void* stream) {
+  TNX_TRY({
+    if (!flag || !status) return set_err(TNX_ERR_VALUE, "tnx_wait_flag: null flag or status");
+    if (timeout_ns <= 0 || timeout_ns > 10000000000ll)
+      return set_err(TNX_ERR_VALUE, "tnx_wait_flag: timeout must be in (0, 10 s]");
+    launch_wait_flag(flag, expected, static_cast<uint64_t>(timeout_ns), status, static_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
+
 int tnx_nrm2(const double* x, int64_t n, double* result, double* scratch, void* stream) {
   TNX_TRY({
     launch_dot(x, x, n, 1, result, scratch, nullptr, static_cast<cudaStream_t>(stream));

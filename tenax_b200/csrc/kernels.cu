@@ -462,6 +462,34 @@ __global__ void finish_max_kernel(const double* __restrict__ partials, int np, d
   if (threadIdx.x == 0) *result = m;
 }
 
+// ---------------------------------------------------------------------------
+// bounded wait on a device flag: the same deadline discipline as the GEMMs'
+// mbarrier waits (%globaltimer, plus an iteration cap), reporting through a
+// status word instead of hanging
+// ---------------------------------------------------------------------------
+__global__ void wait_flag_kernel(const volatile int32_t* flag, int32_t expected, uint64_t timeout_ns,
+                                 int32_t* status) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint64_t t0;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (uint32_t it = 0; it < (1u << 26); ++it) {
+    if (*flag == expected) {
+      *status = 0;
+      return;
+    }
+    if ((it & 63u) == 63u) {
+      uint64_t now;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+      if (now - t0 > timeout_ns) break;
+    }
+  }
+  *status = 5;  // TNX_ERR_TIMEOUT
+}
+
+void launch_wait_flag(const int32_t* flag, int32_t expected, uint64_t timeout_ns, int32_t* status, cudaStream_t st) {
+  wait_flag_kernel<<<1, 32, 0, st>>>(flag, expected, timeout_ns, status);
+}
+
 void launch_maxabs(const double* x, int64_t n, double* result, double* partials, cudaStream_t st) {
   partial_maxabs_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(x, n, partials);
   finish_max_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, result);

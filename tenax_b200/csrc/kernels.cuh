@@ -38,6 +38,8 @@ void launch_scale(const double* w, double* out, int64_t n, const double* s, int 
                   cudaStream_t st);
 void launch_combine(const double* const* basis, const double* coefs, int nv, int64_t n, double* out,
                     cudaStream_t st);
+// *status = 0 once *flag == expected, TNX_ERR_TIMEOUT after timeout_ns (one thread)
+void launch_wait_flag(const int32_t* flag, int32_t expected, uint64_t timeout_ns, int32_t* status, cudaStream_t st);
 int reduce_partials_count();
 // *result = max |x_i| (partials: reduce_partials_count() doubles)
 void launch_maxabs(const double* x, int64_t n, double* result, double* partials, cudaStream_t st);
