@@ -131,6 +131,15 @@ int img_mode_of(int precision) {
 
 int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// tcgen05 groups: MMA K steps (a quarter slab each) that the last K slab of a
+// group of extent K needs; the image past K is zero, so skipping the rest is exact
+int32_t kk_last_of(int64_t K, int mode) {
+  if (mode == IMG_F64 || K <= 0) return 0;
+  const int tk = img_geom(mode).tk, step = tk / 4;
+  const int64_t last = K - (cdiv(K, tk) - 1) * tk;
+  return static_cast<int32_t>(cdiv(last, step));
+}
+
 // row length of an H_eff stage-1 result matrix: N rounded up to 4 elements so
 // every row starts 16-byte aligned (FP32) and the epilogue stores float4s
 int64_t x1_ld(int64_t n) { return (n + 3) / 4 * 4; }
@@ -499,6 +508,7 @@ static void plan_build_device(tnx_plan* p, int precision) {
       x.M = static_cast<int32_t>(P.groups[g].M);
       x.N = static_cast<int32_t>(P.groups[g].N);
       x.nKt = d->G.nKt[g];
+      x.kk_last = kk_last_of(P.groups[g].K, d->mode);
       x.out_slot = 0;
       x.scale = 1.0;
       gr.push_back(x);
@@ -1125,6 +1135,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         x.M = static_cast<int32_t>(H.s1.groups[g].M);
         x.N = static_cast<int32_t>(H.s1.groups[g].N);
         x.nKt = h->g1.nKt[g];
+        x.kk_last = kk_last_of(H.s1.groups[g].K, b->mode);
         x.out_slot = 0;
         x.scale = 1.0;
         const int64_t ld = x1_ld(H.s1.groups[g].N);
@@ -1150,6 +1161,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         x.M = static_cast<int32_t>(H.s4.groups[g].M);
         x.N = static_cast<int32_t>(H.s4.groups[g].N);
         x.nKt = h->g4.nKt[g];
+        x.kk_last = kk_last_of(H.s4.groups[g].K, b->mode);
         x.out_slot = 1 + i;
         x.scale = h->out_scale;  // undoes the power-of-two scaling of L and R
         for (auto v : H.s4_rowoff[g]) R4.push_back(v);

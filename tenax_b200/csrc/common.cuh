@@ -117,7 +117,7 @@ struct DevGroup {
   double scale;             // result = scale * sum_k A B (undoes operand range scaling)
   int32_t vec_ld;           // > 0: every row offset is a multiple of 4 elements and the first
                             // vec_ld (a multiple of 4, >= N) columns may be written: 16-byte stores
-  int32_t pad;
+  int32_t kk_last;          // tcgen05: MMA K steps (of the 4 per slab) the last K slab needs; 0 = all 4
 };
 
 struct DevTile {

@@ -226,8 +226,9 @@ __global__ void __launch_bounds__(THREADS, 1)
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
-      const uint32_t idesc = (1u << 4) | ((TF32 ? 2u : 1u) << 7) | ((TF32 ? 2u : 1u) << 10) |
-                             (static_cast<uint32_t>(TBN >> 3) << 17) | (static_cast<uint32_t>(TBM >> 4) << 24);
+      // instruction descriptor without N: FP32 accumulate, operand kinds, M = 128
+      const uint32_t idesc0 = (1u << 4) | ((TF32 ? 2u : 1u) << 7) | ((TF32 ? 2u : 1u) << 10) |
+                              (static_cast<uint32_t>(TBM >> 4) << 24);
       int s = 0;
       uint32_t ph = 0;
       int acc = 0;
@@ -235,7 +236,16 @@ __global__ void __launch_bounds__(THREADS, 1)
       bool ok = true;
       bool issued = false;
       for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
-        const DevGroup g = groups[tiles[t].g];
+        const DevTile tl = tiles[t];
+        const DevGroup g = groups[tl.g];
+        // MMA extent trimmed to the tile's valid columns (rounded to 16) and
+        // the last slab's valid K steps: the operand images are zero beyond
+        // both, so the skipped products are exact zeros
+        int ncols = g.N - tl.nt * TBN;
+        ncols = ncols > TBN ? TBN : ncols;
+        const uint32_t n_mma = static_cast<uint32_t>((ncols + 15) / 16 * 16);
+        const uint32_t idesc = idesc0 | ((n_mma >> 3) << 17);
+        const int ksub_last = g.kk_last > 0 ? g.kk_last : KSUB;
         if (!wait_or_abort(&tempty[acc], aph ^ 1u, abort_flag, err_flag)) {
           ok = false;
           break;
@@ -250,17 +260,19 @@ __global__ void __launch_bounds__(THREADS, 1)
           tc_fence_after();
           const uint32_t sa = smem_u32(smem + s * NT * TILE_BYTES);
           const uint64_t da = sw128_desc(sa);
+          const int nk = kt + 1 == g.nKt ? ksub_last : KSUB;
           if (TF32) {
             const uint64_t db = sw128_desc(sa + TILE_BYTES);
 #pragma unroll
             for (int kk = 0; kk < KSUB; ++kk)
-              mma_issue<TF32>(d_tmem, da + 2 * kk, db + 2 * kk, idesc, (kt | kk) ? 1u : 0u);
+              if (kk < nk) mma_issue<TF32>(d_tmem, da + 2 * kk, db + 2 * kk, idesc, (kt | kk) ? 1u : 0u);
           } else {
             const uint64_t dal = sw128_desc(sa + TILE_BYTES);
             const uint64_t db = sw128_desc(sa + 2 * TILE_BYTES);
             const uint64_t dbl = sw128_desc(sa + 3 * TILE_BYTES);
 #pragma unroll
             for (int kk = 0; kk < KSUB; ++kk) {
+              if (kk >= nk) break;
               mma_issue<TF32>(d_tmem, da + 2 * kk, db + 2 * kk, idesc, (kt | kk) ? 1u : 0u);
               mma_issue<TF32>(d_tmem, da + 2 * kk, dbl + 2 * kk, idesc, 1u);
               mma_issue<TF32>(d_tmem, dal + 2 * kk, db + 2 * kk, idesc, 1u);
