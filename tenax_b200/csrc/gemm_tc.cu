@@ -126,6 +126,36 @@ __device__ __forceinline__ void tmem_ld16x256b_x4(uint32_t taddr, uint32_t (&v)[
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// The persistent loop over a CTA's tiles with the descriptors of the next
+// tiles in flight: the group record of tile t+1 and the tile record of t+2
+// are requested while tile t is processed, so no role waits on the
+// tile -> group chain of global loads between tiles.
+struct TileIter {
+  const DevTile* tiles;
+  const DevGroup* groups;
+  int n, step, t;
+  DevTile tl, tl1, tl2;
+  DevGroup g, g1;
+  __device__ __forceinline__ TileIter(const DevTile* tiles_, const DevGroup* groups_, int n_, int t0)
+      : tiles(tiles_), groups(groups_), n(n_), step(static_cast<int>(gridDim.x)), t(t0) {
+    if (t < n) {
+      tl = tiles[t];
+      g = groups[tl.g];
+    }
+    if (t + step < n) tl1 = tiles[t + step];
+  }
+  __device__ __forceinline__ void prefetch() {
+    if (t + step < n) g1 = groups[tl1.g];
+    if (t + 2 * step < n) tl2 = tiles[t + 2 * step];
+  }
+  __device__ __forceinline__ void advance() {
+    t += step;
+    tl = tl1;
+    g = g1;
+    tl1 = tl2;
+  }
+};
+
 constexpr int kStagePitch = 33;  // fp32 words per staged row (+1 breaks bank conflicts)
 constexpr int kEpiStageBytes = EPI_WARPS * 32 * kStagePitch * 4;
 
@@ -185,9 +215,10 @@ __global__ void __launch_bounds__(THREADS, 1)
       int last_par[STAGES];
       for (int i = 0; i < STAGES; ++i) last_par[i] = -1;
       bool ok = true;
-      for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
-        const DevTile tl = tiles[t];
-        const DevGroup g = groups[tl.g];
+      for (TileIter it(tiles, groups, n_tiles, blockIdx.x); it.t < n_tiles && ok; it.advance()) {
+        it.prefetch();
+        const DevTile tl = it.tl;
+        const DevGroup g = it.g;
         const uint8_t* ga = reinterpret_cast<const uint8_t*>(g.a_addr) + static_cast<int64_t>(tl.mt) * g.nKt * TILE_BYTES;
         const uint8_t* gb = reinterpret_cast<const uint8_t*>(g.b_addr) + static_cast<int64_t>(tl.nt) * g.nKt * TILE_BYTES;
         for (int kt = 0; kt < g.nKt; ++kt) {
@@ -235,9 +266,10 @@ __global__ void __launch_bounds__(THREADS, 1)
       uint32_t aph = 0;
       bool ok = true;
       bool issued = false;
-      for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
-        const DevTile tl = tiles[t];
-        const DevGroup g = groups[tl.g];
+      for (TileIter it(tiles, groups, n_tiles, blockIdx.x); it.t < n_tiles && ok; it.advance()) {
+        it.prefetch();
+        const DevTile tl = it.tl;
+        const DevGroup g = it.g;
         // MMA extent trimmed to the tile's valid columns (rounded to 16) and
         // the last slab's valid K steps: the operand images are zero beyond
         // both, so the skipped products are exact zeros
@@ -310,14 +342,16 @@ __global__ void __launch_bounds__(THREADS, 1)
     float* stg = epi_stage + e * 32 * kStagePitch;
     int acc = 0;
     uint32_t aph = 0;
-    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-      const DevTile tl = tiles[t];
-      const DevGroup g = groups[tl.g];
+    for (TileIter it(tiles, groups, n_tiles, blockIdx.x); it.t < n_tiles; it.advance()) {
+      it.prefetch();
+      const DevTile tl = it.tl;
+      const DevGroup g = it.g;
+      // the row offset does not depend on the accumulator: request it before waiting
+      const int row = tl.mt * TBM + r_in_tile;
+      const int64_t ro = row < g.M ? rowoff[g.rowoff0 + row] : -1;
       // all lanes wait (the tcgen05.ld below is warp-collective)
       if (!wait_or_abort(&tfull[acc], aph, abort_flag, err_flag)) break;
       tc_fence_after();
-      const int row = tl.mt * TBM + r_in_tile;
-      const int64_t ro = row < g.M ? rowoff[g.rowoff0 + row] : -1;
       OutT* out = reinterpret_cast<OutT*>(out_tab[g.out_slot]);
       const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * TBN);
       // group scales are powers of two, so the multiply is exact in the
