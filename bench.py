@@ -693,7 +693,9 @@ def main():
     ap.add_argument("--lanczos", type=int, default=20)
     ap.add_argument("--cyl-lx", type=int, default=4)
     ap.add_argument("--dmrg-precisions", default="fp64,bf16x3,tf32")
-    ap.add_argument("--svd-driver", default="gesvdj", help="cuSOLVER SVD driver of the DMRG study (or 'default')")
+    ap.add_argument("--svd-driver", default="native",
+                    help="per-sector SVD of the DMRG study: 'native' (tnx_svd_batch), a torch.linalg.svd driver, "
+                         "or 'default'")
     ap.add_argument("--svd-streams", type=int, default=8)
     ap.add_argument("--ctm", action="store_true", help="run the dense CTMRG forward/gradient study instead")
     ap.add_argument("--ctm-chi", type=int, default=80)

@@ -221,6 +221,25 @@ int tnx_renorm_maxabs(int n_tensors, const double* const* x, double* const* y, c
 int tnx_renorm_maxabs_adjoint(int n_tensors, const double* const* x, const double* const* gy, double* const* gx,
                               const int64_t* n, double eps, const double* stat, double* scratch, void* stream);
 
+/* Thin FP64 SVDs of independent sector matrices: the per-sector step of the
+ * block-diagonal truncated SVD (tenax linalg.py:186-192, one
+ * jnp.linalg.svd(matrix, full_matrices=False) per charge sector).
+ * a[i] is m[i] x k[i], row-major, and is preserved; with r = min(m[i], k[i]),
+ * u[i] receives m x r (row-major), s[i] the r singular values in descending
+ * order and vh[i] r x k (row-major).  m, k, a, u, s, vh are HOST arrays of n
+ * entries (extents and device pointers); sectors with m or k = 0 are skipped.
+ * Sectors with min(m, k) >= polar_min run cuSOLVER's polar-decomposition SVD
+ * (Xgesvdp), the others its Jacobi SVD (gesvdj): the polar driver is 2.5-3x
+ * faster on large sectors and slower on small ones (128 is a good split).
+ * They run on up to n_workers library-owned streams (1..32, one host thread
+ * each), ordered after `stream`, which then waits for all of them; the call
+ * returns once every decomposition has finished.  err_sigma (may be NULL)
+ * receives the largest error estimate the polar driver reported.  Worker
+ * scratch grows to the largest sector seen and is kept. */
+int tnx_svd_batch(int32_t n, const int64_t* m, const int64_t* k, const double* const* a, double* const* u,
+                  double* const* s, double* const* vh, int64_t polar_min, int32_t n_workers, double* err_sigma,
+                  void* stream);
+
 /* One Lanczos orthogonalisation step (dmrg.py:1005-1019) on device:
  *   alpha[k] = <v, w>;  w -= alpha[k] v  (- beta[k] v_prev if k > 0);
  *   beta[k+1] = ||w||;  if beta[k+1] < tol or beta[k+1] < tol_rel*|alpha[k]|: *done = 1

@@ -88,6 +88,7 @@ def _load():
         "tnx_dot": (C.c_int, [P, P, i64, P, P, P]),
         "tnx_nrm2": (C.c_int, [P, i64, P, P, P]),
         "tnx_wait_flag": (C.c_int, [P, i32, i64, P, P]),
+        "tnx_svd_batch": (C.c_int, [i32, P, P, P, P, P, P, i64, i32, P, P]),
         "tnx_lanczos_step": (C.c_int, [P, P, P, P, i64, P, P, i32, dbl, dbl, P, P, P]),
         "tnx_combine": (C.c_int, [P, P, i32, i64, P, P]),
         "tnx_scale": (C.c_int, [P, P, i64, P, i32, P]),
@@ -117,6 +118,7 @@ EXPORTED = [
     "tnx_heff_batch_apply_stage", "tnx_heff_stage_flops",
     "tnx_heff_batch_launches", "tnx_heff_batch_error",
     "tnx_heff_batch_set_skip_flag", "tnx_heff_batch_destroy", "tnx_reduce_scratch_len", "tnx_dot", "tnx_nrm2", "tnx_wait_flag",
+    "tnx_svd_batch",
     "tnx_lanczos_step", "tnx_combine", "tnx_scale", "tnx_fuse_plan_create", "tnx_fuse_plan_output",
     "tnx_fuse_execute", "tnx_fuse_plan_destroy", "tnx_fuse_row_map", "tnx_renorm_scratch_len", "tnx_renorm_maxabs",
     "tnx_renorm_maxabs_adjoint",

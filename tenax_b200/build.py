@@ -16,8 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtenax_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
-SOURCES = ["planner.cpp", "kernels.cu", "gemm_f64.cu", "gemm_tc.cu", "capi.cu"]
-HEADERS = ["planner.hpp", "common.cuh", "kernels.cuh"]
+SOURCES = ["planner.cpp", "kernels.cu", "gemm_f64.cu", "gemm_tc.cu", "svd.cu", "capi.cu"]
+HEADERS = ["planner.hpp", "common.cuh", "kernels.cuh", "svd.hpp"]
 
 NVCC_FLAGS = [
     "-std=c++17",
@@ -31,6 +31,9 @@ NVCC_FLAGS = [
     "-cudart",
     "static",
 ]
+
+# cuSOLVER (sector SVDs), linked dynamically from the CUDA toolkit
+LIBS = ["-lcusolver"]
 
 
 def _nvcc() -> str:
@@ -51,7 +54,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     tmp = LIB + ".tmp"
-    cmd = [_nvcc(), *NVCC_FLAGS, f"-I{INCLUDE}", *srcs, "-o", tmp]
+    cmd = [_nvcc(), *NVCC_FLAGS, f"-I{INCLUDE}", *srcs, "-o", tmp, *LIBS]
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, capture_output=True, text=True)

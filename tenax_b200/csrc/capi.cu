@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "planner.hpp"
+#include "svd.hpp"
 
 using namespace tnx;
 
@@ -1509,6 +1510,20 @@ int tnx_wait_flag(const int32_t* flag, int32_t expected, int64_t timeout_ns, int
       return set_err(TNX_ERR_VALUE, "tnx_wait_flag: timeout must be in (0, 10 s]");
     launch_wait_flag(flag, expected, static_cast<uint64_t>(timeout_ns), status, static_cast<cudaStream_t>(stream));
     CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
+
+int tnx_svd_batch(int32_t n, const int64_t* m, const int64_t* k, const double* const* a, double* const* u,
+                  double* const* s, double* const* vh, int64_t polar_min, int32_t n_workers, double* err_sigma,
+                  void* stream) {
+  TNX_TRY({
+    if (n < 0) return set_err(TNX_ERR_VALUE, "tnx_svd_batch: negative sector count");
+    if (n > 0 && (!m || !k || !a || !u || !s || !vh)) return set_err(TNX_ERR_VALUE, "tnx_svd_batch: null array");
+    std::vector<SvdJob> jobs(static_cast<size_t>(n));
+    for (int32_t i = 0; i < n; ++i) jobs[i] = SvdJob{m[i], k[i], a[i], u[i], s[i], vh[i]};
+    const double e = svd_batch(jobs, polar_min, n_workers, static_cast<cudaStream_t>(stream));
+    if (err_sigma) *err_sigma = e;
     return TNX_OK;
   })
 }
