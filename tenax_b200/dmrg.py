@@ -547,13 +547,6 @@ def dmrg(hamiltonian: TensorNetwork, initial_mps: TensorNetwork, config: DMRGCon
         raise _capi.TnxUnsupported("only two-site DMRG is implemented on the GPU path")
     prec = "fp64"
 
-    def build_left():
-        envs = [None] * (Ln + 1)
-        envs[0] = _trivial_env(True)
-        for i in range(Ln - 1):
-            envs[i + 1] = update_left_env(envs[i], mps[i], mpo[i], prec)
-        return envs
-
     def build_right():
         envs = [None] * (Ln + 1)
         envs[Ln] = _trivial_env(False)
@@ -561,7 +554,18 @@ def dmrg(hamiltonian: TensorNetwork, initial_mps: TensorNetwork, config: DMRGCon
             envs[i] = update_right_env(envs[i + 1], mps[i], mpo[i], prec)
         return envs
 
-    left, right = build_left(), build_right()
+    # The reference builds every left environment up front and rebuilds all
+    # left environments before each left-to-right pass and all right
+    # environments before each right-to-left pass (dmrg.py:170-172, :182-184,
+    # :225).  In the two-site sweep each pass reads left_envs[i] (resp.
+    # right_envs[i + 2]) only after its previous step has overwritten it, the
+    # boundary entries excepted, so none of those values is ever read: only
+    # the boundary left environment and the initial right environments (read
+    # by the first left-to-right pass) are computed here, and the sweep's
+    # results are the same.
+    left = [None] * (Ln + 1)
+    left[0] = _trivial_env(True)
+    right = build_right()
     energies, terrs = [], []
     energy, converged = 0.0, False
     for sweep in range(config.num_sweeps):
@@ -569,10 +573,6 @@ def dmrg(hamiltonian: TensorNetwork, initial_mps: TensorNetwork, config: DMRGCon
         t_sweep = time.perf_counter()
         n_site_stats = len(stats) if stats is not None else 0
         prev = energy
-        if sweep > 0:
-            t1 = time.perf_counter()
-            left = build_left()
-            _tick(phases, "env_rebuild", t1)
         for i in range(Ln - 1):
             r = right[i + 2] if right[i + 2] is not None else _trivial_env(False)
             th, e = two_site_update(mps[i], mps[i + 1], left[i], mpo[i], mpo[i + 1], r, config, stats, phases)
@@ -584,9 +584,6 @@ def dmrg(hamiltonian: TensorNetwork, initial_mps: TensorNetwork, config: DMRGCon
             terrs.append(err)
             left[i + 1] = update_left_env(left[i], A, mpo[i], prec)
             _tick(phases, "env", t1)
-        t1 = time.perf_counter()
-        right = build_right()
-        _tick(phases, "env_rebuild", t1)
         for i in range(Ln - 2, -1, -1):
             r2 = right[i + 2] if right[i + 2] is not None else _trivial_env(False)
             th, e = two_site_update(mps[i], mps[i + 1], left[i], mpo[i], mpo[i + 1], r2, config, stats, phases)
