@@ -396,14 +396,19 @@ def run_dmrg_study(args):
     out["plans"] = "contraction plan caches cleared before every run: each arm plans its own contractions"
     from tenax_b200 import contraction as _contraction, dense as _dense
 
-    for prec in args.dmrg_precisions.split(","):
+    polish = [int(x) for x in str(args.fp64_polish).split(",")]
+    arms = [(p, None) if p == "fp64" else (p, k) for p in args.dmrg_precisions.split(",")
+            for k in (polish if p != "fp64" else [None])]
+    for prec, k_polish in arms:
+        name = prec if (prec == "fp64" or len(polish) == 1) else f"{prec}/polish{k_polish}"
         _contraction._PLANS.clear()
         _dense._PLANS.clear()
         mps = random_symmetric_mps(Lx * Ly, args.chi, seed=args.seed)
         cfg = DMRGConfig(max_bond_dim=args.chi, num_sweeps=args.sweeps, lanczos_max_iter=args.lanczos,
                          convergence_tol=0.0, precision=prec, check_matvec_residual=prec != "fp64",
                          svd_driver=None if args.svd_driver == "default" else args.svd_driver,
-                         svd_streams=args.svd_streams)
+                         svd_streams=args.svd_streams,
+                         fp64_polish_steps=k_polish if k_polish is not None else DMRGConfig.fp64_polish_steps)
         stats: list = []
         phases: dict = {}
         res = dmrg(mpo, mps, cfg, stats, phases)
@@ -428,7 +433,9 @@ def run_dmrg_study(args):
             fp64_e = run["energies"]
         elif fp64_e is not None:
             run["dE_vs_fp64"] = [float(a - b) for a, b in zip(run["energies"], fp64_e)]
-        out["runs"][prec] = run
+        if k_polish is not None:
+            run["fp64_polish_steps"] = k_polish
+        out["runs"][name] = run
         del res, mps
         torch.cuda.empty_cache()
     print(json.dumps(out), flush=True)
@@ -697,6 +704,8 @@ def main():
                     help="per-sector SVD of the DMRG study: 'native' (tnx_svd_batch), a torch.linalg.svd driver, "
                          "or 'default'")
     ap.add_argument("--svd-streams", type=int, default=8)
+    ap.add_argument("--fp64-polish", default="3",
+                    help="FP64 Lanczos steps after a mixed solve (comma list: one mixed arm per value)")
     ap.add_argument("--ctm", action="store_true", help="run the dense CTMRG forward/gradient study instead")
     ap.add_argument("--ctm-chi", type=int, default=80)
     ap.add_argument("--ctm-iters", type=int, default=30)

@@ -97,8 +97,14 @@ struct Worker {
   Scratch ws, tall, utmp, info;
   std::vector<char> host_ws;
 
-  void init() {
-    SVD_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  // the first worker receives the largest sector (longest-first assignment)
+  // and gets the highest stream priority: its decomposition is the batch's
+  // critical path (8-worker batch of chi = 2048 sector shapes: 64-65 ms
+  // against 66-68 ms at equal priorities; the largest sector alone 42 ms)
+  void init(bool high) {
+    int least = 0, greatest = 0;
+    SVD_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    SVD_CUDA(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, high ? greatest : least));
     SVD_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
     SVD_SOLVER(cusolverDnCreate(&h));
     SVD_SOLVER(cusolverDnSetStream(h, st));
@@ -176,7 +182,7 @@ double svd_batch(const std::vector<SvdJob>& jobs, int64_t polar_min, int n_worke
   std::lock_guard<std::mutex> lk(pool.mu);
   while (static_cast<int>(pool.workers.size()) < n_workers) {
     pool.workers.emplace_back();
-    pool.workers.back().init();
+    pool.workers.back().init(pool.workers.size() == 1);
   }
   // longest first, greedy by m*k*min(m,k)
   std::vector<int> order;
