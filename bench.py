@@ -48,7 +48,11 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks/throttle reasons sampled every 100 ms.
+
+    Started before the warm-up (nvidia-smi takes a few hundred ms to print its
+    first line); ``mark_start``/``mark_end`` bracket the timed region on the
+    host clock and ``summary`` keeps only the samples read inside it."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -57,22 +61,33 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
-        self.lines: list = []
+        self.lines: list = []  # (host monotonic time read, line)
+        self.ready = threading.Event()
+        self.window = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
                  "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            self.ready.wait(timeout=10.0)
         except OSError:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+            self.ready.set()
+
+    def mark_start(self):
+        self.window = [time.monotonic(), None]
+
+    def mark_end(self):
+        if self.window is not None:
+            self.window[1] = time.monotonic()
 
     def __exit__(self, *a):
         if self.proc:
@@ -85,7 +100,10 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lo, hi = (self.window if self.window and self.window[1] is not None else (-1e300, 1e300))
+        for t, ln in self.lines:
+            if not lo <= t <= hi:
+                continue
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -145,18 +163,21 @@ def run_ours(args):
         batch = HeffBatch(ops)
         flops = batch.flops
         st = torch.cuda.current_stream()
+        if sampler:
+            sampler.__enter__()
         for _ in range(args.warmup):
             batch.apply(xs, ys)
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         if sampler:
-            sampler.__enter__()
+            sampler.mark_start()
         e0.record(st)
         for _ in range(args.steps):
             batch.apply(xs, ys)
         e1.record(st)
         barrier()
         if sampler:
+            sampler.mark_end()
             sampler.__exit__()
         ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
         err = batch.device_error()
