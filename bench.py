@@ -595,19 +595,21 @@ def run_split_ctm_study(args):
         torch.cuda.synchronize()
         return r, time.perf_counter() - t0, torch.cuda.max_memory_allocated() / 2 ** 30
 
-    for label, trivial in (("u1_charges_-2..2", False), ("trivial_charges", True)):
-        A = site(trivial, args.seed + 5)
-        Ad = A.todense()
-        run = {}
+    def arms(A, Ad, driver):
+        """FP64 free run (recording its projectors), split-BF16x3 run replaying
+        them, and forward+gradient of both with those projectors, all with
+        one edge-SVD driver."""
+        run = {"svd_driver": driver}
         rec: list = []
         with torch.no_grad():
-            env, t, mem = timed(lambda: gs.ctm_split_tensor(A, chi, iters, conv_tol=0.0, record=rec))
+            env, t, mem = timed(lambda: gs.ctm_split_tensor(A, chi, iters, conv_tol=0.0, record=rec,
+                                                            svd_driver=driver))
             E = float(gs.compute_energy_split_ctm_tensor(A, env, H, 2))
         run["fp64_forward"] = {"s": round(t, 3), "peak_GiB": round(mem, 2), "energy": E,
                                "env_max_abs": max(float(x.abs().max()) for x in env)}
         with torch.no_grad():
             envm, t, mem = timed(lambda: gs.ctm_split_tensor(A, chi, iters, conv_tol=0.0, projectors=rec,
-                                                            precision="bf16x3"))
+                                                             precision="bf16x3", svd_driver=driver))
             Em = float(gs.compute_energy_split_ctm_tensor(A, envm, H, 2))
         run["bf16x3_forward"] = {"s": round(t, 3), "peak_GiB": round(mem, 2), "energy": Em, "dE_vs_fp64": Em - E}
         grads = {}
@@ -615,7 +617,7 @@ def run_split_ctm_study(args):
             def fg():
                 x = Ad.clone().requires_grad_(True)
                 e = gs.ctm_split_tensor(A, chi, iters, conv_tol=0.0, projectors=rec, A_dense=x, precision=prec,
-                                        checkpoint_every=ck)
+                                        checkpoint_every=ck, svd_driver=driver)
                 En = gs.compute_energy_split_ctm_tensor(A, e, H, 2, A_dense=x)
                 (g,) = torch.autograd.grad(En, x)
                 return g
@@ -628,6 +630,18 @@ def run_split_ctm_study(args):
         g64, gmx = grads["fp64"], grads["bf16x3"]
         if torch.isfinite(g64).all() and torch.isfinite(gmx).all() and float(g64.abs().max()) > 0:
             run["grad_rel_err_bf16x3_vs_fp64"] = float((gmx - g64).abs().max() / g64.abs().max())
+        return run
+
+    out["note"] = ("the split-BF16x3 arms replay the FP64 run's projectors and compute their own edge SVDs; "
+                   "inside degenerate singular-value clusters the polar driver's basis moves with the "
+                   "perturbation, so the replayed projectors no longer match it: the Jacobi pair measures "
+                   "the arithmetic's effect")
+    for label, trivial in (("u1_charges_-2..2", False), ("trivial_charges", True)):
+        A = site(trivial, args.seed + 5)
+        Ad = A.todense()
+        run = arms(A, Ad, "polar")
+        if trivial:
+            run["jacobi_pair"] = arms(A, Ad, "jacobi")
         out["runs"][label] = run
     if not args.no_cpu_baseline:
         import oracle.split_ctm as osc

@@ -137,17 +137,87 @@ def fuse_dense(x, ax_a, ax_b, leg_a, leg_b, modulus):
     return nat[torch.from_numpy(inv)]
 
 
-def svd_split(T_full, chi_I, usv=None):
-    """(chi, D^2, chi) -> ket (chi, D, k), bra (k, D, chi) (:1058-1074)."""
+# Lorentzian width of the broadened SVD adjoint (algorithms/ad_utils.py:80)
+BROADENING = 1e-12
+
+
+class BroadenedSVD(torch.autograd.Function):
+    """Thin SVD whose reverse pass stays finite on degenerate spectra.
+
+    The reference differentiates ``jnp.linalg.svd`` and ``jnp.sqrt`` directly
+    (:1069-1071).  The first moves of every split CTM start from an
+    identity-like environment whose edges have exactly degenerate pairs and
+    exactly zero kept singular values, so that reverse pass is NaN there.
+    This adjoint is the one a finite gradient of the fixed-projector energy
+    needs.  It is Townsend's reverse mode ("Differentiating the singular value
+    decomposition", 2016) over all min(m, n) triplets.  The factor
+    1/(s_j^2 - s_i^2) is replaced by the Lorentzian d/(d^2 + eps^2),
+    d = s_j^2 - s_i^2, with the reference's eps (Francuz et al., PRR 7,
+    013237).  The caller truncates by slicing, so the coupling to the
+    discarded triplets is exact."""
+
+    @staticmethod
+    def forward(ctx, A):
+        U, s, Vh = torch.linalg.svd(A, full_matrices=False)
+        ctx.save_for_backward(U, s, Vh)
+        return U, s, Vh
+
+    @staticmethod
+    def backward(ctx, dU, ds, dVh):
+        U, s, Vh = ctx.saved_tensors
+        V = Vh.T
+        m, n, r = U.shape[0], V.shape[0], s.shape[0]
+        dU = torch.zeros_like(U) if dU is None else dU
+        ds = torch.zeros_like(s) if ds is None else ds
+        dV = torch.zeros_like(V) if dVh is None else dVh.T
+        d = s[None, :] ** 2 - s[:, None] ** 2
+        F = d / (d * d + BROADENING ** 2)
+        F = F * (1.0 - torch.eye(r, dtype=s.dtype))
+        a = U.T @ dU
+        b = V.T @ dV
+        inner = (F * (a - a.T)) @ torch.diag(s) + torch.diag(ds) + torch.diag(s) @ (F * (b - b.T))
+        dA = U @ inner @ Vh
+        s_inv = torch.where(s > BROADENING, 1.0 / s, torch.zeros_like(s))
+        if m > r:
+            dA = dA + ((dU - U @ a) @ torch.diag(s_inv)) @ Vh
+        if n > r:
+            dA = dA + U @ (torch.diag(s_inv) @ (dV - V @ b).T)
+        return dA
+
+
+class SqrtZeroSafe(torch.autograd.Function):
+    """sqrt(s) with derivative 0 at s == 0: the exactly zero singular values
+    of the first moves stay zero for every site tensor."""
+
+    @staticmethod
+    def forward(ctx, s):
+        r = torch.sqrt(s)
+        ctx.save_for_backward(r)
+        return r
+
+    @staticmethod
+    def backward(ctx, g):
+        (r,) = ctx.saved_tensors
+        safe = torch.where(r > 0, r, torch.ones_like(r))
+        return torch.where(r > 0, g / (2.0 * safe), torch.zeros_like(g))
+
+
+def svd_split(T_full, chi_I, usv=None, broadened=False):
+    """(chi, D^2, chi) -> ket (chi, D, k), bra (k, D, chi) (:1058-1074).
+
+    ``broadened`` differentiates through ``BroadenedSVD`` and ``SqrtZeroSafe``
+    instead of the plain SVD and sqrt; the forward values are the same."""
     chi, D2 = T_full.shape[0], T_full.shape[1]
     D = math.isqrt(D2)
     T_mat = T_full.reshape(chi, D, D, chi).reshape(chi * D, D * chi)
-    if usv is None:
-        U, s, Vh = torch.linalg.svd(T_mat, full_matrices=False)
-    else:
+    if usv is not None:
         U, s, Vh = usv
+    elif broadened:
+        U, s, Vh = BroadenedSVD.apply(T_mat)
+    else:
+        U, s, Vh = torch.linalg.svd(T_mat, full_matrices=False)
     k = min(chi_I, s.shape[0])
-    r = torch.sqrt(s[:k])
+    r = SqrtZeroSafe.apply(s[:k]) if broadened else torch.sqrt(s[:k])
     return (U[:, :k] * r[None, :]).reshape(chi, D, k), (r[:, None] * Vh[:k, :]).reshape(k, D, chi)
 
 
@@ -207,7 +277,8 @@ def grow_edge(site: Site, T_ket, T_bra, leg, out_order):
     return g.reshape(chi * D * D, D * D, chi * D * D)
 
 
-def move(env, legs, site: Site, name, chi, chi_I, projectors=None, svds=None, rec_p=None, rec_svd=None):
+def move(env, legs, site: Site, name, chi, chi_I, projectors=None, svds=None, rec_p=None, rec_svd=None,
+         broadened=False):
     """One directional move (_split_ctm_tensor.py:512-1050)."""
     mv = MOVES[name]
     mod = site.modulus
@@ -234,7 +305,7 @@ def move(env, legs, site: Site, name, chi, chi_I, projectors=None, svds=None, re
     Tg = grow_edge(site, env[e + "_ket"], env[e + "_bra"], mv["leg"], mv["out"])
     Tn = torch.einsum("ia,idj,jb->adb", Pf, Tg, Pf)
     usv = svds.pop(0) if svds else None
-    tk, tb = svd_split(Tn, chi_I, usv)
+    tk, tb = svd_split(Tn, chi_I, usv, broadened)
     if rec_svd is not None:
         rec_svd.append(Tn.detach())
     new[e + "_ket"] = tk * charge_mask(legs[e + "_ket"], mod)
@@ -256,15 +327,16 @@ def renormalize(env):
     return out
 
 
-def ctm_split(site: Site, chi, iters, chi_I=None, projectors=None, svds=None, rec_p=None):
-    """Fixed-count split CTM (ctm_split_tensor with conv_tol=0, :1243-1289)."""
+def ctm_split(site: Site, chi, iters, chi_I=None, projectors=None, svds=None, rec_p=None, broadened=False):
+    """Fixed-count split CTM (ctm_split_tensor with conv_tol=0, :1243-1289).
+    ``broadened``: the edge split's reverse pass through ``BroadenedSVD``."""
     chi_I = chi if chi_I is None else chi_I
     env, legs = init_env(site, chi, chi_I)
     ps = list(projectors) if projectors is not None else None
     sv = list(svds) if svds is not None else None
     for _ in range(iters):
         for name in ORDER:
-            env = move(env, legs, site, name, chi, chi_I, ps, sv, rec_p)
+            env = move(env, legs, site, name, chi, chi_I, ps, sv, rec_p, broadened=broadened)
         env = renormalize(env)
     return env
 

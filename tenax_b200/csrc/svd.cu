@@ -15,9 +15,9 @@
 //
 // cuSOLVER is column-major and the sector matrices are row-major.  A
 // row-major m x k buffer read column-major is the k x m transpose, so for
-// k >= m the buffer is decomposed as the tall matrix B = A^T = U_B S V_B^T:
+// k > m the buffer is decomposed as the tall matrix B = A^T = U_B S V_B^T:
 // U_B (k x m, column-major) is already Vh in row-major order, and U = V_B is
-// transposed.  For k < m the input is first transposed into a column-major
+// transposed.  For k <= m the input is first transposed into a column-major
 // m x k copy C = A = U_C S V_C^T: V_C (k x k, column-major) is Vh in row-major
 // order, and U = U_C is transposed.
 #include <cuda_runtime.h>
@@ -114,7 +114,9 @@ struct Worker {
 
   // one sector: a (m x k row-major) -> u (m x r), s (r), vh (r x k), r = min(m, k)
   double run(const SvdJob& j, bool polar, int* d_info) {
-    const bool wide = j.k >= j.m;  // the row-major buffer read column-major is already tall
+    // the row-major buffer read column-major is A^T: tall when k > m; square
+    // matrices take the transposed copy, so the solver sees A itself
+    const bool wide = j.k > j.m;
     const int64_t rows = wide ? j.k : j.m, cols = wide ? j.m : j.k;  // the tall column-major matrix
     double* t = static_cast<double*>(tall.need(sizeof(double) * static_cast<size_t>(rows * cols)));
     if (wide)

@@ -21,6 +21,7 @@ from tenax_b200 import _capi, vector
 from tenax_b200.contraction import blockwise_contract, contract
 from tenax_b200.core import FlowDirection, TensorIndex, U1Symmetry
 from tenax_b200.heff import HeffBatch, HeffOperator
+from tenax_b200.linalg import POLAR_MIN, svd_batch
 from tenax_b200.network import TensorNetwork
 from tenax_b200.tensor import SymmetricTensor, _device, block_shape, embed_in_keys, restrict_to_keys
 
@@ -238,35 +239,9 @@ def _svd_workers(device: torch.device, n: int):
     return w
 
 
-POLAR_MIN = 128
-
-
 def native_sector_svds(mats, n_workers: int = 8, polar_min: int = POLAR_MIN):
-    """Thin SVD of every sector matrix through ``tnx_svd_batch``: cuSOLVER's
-    polar-decomposition SVD for sectors with min(m, k) >= ``polar_min``, its
-    Jacobi SVD for the others, on up to ``n_workers`` library-owned streams,
-    one host thread each (the call blocks until all sectors are done).
-    Returns ``[(U, S, Vh), ...]`` like ``torch.linalg.svd(M, full_matrices=False)``."""
-    import ctypes as C
-
-    from . import _capi
-
-    if not mats:
-        return []
-    dev = mats[0].device
-    A = [M.to(torch.float64).contiguous() for M in mats]
-    n = len(A)
-    r = [min(M.shape) for M in A]
-    U = [torch.empty((M.shape[0], k), dtype=torch.float64, device=dev) for M, k in zip(A, r)]
-    S = [torch.empty((k,), dtype=torch.float64, device=dev) for k in r]
-    Vh = [torch.empty((k, M.shape[1]), dtype=torch.float64, device=dev) for M, k in zip(A, r)]
-    i64 = C.c_int64 * n
-    ptrs = C.c_void_p * n
-    _capi.check(_capi.LIB.tnx_svd_batch(
-        n, i64(*[M.shape[0] for M in A]), i64(*[M.shape[1] for M in A]), ptrs(*[M.data_ptr() for M in A]),
-        ptrs(*[x.data_ptr() for x in U]), ptrs(*[x.data_ptr() for x in S]), ptrs(*[x.data_ptr() for x in Vh]),
-        int(polar_min), int(n_workers), None, C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
-    return list(zip(U, S, Vh))
+    """The library's sector SVD batch (``tenax_b200.linalg.svd_batch``)."""
+    return svd_batch(mats, n_workers, polar_min)
 
 
 def sector_svds(mats, driver: str | None = None, n_streams: int = 1):

@@ -49,6 +49,7 @@ import torch.utils.checkpoint
 from tenax_b200 import _capi
 from tenax_b200.dense import contract, einsum
 from tenax_b200.ipeps import CTMEnvironment, compute_energy_ctm
+from tenax_b200.linalg import POLAR_MIN, svd as linalg_svd
 
 EPS = 1e-15  # tenax core/__init__.py:15
 LOG_EPS = 1e-250  # tenax core/__init__.py:16
@@ -220,8 +221,8 @@ SVD_BROADENING = 1e-12
 
 
 class _SVD(torch.autograd.Function):
-    """Reduced SVD A = U diag(s) V^T (FP64, cuSOLVER) with a reverse pass
-    that stays finite on degenerate spectra.
+    """Reduced SVD A = U diag(s) V^T (FP64, the library's cuSOLVER polar or
+    Jacobi SVD) with a reverse pass that stays finite on degenerate spectra.
 
     Reverse mode of the SVD (Townsend, "Differentiating the singular value
     decomposition", 2016), over all min(m, n) singular triplets:
@@ -240,8 +241,18 @@ class _SVD(torch.autograd.Function):
     exactly through F."""
 
     @staticmethod
-    def forward(ctx, A):
-        U, s, Vh = torch.linalg.svd(A, full_matrices=False)
+    def forward(ctx, A, polar_min=POLAR_MIN):
+        if int(torch.count_nonzero(A)) == 0:
+            # the zero edge of a collapsed environment (the U(1) runs): any
+            # orthonormal U, V; this one costs nothing (a polar decomposition
+            # of a zero matrix is slow)
+            m, n = A.shape
+            r = min(m, n)
+            U = torch.eye(m, r, dtype=A.dtype, device=A.device)
+            s = torch.zeros(r, dtype=A.dtype, device=A.device)
+            Vh = torch.eye(r, n, dtype=A.dtype, device=A.device)
+        else:
+            U, s, Vh = linalg_svd(A, polar_min)
         ctx.save_for_backward(U, s, Vh)
         ctx.shape = A.shape
         return U, s, Vh
@@ -271,7 +282,7 @@ class _SVD(torch.autograd.Function):
         if n > k:
             Y = gV - einsum("ni,ij->nj", V.contiguous(), VtgV.contiguous())
             gA = gA + einsum("mj,nj->mn", (U * sinv[None, :]).contiguous(), Y.contiguous())
-        return gA
+        return gA, None
 
 
 class _SqrtSV(torch.autograd.Function):
@@ -292,7 +303,8 @@ class _SqrtSV(torch.autograd.Function):
         return torch.where(r > 0, g / (2.0 * torch.where(r > 0, r, torch.ones_like(r))), torch.zeros_like(g))
 
 
-def _move(env: dict, S: _Structure, A, i, chi, chi_I, prec, P_in=None, svd_in=None, rec=None, probe=None):
+def _move(env: dict, S: _Structure, A, i, chi, chi_I, prec, P_in=None, svd_in=None, rec=None, probe=None,
+          polar_min=POLAR_MIN):
     mv = _MOVES[i]
     D = A.shape[0]
     (c1n, e1n, s1, ax1), (c2n, e2n, s2, ax2) = mv["c1"], mv["c2"]
@@ -335,7 +347,7 @@ def _move(env: dict, S: _Structure, A, i, chi, chi_I, prec, P_in=None, svd_in=No
     if svd_in is not None:
         U, s, Vh = svd_in
     else:
-        U, s, Vh = _SVD.apply(Tmat)
+        U, s, Vh = _SVD.apply(Tmat, polar_min)
     kk = min(chi_I, s.shape[0])
     rs = _SqrtSV.apply(s[:kk])
     tk = (U[:, :kk] * rs[None, :]).reshape(k, D, kk)
@@ -359,13 +371,13 @@ def _renormalize(env: dict) -> dict:
     return out
 
 
-def _sweeps(env: dict, S, A, chi, chi_I, renormalize, prec, n, Ps, svds, rec, p0, probe=None):
+def _sweeps(env: dict, S, A, chi, chi_I, renormalize, prec, n, Ps, svds, rec, p0, probe=None, polar_min=POLAR_MIN):
     for it in range(n):
         for i in range(4):
             j = 4 * (p0 + it) + i
             pin = None if Ps is None else (Ps[2 * j], Ps[2 * j + 1])
             sin = None if svds is None else svds[j]
-            env = _move(env, S, A, i, chi, chi_I, prec, pin, sin, rec, probe)
+            env = _move(env, S, A, i, chi, chi_I, prec, pin, sin, rec, probe, polar_min)
         if renormalize:
             env = _renormalize(env)
     return env
@@ -374,7 +386,7 @@ def _sweeps(env: dict, S, A, chi, chi_I, renormalize, prec, n, Ps, svds, rec, p0
 def ctm_split_tensor(A, chi: int, max_iter: int = 100, conv_tol: float = 1e-8, chi_I: int | None = None,
                      renormalize: bool = True, precision: str = "fp64", projectors=None, svds=None, record=None,
                      checkpoint_every: int = 0, A_dense: torch.Tensor | None = None,
-                     probe=None) -> SplitCTMTensorEnv:
+                     probe=None, svd_driver: str = "polar") -> SplitCTMTensorEnv:
     """Split CTM to convergence (_split_ctm_tensor.py:1243-1289).
 
     Stops when the normalised singular values of C1 change by less than
@@ -388,7 +400,16 @@ def ctm_split_tensor(A, chi: int, max_iter: int = 100, conv_tol: float = 1e-8, c
     differentiable input) while A supplies the leg charges.  ``probe``, if
     given, is called at every move (not under checkpointing) as
     probe(move, (g1, g2, P1), (h1, h2, P2)) with the two pairs of grown
-    corners and the projectors made from them -- a diagnostic hook."""
+    corners and the projectors made from them -- a diagnostic hook.
+    ``svd_driver`` picks the edge split's SVD: "polar" (the library's
+    polar-decomposition driver for edges of 128 and more, Jacobi below) or
+    "jacobi" (Jacobi for every edge).  Both agree to rounding, but inside
+    degenerate singular-value clusters they pick different bases, which the
+    later projectors depend on: runs that replay projectors recorded by
+    another run should use the recording run's driver."""
+    if svd_driver not in ("polar", "jacobi"):
+        raise ValueError(f"Unknown svd_driver {svd_driver!r}: expected 'polar' or 'jacobi'")
+    polar_min = POLAR_MIN if svd_driver == "polar" else 1 << 62
     chi_I = chi if chi_I is None else chi_I
     a, q, f, mod = _site(A)
     if A_dense is not None:
@@ -402,7 +423,8 @@ def ctm_split_tensor(A, chi: int, max_iter: int = 100, conv_tol: float = 1e-8, c
         if Ps is None:
             Ps = []
             with torch.no_grad():
-                _sweeps(dict(env), S, a.detach(), chi, chi_I, renormalize, precision, max_iter, None, svds, Ps, 0)
+                _sweeps(dict(env), S, a.detach(), chi, chi_I, renormalize, precision, max_iter, None, svds, Ps, 0,
+                        polar_min=polar_min)
         if record is not None:
             record.extend(Ps)
         done = 0
@@ -411,7 +433,8 @@ def ctm_split_tensor(A, chi: int, max_iter: int = 100, conv_tol: float = 1e-8, c
 
             def seg(*xs, _n=n, _p0=done):
                 e = dict(zip(_FIELDS, xs[:12]))
-                e = _sweeps(e, S, xs[12], chi, chi_I, renormalize, precision, _n, Ps, svds, None, _p0)
+                e = _sweeps(e, S, xs[12], chi, chi_I, renormalize, precision, _n, Ps, svds, None, _p0,
+                            polar_min=polar_min)
                 return tuple(e[k] for k in _FIELDS)
 
             out = torch.utils.checkpoint.checkpoint(seg, *[env[k] for k in _FIELDS], a, use_reentrant=False)
@@ -420,7 +443,8 @@ def ctm_split_tensor(A, chi: int, max_iter: int = 100, conv_tol: float = 1e-8, c
         return SplitCTMTensorEnv(**env)
     prev = None
     for it in range(max_iter):
-        env = _sweeps(env, S, a, chi, chi_I, renormalize, precision, 1, projectors, svds, record, it, probe)
+        env = _sweeps(env, S, a, chi, chi_I, renormalize, precision, 1, projectors, svds, record, it, probe,
+                      polar_min)
         if conv_tol > 0:
             with torch.no_grad():
                 sv = torch.linalg.svdvals(env["C1"])

@@ -6,9 +6,12 @@
 * Projectors computed on the GPU equal the reference's where the eigenvalue
   gap at the cut is clear (1e-10 on P P^T).
 * Gradient with the projectors fixed: equal to torch autograd of the oracle
-  (1e-10) and to central differences (h = 1e-6, relative 1e-6) on a case
-  whose edge spectra have no degeneracy across the truncation; recomputing
-  groups of sweeps (checkpointing) changes nothing.
+  with its broadened edge-split adjoint (1e-10) and to central differences
+  (h = 1e-6, relative 1e-6) on a case whose edge spectra have no nonzero
+  degeneracy across the truncation; recomputing groups of sweeps
+  (checkpointing) changes nothing.  The reference's own reverse pass (plain
+  SVD and sqrt) is NaN on these runs: their first moves start from an
+  identity-like environment with exactly degenerate and zero singular values.
 * The mixed-precision (split-BF16x3) forward moves the energy by < 2e-5.
 """
 
@@ -95,12 +98,12 @@ def test_projectors_match_reference(fix, name):
 
 
 def test_gradient_matches_oracle_and_fd(fix):
-    m, t, A, _, _, H = case(fix, "triv_d2_chi6")
+    """The projectors are the reference's recorded ones: a free run's
+    projectors depend on the gauge its edge SVDs chose inside degenerate
+    clusters, and so does the conditioning of the fixed-projector energy."""
+    m, t, A, rec, _, H = case(fix, "triv_d2_chi6")
     n, chi = m["iters"], m["chi"]
     Ad = A.todense()
-    rec: list = []
-    with torch.no_grad():
-        gs.ctm_split_tensor(A, chi, n, conv_tol=0.0, record=rec)
 
     def energy(x, grad=False, **kw):
         env = gs.ctm_split_tensor(A, chi, n, conv_tol=0.0, projectors=rec, A_dense=x, **kw)
@@ -111,10 +114,10 @@ def test_gradient_matches_oracle_and_fd(fix):
     x2 = Ad.clone().requires_grad_(True)
     (g_ck,) = torch.autograd.grad(energy(x2, checkpoint_every=2), x2)
     assert float((g_ck - g).abs().max()) <= 1e-13 * float(g.abs().max())
-    # oracle autograd under the same projectors
+    # oracle autograd under the same projectors, through the broadened edge-split adjoint
     a0 = torch.from_numpy(todense(t)).requires_grad_(True)
     site = osc.Site(a0, [l.charges for l in t.legs], [l.flow for l in t.legs])
-    E0 = osc.energy(site, osc.ctm_split(site, chi, n, projectors=[p.cpu() for p in rec]), H.cpu())
+    E0 = osc.energy(site, osc.ctm_split(site, chi, n, projectors=[p.cpu() for p in rec], broadened=True), H.cpu())
     (g0,) = torch.autograd.grad(E0, a0)
     assert float((g.cpu() - g0).abs().max()) <= 1e-10 * float(g0.abs().max())
     # central differences of the fixed-projector energy
@@ -140,3 +143,17 @@ def test_mixed_forward_close_to_fp64(fix):
         E64 = float(gs.compute_energy_split_ctm_tensor(A, e64, H, 2))
         Emx = float(gs.compute_energy_split_ctm_tensor(A, emx, H, 2))
     assert abs(Emx - E64) <= 2e-5
+
+
+def test_svd_driver_choice(fix):
+    """Both edge-SVD drivers give the same environment when nothing forces a
+    basis choice (the fixture's edges are 12 x 12, below the polar driver's
+    size, so both run Jacobi); an unknown driver is a ValueError."""
+    m, _, A, _, _, H = case(fix, "triv_d2_chi6")
+    with torch.no_grad():
+        ep = gs.ctm_split_tensor(A, m["chi"], m["iters"], conv_tol=0.0, svd_driver="polar")
+        ej = gs.ctm_split_tensor(A, m["chi"], m["iters"], conv_tol=0.0, svd_driver="jacobi")
+    for a, b in zip(ep, ej):
+        assert torch.equal(a, b)
+    with pytest.raises(ValueError, match="svd_driver"):
+        gs.ctm_split_tensor(A, m["chi"], 1, conv_tol=0.0, svd_driver="gesvd")
