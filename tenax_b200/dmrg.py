@@ -150,12 +150,22 @@ def lanczos(op: HeffOperator, theta: SymmetricTensor, num_steps: int, tol: float
 
     Krylov vectors live on the operator's closed key layout; alpha/beta and
     the early-exit flag stay on the device until the single read-back after
-    the loop.  Returns (eigenvalue, eigenvector SymmetricTensor with the
-    reference's key set, LanczosStats).
+    the loop.  ``fp64_op`` may also be a zero-argument callable returning
+    the FP64 operator: it is then called after the first loop is queued on
+    the device and before its read-back, so that the operator's host-side
+    planning overlaps the device work.  Returns (eigenvalue, eigenvector
+    SymmetricTensor with the reference's key set, LanczosStats).
     """
     t0 = time.perf_counter()
     x0 = embed_in_keys(theta, op.keys).data
-    energy, vec, m, a, b = _krylov(op, x0, num_steps, tol, tol_rel)
+    built = {}
+
+    def build():
+        if fp64_op is not None and not isinstance(fp64_op, HeffOperator):
+            built["op"] = fp64_op()
+
+    energy, vec, m, a, b = _krylov(op, x0, num_steps, tol, tol_rel, between=build)
+    fp64_op = built.get("op", fp64_op)
     key_seq = op.key_seq
     keys = key_seq[0] if m <= 1 else key_seq[min(m - 1, len(key_seq) - 1)]
     if fp64_op is not None and polish_steps > 0:
@@ -171,9 +181,11 @@ def lanczos(op: HeffOperator, theta: SymmetricTensor, num_steps: int, tol: float
     return energy, result, LanczosStats(m, a[:m], b[1:m + 1], time.perf_counter() - t0)
 
 
-def _krylov(op: HeffOperator, x0: torch.Tensor, num_steps: int, tol: float, tol_rel: float):
+def _krylov(op: HeffOperator, x0: torch.Tensor, num_steps: int, tol: float, tol_rel: float, between=None):
     """Device Lanczos loop from x0 on op's key layout: returns
-    (Ritz value, normalised Ritz vector, steps used, alphas, betas)."""
+    (Ritz value, normalised Ritz vector, steps used, alphas, betas).
+    ``between`` (if given) runs on the host once the loop is queued, before
+    the read-back waits for it."""
     dev = x0.device
     n = op.size
     basis = torch.empty((num_steps + 1, max(n, 1)), dtype=torch.float64, device=dev)
@@ -192,6 +204,8 @@ def _krylov(op: HeffOperator, x0: torch.Tensor, num_steps: int, tol: float, tol_
             w.data_ptr(), basis[k].data_ptr(), basis[k - 1].data_ptr() if k > 0 else 0,
             basis[k + 1].data_ptr(), n, alpha.data_ptr(), beta.data_ptr(), k, float(tol), float(tol_rel),
             done.data_ptr(), scr.data_ptr(), st))
+    if between is not None:
+        between()
     a = alpha.cpu().numpy()
     b = beta.cpu().numpy()
     if batch.device_error():
@@ -473,25 +487,36 @@ def two_site_update(site_l, site_r, L, Wl, Wr, R, config, stats: list | None = N
             theta = _pad(theta, False)
     t1 = _tick(phases, "theta", t0)
     op = HeffOperator(L, Wl, Wr, R, theta.indices, theta.keys, config.precision)
-    fp64_op = None
-    rel = None
-    if config.precision != "fp64" and config.fp64_energy:
-        fp64_op = HeffOperator(L, Wl, Wr, R, theta.indices, theta.keys, "fp64")
+    fp64 = {}
+
+    def make_fp64():
+        # built while the mixed Krylov loop runs (the polish and the FP64
+        # energy need it only after that loop's read-back)
+        fp64["op"] = HeffOperator(L, Wl, Wr, R, theta.indices, theta.keys, "fp64")
+        return fp64["op"]
+
+    need_fp64 = config.precision != "fp64" and config.fp64_energy
     t1 = _tick(phases, "operators", t1)
-    t_diag = time.perf_counter()
+    tol_rel = NOISE_REL.get(config.precision, 0.0) if config.lanczos_tol_rel is None else config.lanczos_tol_rel
+    energy, th, ls = lanczos(op, theta, config.lanczos_max_iter, config.lanczos_tol,
+                             make_fp64 if need_fp64 else None, tol_rel,
+                             config.fp64_polish_steps if need_fp64 else 0)
+    t1 = _tick(phases, "lanczos", t1)
+    rel = None
+    diag_s = 0.0
+    fp64_op = fp64.get("op")
     if fp64_op is not None and config.check_matvec_residual:
+        # diagnostic, excluded from the sweep time: mixed vs FP64 matvec of
+        # the initial theta (unchanged by the solve)
+        t_diag = time.perf_counter()
         x = embed_in_keys(theta, op.keys).data
         ym, yd = op.apply(x), fp64_op.apply(x)
         torch.cuda.synchronize()
         if op._batch.device_error() or fp64_op._batch.device_error():
             raise RuntimeError("tcgen05 GEMM reported a device-side timeout")
         rel = float(vector.nrm2(ym - yd)) / max(float(vector.nrm2(yd)), 1e-300)
-    diag_s = time.perf_counter() - t_diag if rel is not None else 0.0
-    t1 = _tick(phases, "residual_check", t1)
-    tol_rel = NOISE_REL.get(config.precision, 0.0) if config.lanczos_tol_rel is None else config.lanczos_tol_rel
-    energy, th, ls = lanczos(op, theta, config.lanczos_max_iter, config.lanczos_tol, fp64_op, tol_rel,
-                             config.fp64_polish_steps if fp64_op is not None else 0)
-    _tick(phases, "lanczos", t1)
+        diag_s = time.perf_counter() - t_diag
+        _tick(phases, "residual_check", t1)
     if ndim0 == 3:
         th = _unpad(th, pad_left)
     if stats is not None:
