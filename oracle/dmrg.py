@@ -152,7 +152,8 @@ def two_site_update(site_l, site_r, L, Wl, Wr, R, lanczos_max_iter, lanczos_tol)
     return th, e
 
 
-def truncated_svd(t: OTensor, left_labels, right_labels, new_bond_label, max_sv=None, max_err=None):
+def truncated_svd(t: OTensor, left_labels, right_labels, new_bond_label, max_sv=None, max_err=None,
+                  normalize=False):
     """Block-diagonal SVD with global truncation (linalg.py:75-333).
 
     Blocks are grouped by the fused flow-weighted charge of the left legs
@@ -218,6 +219,8 @@ def truncated_svd(t: OTensor, left_labels, right_labels, new_bond_label, max_sv=
     kept = pairs[:n_keep]
     bond_charges = np.array([q for _, q, _ in kept], dtype=np.int32)
     s_kept = np.array([v for v, _, _ in kept])
+    if normalize and s_kept.sum() > 0:  # linalg.py:251-252
+        s_kept = s_kept / s_kept.sum()
     cols: dict = {}
     for g, (_, q, i) in enumerate(kept):
         cols.setdefault(q, []).append((g, i))
