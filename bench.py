@@ -462,6 +462,75 @@ def run_dmrg_study(args):
     print(json.dumps(out), flush=True)
 
 
+def run_dmrg_c1_study(args):
+    """Config 1: two-site DMRG on the L=20 Heisenberg chain (Dw=5 MPO,
+    virtual charges -4..4, chi=64, 2 sweeps, 10 Lanczos steps) from the
+    fixture's MPO and random MPS (the inputs of the reference's own run,
+    tests/golden/dmrg_c1_L20.npz).  Times the whole dmrg() call on the GPU
+    (FP64 and split-BF16x3; the first call of a process, then a repeat) and
+    the oracle's port of the reference's algorithm on the host cores, and
+    compares every energy with the reference's."""
+    import time
+
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from fixture_io import unpack_tensor
+
+    from tenax_b200.core import FlowDirection, TensorIndex, U1Symmetry
+    from tenax_b200.dmrg import DMRGConfig, dmrg
+    from tenax_b200.network import TensorNetwork
+    from tenax_b200.tensor import SymmetricTensor
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    z = np.load(os.path.join(ROOT, "tests", "golden", "dmrg_c1_L20.npz"))
+    L = 20
+    host_mps = [unpack_tensor(z, f"mps{i}") for i in range(L)]
+    host_mpo = [unpack_tensor(z, f"mpo{i}") for i in range(L)]
+    e_ref = float(z["energy"])
+
+    def dev(t):
+        u1 = U1Symmetry()
+        idx = tuple(TensorIndex(u1, l.charges, FlowDirection(l.flow), l.label) for l in t.legs)
+        return SymmetricTensor(t.blocks, idx, _validate=False)
+
+    def nets():
+        mps, mpo = TensorNetwork("mps"), TensorNetwork("mpo")
+        for i in range(L):
+            mps.add_node(i, dev(host_mps[i]))
+            mpo.add_node(i, dev(host_mpo[i]))
+        return mpo, mps
+
+    out = {"study": "config 1: two-site DMRG, L=20 Heisenberg chain, chi=64, 2 sweeps, 10 Lanczos steps",
+           "data": "the reference run's own MPO and seeded random MPS (fixture)", "reference_energy": e_ref,
+           "runs": {}}
+    for prec in ("fp64", "bf16x3"):
+        run = {}
+        for label in ("first_call_s", "repeat_s"):
+            mpo, mps = nets()
+            cfg = DMRGConfig(max_bond_dim=64, num_sweeps=2, lanczos_max_iter=10, two_site=True, precision=prec)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = dmrg(mpo, mps, cfg)
+            torch.cuda.synchronize()
+            run[label] = round(time.perf_counter() - t0, 3)
+            run["energy"] = float(res.energy)
+            run["dE_vs_reference"] = float(res.energy) - e_ref
+        out["runs"][prec] = run
+    if not args.no_cpu_baseline:
+        import oracle.dmrg as odmrg
+
+        t0 = time.perf_counter()
+        res = odmrg.dmrg(host_mpo, host_mps, max_bond_dim=64, num_sweeps=2, lanczos_max_iter=10)
+        t1 = time.perf_counter() - t0
+        e = float(res[0] if isinstance(res, tuple) else res)
+        out["cpu_baseline"] = {"value": round(t1, 2), "unit": "s (whole run)", "cores": os.cpu_count(),
+                               "kind": "port", "energy": e, "dE_vs_reference": e - e_ref,
+                               "sample": "the whole config-1 run: the oracle's NumPy port of the reference's "
+                                         "dmrg() with BLAS on all host cores"}
+    print(json.dumps(out), flush=True)
+
+
 def run_ctm_study(args):
     """Dense 1-site CTMRG (D=4, d=2, chi=80, 30 QR sweeps, square-lattice
     Heisenberg NN energy): forward and forward+gradient seconds on the GPU,
@@ -730,6 +799,8 @@ def run_ctm_tensor_study(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--dmrg", action="store_true", help="run the cylinder DMRG precision study instead")
+    ap.add_argument("--dmrg-c1", action="store_true",
+                    help="run the config-1 chain DMRG (GPU path against the oracle's CPU port) instead")
     ap.add_argument("--chi", type=int, default=2048)
     ap.add_argument("--sweeps", type=int, default=4)
     ap.add_argument("--lanczos", type=int, default=20)
@@ -770,6 +841,8 @@ def main():
     sys.path.insert(0, ROOT)
     if args.dmrg:
         run_dmrg_study(args)
+    elif args.dmrg_c1:
+        run_dmrg_c1_study(args)
     elif args.ctm:
         run_ctm_study(args)
     elif args.split_ctm:
