@@ -3,7 +3,8 @@
 // C_g[row, col] = sum_k A_g[row, k] * B_g[col, k] over every sector group g,
 // one work-list entry per 128x128 output tile.  Operands are pre-swizzled
 // SWIZZLE_128B K-major image tiles (16 KB each) moved by 1-D bulk async copies
-// (cp.async.bulk, no tensor map, no multicast) into a STAGES-deep ring.
+// (cp.async.bulk, no tensor map; every CTA fetches its own tiles) into a
+// STAGES-deep ring.
 //   BF16X3: A = A_hi + A_lo, B = B_hi + B_lo (bf16 splits of FP64 data);
 //           acc += A_hi B_hi + A_hi B_lo + A_lo B_hi, FP32 accumulation in TMEM.
 //   TF32:   acc += A B with kind::tf32.
