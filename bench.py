@@ -278,10 +278,42 @@ def run_ours(args):
         }
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(problems, rmx["per_problem_flops"], budget_s=args.cpu_budget)
+        if world == 1 and not args.no_dmrg:
+            del problems
+            torch.cuda.empty_cache()
+            out["dmrg"] = dmrg_sweeps(chi=args.chi, sweeps=2, lanczos=args.lanczos, seed=args.seed)
         print(json.dumps(out), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def dmrg_sweeps(chi=2048, sweeps=2, lanczos=20, seed=0):
+    """The sweep-seconds half of the metric, compactly: two-site DMRG on the
+    4x6 Heisenberg cylinder at chi (the --dmrg study's workload, fewer
+    sweeps), FP64 and split-BF16x3, each arm with empty plan caches.
+    Returns per-sweep seconds, final energies and their difference."""
+    from tenax_b200 import contraction as _contraction, dense as _dense
+    from tenax_b200.dmrg import DMRGConfig, SweepStats, dmrg
+    from tenax_b200.workloads import cylinder_mpo, random_symmetric_mps
+
+    mpo = cylinder_mpo(4, 6)
+    res = {"workload": f"two-site DMRG, 4x6 Heisenberg cylinder (U(1), Dw=26), chi={chi}, {sweeps} sweeps, "
+                       f"{lanczos} Lanczos steps, seeded random initial MPS", "sweep_s": {}, "energy": {}}
+    for prec in ("fp64", "bf16x3"):
+        _contraction._PLANS.clear()
+        _dense._PLANS.clear()
+        mps = random_symmetric_mps(24, chi, seed=seed)
+        cfg = DMRGConfig(max_bond_dim=chi, num_sweeps=sweeps, lanczos_max_iter=lanczos, convergence_tol=0.0,
+                         precision=prec)
+        stats: list = []
+        r = dmrg(mpo, mps, cfg, stats)
+        res["sweep_s"][prec] = [round(x.seconds, 3) for x in stats if isinstance(x, SweepStats)]
+        res["energy"][prec] = float(r.energy)
+        del r, mps
+    res["dE_vs_fp64"] = res["energy"]["bf16x3"] - res["energy"]["fp64"]
+    res["last_sweep_fp64_over_mixed"] = round(res["sweep_s"]["fp64"][-1] / res["sweep_s"]["bf16x3"][-1], 3)
+    return res
 
 
 def _host_problem(p):
@@ -832,6 +864,7 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-dmrg", action="store_true", help="leave the 2-sweep chi=2048 DMRG out of the default run")
     ap.add_argument("--ref-problems", type=int, default=2)
     ap.add_argument("--problems", type=int, default=N_PROBLEMS,
                     help="problems per GPU (64 = the benchmark workload; smaller only for profiling)")
