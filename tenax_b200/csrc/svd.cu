@@ -58,6 +58,8 @@ void transpose(const double* in, double* out, int64_t rows, int64_t cols, cudaSt
   const dim3 grid(static_cast<unsigned>((cols + 31) / 32), static_cast<unsigned>((rows + 31) / 32));
   if (grid.y > 65535u) throw PlanError{TNX_ERR_UNSUPPORTED, "sector matrix too tall for the transpose grid"};
   transpose_cm_to_rm<<<grid, dim3(32, 8), 0, st>>>(in, out, rows, cols);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw PlanError{TNX_ERR_CUDA, std::string("transpose launch: ") + cudaGetErrorString(e)};
 }
 
 #define SVD_CUDA(x)                                                                                   \
