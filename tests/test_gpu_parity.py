@@ -176,3 +176,26 @@ def test_vector_primitives():
     n = float(vector.nrm2(x))
     assert abs(d - float(torch.dot(x, y))) < 1e-9 * max(1.0, abs(d))
     assert abs(n - float(torch.linalg.norm(x))) < 1e-12 * n
+
+
+@pytest.mark.parametrize("steps", [1, 2, 3])
+def test_batch_host_streaming_short_runs(steps):
+    """The streamed apply's pipeline edges: with 1, 2 or 3 steps the copy-in
+    of step s+1 and copy-out of step s-1 have nothing (or one step) to overlap
+    with; every output still equals the device-resident apply bit for bit."""
+    probs = [_random_problem(c, s, n_sectors=8, hi=40) for c, s in ((96, 4), (140, 5))]
+    ops = [tb.HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, "bf16x3") for p in probs]
+    batch = tb.HeffBatch(ops)
+    rng = np.random.default_rng(11 + steps)
+    h_in = [torch.from_numpy(rng.standard_normal(batch.total)).pin_memory() for _ in range(steps)]
+    h_out = [torch.full((batch.total,), np.nan, dtype=torch.float64).pin_memory() for _ in range(steps)]
+    batch.apply_host(h_in, h_out)
+    torch.cuda.synchronize()
+    for s in range(steps):
+        x = h_in[s].cuda()
+        y = torch.empty_like(x)
+        batch.apply([x[o:o + op.size] for o, op in zip(batch.offsets, ops)],
+                    [y[o:o + op.size] for o, op in zip(batch.offsets, ops)])
+        torch.cuda.synchronize()
+        torch.testing.assert_close(h_out[s], y.cpu(), rtol=0, atol=0)
+    assert batch.device_error() == 0
