@@ -103,12 +103,12 @@ def test_fused_heff_golden(golden_dir, precision, tol):
     assert rel_err({k: v for k, v in got.items() if k in ref}, ref) < tol
 
 
-def _random_problem(chi, seed, n_sectors=12, hi=64, cylinder=True):
+def _random_problem(chi, seed, n_sectors=12, hi=64, cylinder=True, lo=4):
     from tenax_b200 import workloads as W
 
     Wl, Wr = W.cylinder_bulk_w() if cylinder else W.chain_bulk_w()
     gen = np.random.default_rng(seed)
-    return W.make_heff_problem(chi, chi, Wl, Wr, gen, n_sectors=n_sectors, hi=hi)
+    return W.make_heff_problem(chi, chi, Wl, Wr, gen, n_sectors=n_sectors, hi=hi, lo=lo)
 
 
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("bf16x3", 2e-5)])
@@ -123,6 +123,29 @@ def test_fused_heff_random_multi_tile(precision, tol):
     got = SymmetricTensor.from_flat(p.theta.indices, op.keys, y).numpy_blocks()
     ref = o_blockwise([to_host(t) for t in (p.L, x, p.Wl, p.Wr, p.R)], "abc,apqd,bpse,eqtf,dfg->cstg").blocks
     assert rel_err(got, ref) < tol
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("bf16x3", 2e-5)])
+@pytest.mark.parametrize("shape", ["tiny_sectors", "wide_sectors"])
+def test_fused_heff_sector_extremes(shape, precision, tol):
+    """Sectors of extent 1-6 (every tile mostly padding; K below one MMA step)
+    and sectors up to 320 wide (several K slabs in stage 1, two N tiles)
+    against the oracle's per-combination H_eff."""
+    if shape == "tiny_sectors":
+        p = _random_problem(30, 9, n_sectors=12, hi=6, lo=1)
+    else:
+        p = _random_problem(1400, 10, n_sectors=8, hi=320, cylinder=False)
+    op = tb.HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, precision)
+    x = embed_in_keys(p.theta, op.keys)
+    y = op.apply(x.data)
+    torch.cuda.synchronize()
+    assert op._batch.device_error() == 0
+    got = SymmetricTensor.from_flat(p.theta.indices, op.keys, y).numpy_blocks()
+    ref = o_blockwise([to_host(t) for t in (p.L, x, p.Wl, p.Wr, p.R)], "abc,apqd,bpse,eqtf,dfg->cstg").blocks
+    for k in got:
+        if k not in ref:
+            assert np.all(got[k] == 0.0), k
+    assert rel_err({k: v for k, v in got.items() if k in ref}, ref) < tol
 
 
 def test_batch_equals_individual():
