@@ -195,11 +195,16 @@ def _krylov(op: HeffOperator, x0: torch.Tensor, num_steps: int, tol: float, tol_
     w = torch.empty(max(n, 1), dtype=torch.float64, device=dev)
     nrm = vector.nrm2(x0)
     vector.scale(x0, nrm, 2, out=basis[0, :n])
-    batch = HeffBatch([op], skip_flag=done)
+    # fused operators skip their kernels once the early-exit flag is set; a
+    # general-path operator applies every step (the extra results are unused)
+    batch = HeffBatch([op], skip_flag=done) if op.fused else None
     scr = vector.scratch(dev)
     st = torch.cuda.current_stream().cuda_stream
     for k in range(num_steps):
-        batch.apply([basis[k, :n]], [w[:n]])
+        if batch is not None:
+            batch.apply([basis[k, :n]], [w[:n]])
+        else:
+            op.apply(basis[k, :n], w[:n])
         _capi.check(_capi.LIB.tnx_lanczos_step(
             w.data_ptr(), basis[k].data_ptr(), basis[k - 1].data_ptr() if k > 0 else 0,
             basis[k + 1].data_ptr(), n, alpha.data_ptr(), beta.data_ptr(), k, float(tol), float(tol_rel),
@@ -208,7 +213,7 @@ def _krylov(op: HeffOperator, x0: torch.Tensor, num_steps: int, tol: float, tol_
         between()
     a = alpha.cpu().numpy()
     b = beta.cpu().numpy()
-    if batch.device_error():
+    if batch is not None and batch.device_error():
         raise RuntimeError("tcgen05 GEMM reported a device-side timeout")
     m = num_steps
     for k in range(num_steps):
@@ -512,7 +517,7 @@ def two_site_update(site_l, site_r, L, Wl, Wr, R, config, stats: list | None = N
         x = embed_in_keys(theta, op.keys).data
         ym, yd = op.apply(x), fp64_op.apply(x)
         torch.cuda.synchronize()
-        if op._batch.device_error() or fp64_op._batch.device_error():
+        if op.device_error() or fp64_op.device_error():
             raise RuntimeError("tcgen05 GEMM reported a device-side timeout")
         rel = float(vector.nrm2(ym - yd)) / max(float(vector.nrm2(yd)), 1e-300)
         diag_s = time.perf_counter() - t_diag

@@ -75,8 +75,18 @@ def _closure(L, th_indices, th_keys, Wl, Wr, R, precision, max_iter: int = 64):
     raise RuntimeError("H_eff key closure did not converge")
 
 
+HEFF_SUBSCRIPTS = "abc,apqd,bpse,eqtf,dfg->cstg"  # algorithms/dmrg.py:1282-1289
+
+
 class HeffOperator:
-    """H_eff of one two-site problem; theta/outputs live on a closed key set."""
+    """H_eff of one two-site problem; theta/outputs live on a closed key set.
+
+    The fused path (four launches per apply, batchable) needs every stage-4
+    group to write a single output charge, which the sector structures of
+    U(1) MPS/MPO problems satisfy.  Other structures (``fused`` False) apply
+    H_eff through the general unfiltered contraction engine, the
+    reference's ``_blockwise_contract`` semantics, one pairwise chain per
+    apply: the same result, without the fused kernels."""
 
     def __init__(self, L: SymmetricTensor, Wl: SymmetricTensor, Wr: SymmetricTensor, R: SymmetricTensor,
                  theta_indices, theta_keys, precision: str = "fp64"):
@@ -86,15 +96,16 @@ class HeffOperator:
         self.keys = self.key_seq[-1]
         closed = C.c_int32()
         _capi.check(_capi.LIB.tnx_heff_closed(self.handle, C.byref(closed)))
-        if not closed.value:
-            raise _capi.TnxUnsupported("H_eff sector structure outside the fused path (a stage-4 group spans "
-                                       "several output charges)")
+        self.fused = bool(closed.value)
         self.precision = precision
         self.flops = float(_capi.LIB.tnx_heff_flops(self.handle))
-        _capi.check(_capi.LIB.tnx_heff_set_operators(self.handle, L.data.data_ptr(), Wl.data.data_ptr(),
-                                                     Wr.data.data_ptr(), R.data.data_ptr(),
-                                                     _capi.PRECISIONS[precision],
-                                                     torch.cuda.current_stream().cuda_stream))
+        if self.fused:
+            _capi.check(_capi.LIB.tnx_heff_set_operators(self.handle, L.data.data_ptr(), Wl.data.data_ptr(),
+                                                         Wr.data.data_ptr(), R.data.data_ptr(),
+                                                         _capi.PRECISIONS[precision],
+                                                         torch.cuda.current_stream().cuda_stream))
+        else:
+            self._operands = (L, Wl, Wr, R)
         sizes = [int(np.prod([int(np.count_nonzero(i.charges == q)) for i, q in zip(self.theta_indices, k)]))
                  for k in self.keys]
         self.size = int(sum(sizes))
@@ -104,12 +115,26 @@ class HeffOperator:
         return torch.empty(self.size, dtype=torch.float64, device=torch.device("cuda", torch.cuda.current_device()))
 
     def apply(self, x: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
-        if self._batch is None:
-            self._batch = HeffBatch([self])
         if out is None:
             out = self.out_like()
+        if not self.fused:
+            from tenax_b200.contraction import blockwise_contract
+            from tenax_b200.tensor import embed_in_keys
+
+            L, Wl, Wr, R = self._operands
+            th = SymmetricTensor.from_flat(self.theta_indices, self.keys, x)
+            y = blockwise_contract([L, th, Wl, Wr, R], HEFF_SUBSCRIPTS, self.theta_indices,
+                                   None if self.precision == "fp64" else self.precision)
+            out.copy_(embed_in_keys(y, self.keys).data)
+            return out
+        if self._batch is None:
+            self._batch = HeffBatch([self])
         self._batch.apply([x], [out])
         return out
+
+    def device_error(self) -> int:
+        """The fused kernels' device-side timeout flag (0 on the general path)."""
+        return self._batch.device_error() if self._batch is not None else 0
 
     def __del__(self):
         if getattr(self, "handle", None) is not None and _capi.LIB is not None:
@@ -123,6 +148,9 @@ class HeffBatch:
 
     def __init__(self, ops, skip_flag: torch.Tensor | None = None):
         self.ops = list(ops)
+        if not all(o.fused for o in self.ops):
+            raise _capi.TnxUnsupported("HeffBatch needs the fused H_eff path: an operator's sector structure "
+                                       "has a stage-4 group writing several output charges")
         prec = {o.precision for o in self.ops}
         if len(prec) != 1:
             raise ValueError("all problems of a batch must use one precision")

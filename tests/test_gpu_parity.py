@@ -91,6 +91,7 @@ def test_fused_heff_golden(golden_dir, precision, tol):
     z, (L, th, Wl, Wr, R) = _heff_fixture(golden_dir)
     dL, dth, dWl, dWr, dR = map(to_dev, (L, th, Wl, Wr, R))
     op = tb.HeffOperator(dL, dWl, dWr, dR, dth.indices, dth.keys, precision)
+    assert op.fused  # the U(1) two-site structure takes the fused kernels
     x = embed_in_keys(dth, op.keys)
     y = op.apply(x.data)
     torch.cuda.synchronize()
@@ -146,6 +147,54 @@ def test_fused_heff_sector_extremes(shape, precision, tol):
         if k not in ref:
             assert np.all(got[k] == 0.0), k
     assert rel_err({k: v for k, v in got.items() if k in ref}, ref) < tol
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("bf16x3", 2e-5)])
+def test_heff_z3(precision, tol):
+    """H_eff on Z3 charges: random charge-conserving operands with the
+    two-site problem's legs and flows (L, theta, W_l, W_r, R), against the
+    oracle's per-combination H_eff (blocks match by charge value,
+    dmrg.py:1094-1136).  Such structures may have stage-4 groups that write
+    several output charges; the operator then takes the general contraction
+    path, and Lanczos on it must still reach the oracle's eigenvalue."""
+    from oracle.blocksparse import random_tensor
+
+    u = _random_problem(40, 12, n_sectors=6, hi=12, cylinder=False)
+    rng = np.random.default_rng(12)
+    bond = np.array([0] * 5 + [1] * 7 + [2] * 6, np.int32)
+    mpo = np.array([0, 1, 2, 0, 1], np.int32)
+    phys = np.array([0, 2], np.int32)
+    charges = {"vl": bond, "vl_c": bond, "vr": bond, "vr_c": bond, "wl": mpo, "wr": mpo, "p1": phys, "p2": phys}
+
+    def z3_like(t, leg_charges):
+        legs = tuple(Leg(leg_charges[i], int(ix.flow), ix.label) for i, ix in enumerate(t.indices))
+        return random_tensor(legs, rng, 3, 0)
+
+    L = z3_like(u.L, [charges[i.label] for i in u.L.indices])
+    R = z3_like(u.R, [charges[i.label] for i in u.R.indices])
+    th = z3_like(u.theta, [charges[i.label] for i in u.theta.indices])
+    # W_l (b, p, s, e) and W_r (e, q, t, f): MPO legs carry mpo charges, physical legs phys charges
+    Wl = z3_like(u.Wl, [mpo, phys, phys, mpo])
+    Wr = z3_like(u.Wr, [mpo, phys, phys, mpo])
+    dL, dth, dWl, dWr, dR = map(to_dev, (L, th, Wl, Wr, R))
+    op = tb.HeffOperator(dL, dWl, dWr, dR, dth.indices, dth.keys, precision)
+    x = embed_in_keys(dth, op.keys)
+    y = op.apply(x.data)
+    torch.cuda.synchronize()
+    assert op.device_error() == 0
+    got = SymmetricTensor.from_flat(dth.indices, op.keys, y).numpy_blocks()
+    ref = o_blockwise([L, to_host(x), Wl, Wr, R], "abc,apqd,bpse,eqtf,dfg->cstg").blocks
+    assert ref
+    for k in got:
+        if k not in ref:
+            assert np.all(got[k] == 0.0), k
+    assert rel_err({k: v for k, v in got.items() if k in ref}, ref) < tol
+    if precision == "fp64":
+        from tenax_b200 import dmrg as gd
+
+        e, _, _ = gd.lanczos(op, dth, 8, 1e-12)
+        e_ref = odmrg.lanczos(lambda v: odmrg.heff_matvec(L, v, Wl, Wr, R), th, 8, 1e-12)[0]
+        assert abs(e - float(e_ref)) <= 1e-9 * max(1.0, abs(float(e_ref)))
 
 
 def test_batch_equals_individual():
