@@ -102,9 +102,13 @@ void tnx_plan_destroy(tnx_plan* plan);
  * file-scope 16 MiB device array that every GPU loading this library holds
  * until exit.  Plans that need more scratch fail with TNX_ERR_VALUE.  The
  * first call on a device looks up that array's device address (with that
- * device current), so make it before any stream capture.  All calls share
- * the array: calls that overlap on the GPU race on it.  Allocates nothing:
- * no cudaMalloc/cudaFree and no allocating library routine. */
+ * device current).  Every call copies its tables, operand pointers and a
+ * scalar from pageable host memory with cudaMemcpyAsync, so no call may be
+ * made under stream capture (a CUDA graph or a command buffer): an XLA FFI
+ * handler wrapping it must not declare itself command-buffer compatible.
+ * All calls share the array: calls that overlap on the GPU race on it.
+ * Allocates nothing: no cudaMalloc/cudaFree and no allocating library
+ * routine. */
 int tnx_plan_execute_static(const tnx_plan* plan, const double* const* inputs, double* out, void* stream);
 
 /* Two-site effective Hamiltonian "abc,apqd,bpse,eqtf,dfg->cstg"

@@ -33,6 +33,59 @@ def heff_matvec(L, theta, Wl, Wr, R):
     return blockwise_contract([L, theta, Wl, Wr, R], HEFF_SUBSCRIPTS, out_legs=theta.legs)
 
 
+def heff_flops(L, theta, Wl, Wr, R) -> float:
+    """Algorithmic FLOPs of one two-site H_eff application, counted from the
+    stored block dims of the operands (the reference's sector structure,
+    ``algorithms/dmrg.py:1282-1289``) over the canonical four pairwise stages:
+    L.theta over a; .W_l over (b, p); .W_r over (e, q); .R over (d, f).
+    Each stage sums 2*m*n*k over its matching block pairs; blocks of zero
+    size are skipped; the stage-3 inputs are the distinct stage-2 result
+    blocks.  No padding and no dense equivalent."""
+    def shapes(t):
+        return {k: tuple(int(x) for x in np.shape(v)) for k, v in t.blocks.items() if np.size(v) > 0}
+
+    sL, sT, sWl, sWr, sR = map(shapes, (L, theta, Wl, Wr, R))
+    # stage 1: X1[b,c,p,q,d] = L[a,b,c] theta[a,p,q,d]
+    rows, cols, ka = {}, {}, {}
+    for (qa, qb, qc), (ma, mb, mc) in sL.items():
+        rows[qa] = rows.get(qa, 0) + mb * mc
+        ka[qa] = ma
+    for (qa, qp, qq, qd), (ma, mp, mq, md) in sT.items():
+        cols[qa] = cols.get(qa, 0) + mp * mq * md
+    flops = sum(2.0 * rows[q] * cols[q] * ka[q] for q in rows if q in cols)
+    x1 = {}
+    for (qa, qb, qc), (ma, mb, mc) in sL.items():
+        for (qa2, qp, qq, qd), (_, mp, mq, md) in sT.items():
+            if qa2 == qa:
+                x1[(qb, qc, qp, qq, qd)] = (mb, mc, mp, mq, md)
+    # stage 2: X2[c,s,e,q,d] = X1[b,c,p,q,d] W_l[b,p,s,e]
+    wl_by = {}
+    for (qb, qp, qs, qe), d in sWl.items():
+        wl_by.setdefault((qb, qp), []).append(((qs, qe), d))
+    x2 = {}
+    for (qb, qc, qp, qq, qd), (mb, mc, mp, mq, md) in x1.items():
+        for (qs, qe), (_, _, ms, me) in wl_by.get((qb, qp), []):
+            x2[(qc, qs, qe, qq, qd)] = (mc, ms, me, mq, md)
+            flops += 2.0 * (mc * mq * md) * (ms * me) * (mb * mp)
+    # stage 3: X3[c,s,t,f,d] = X2[c,s,e,q,d] W_r[e,q,t,f]
+    wr_by = {}
+    for (qe, qq, qt, qf), d in sWr.items():
+        wr_by.setdefault((qe, qq), []).append(((qt, qf), d))
+    x3 = {}
+    for (qc, qs, qe, qq, qd), (mc, ms, me, mq, md) in x2.items():
+        for (qt, qf), (_, _, mt, mf) in wr_by.get((qe, qq), []):
+            x3[(qc, qs, qt, qf, qd)] = (mc, ms, mt, mf, md)
+            flops += 2.0 * (mc * ms * md) * (mt * mf) * (me * mq)
+    # stage 4: Y[c,s,t,g] = X3[c,s,t,f,d] R[d,f,g]
+    r_by = {}
+    for (qd, qf, qg), (md, mf, mg) in sR.items():
+        r_by.setdefault((qf, qd), []).append(mg)
+    for (qc, qs, qt, qf, qd), (mc, ms, mt, mf, md) in x3.items():
+        for mg in r_by.get((qf, qd), []):
+            flops += 2.0 * (mc * ms * mt) * mg * (mf * md)
+    return float(flops)
+
+
 def lanczos(matvec, initial, num_steps, tol):
     """Plain 3-term Lanczos (algorithms/dmrg.py:978-1045).
 

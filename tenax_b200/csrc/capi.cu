@@ -828,7 +828,9 @@ extern "C" int tnx_plan_execute_static(const tnx_plan* plan, const double* const
                                             "holds " + std::to_string(kStaticArenaBytes) + " bytes");
         if (pass == 0) continue;
         const double* a_ptr = plan->a_src[s] >= 0 ? inputs[plan->a_src[s]] : inter[s - 1];
-        const double* b_ptr = inputs[plan->b_src[s]];
+        // a single-operand plan pairs its operand with the scalar 1.0: its
+        // caller passes one input pointer, so inputs[b_src] is never read
+        const double* b_ptr = plan->has_scalar ? nullptr : inputs[plan->b_src[s]];
         if (plan->has_scalar) {
           const double v1 = 1.0;
           CUDA_OK(cudaMemcpyAsync(one, &v1, sizeof(double), cudaMemcpyHostToDevice, st));

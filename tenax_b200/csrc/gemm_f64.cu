@@ -134,11 +134,11 @@ void launch_gemm_f64(const DevGroup* groups, const DevTile* tiles, int n_tiles, 
                      const uint64_t* out_tab, const int32_t* skip, cudaStream_t st) {
   if (n_tiles <= 0) return;
   const int smem = 2 * STAGES * TILE_DBL * static_cast<int>(sizeof(double));
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr_set = true;
-  }
+  // set on every launch: the attribute belongs to the current device, and one
+  // process may drive several.  A failure is the thread's last CUDA error,
+  // which every caller checks after its launches.
+  if (cudaFuncSetAttribute(gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+    return;
   int grid = device_sm_count() * 3;
   if (grid > n_tiles) grid = n_tiles;
   gemm_f64_kernel<<<grid, THREADS, smem, st>>>(groups, tiles, n_tiles, rowoff, out_tab, skip);

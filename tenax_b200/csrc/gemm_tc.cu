@@ -440,7 +440,9 @@ void launch_tc_impl(const DevGroup* groups, const DevTile* tiles, int n_tiles, c
   constexpr int NT = TF32 ? 2 : 4;
   constexpr int STAGES = TF32 ? 6 : 3;
   const int smem = STAGES * NT * TILE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + kEpiStageBytes;
-  cudaFuncSetAttribute(gemm_tc_kernel<TF32, OutT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (cudaFuncSetAttribute(gemm_tc_kernel<TF32, OutT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+      cudaSuccess)
+    return;  // the thread's last CUDA error, checked by every caller
   int grid = device_sm_count();
   if (grid > n_tiles) grid = n_tiles;
   gemm_tc_kernel<TF32, OutT>

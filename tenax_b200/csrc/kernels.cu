@@ -367,7 +367,8 @@ void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevM
   if (n_chunks <= 0) return;
   const int smem = static_cast<int>(smem_bytes);
   auto go = [&](auto kernel) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    // a failure here is the thread's last CUDA error, checked by every caller
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return;
     kernel<<<n_chunks, kMpoThreads, smem, st>>>(pairs, islots, oslots, terms, chunks, skip);
   };
   if (!x1_f32)

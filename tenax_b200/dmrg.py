@@ -181,6 +181,9 @@ def lanczos(op: HeffOperator, theta: SymmetricTensor, num_steps: int, tol: float
     return energy, result, LanczosStats(m, a[:m], b[1:m + 1], time.perf_counter() - t0)
 
 
+_GENERAL_DONE_POLL = 4  # steps between early-exit checks of a general-path operator
+
+
 def _krylov(op: HeffOperator, x0: torch.Tensor, num_steps: int, tol: float, tol_rel: float, between=None):
     """Device Lanczos loop from x0 on op's key layout: returns
     (Ritz value, normalised Ritz vector, steps used, alphas, betas).
@@ -196,7 +199,8 @@ def _krylov(op: HeffOperator, x0: torch.Tensor, num_steps: int, tol: float, tol_
     nrm = vector.nrm2(x0)
     vector.scale(x0, nrm, 2, out=basis[0, :n])
     # fused operators skip their kernels once the early-exit flag is set; a
-    # general-path operator applies every step (the extra results are unused)
+    # general-path operator (planning and allocating per apply) reads the flag
+    # back every few steps and stops issuing applies once it is set
     batch = HeffBatch([op], skip_flag=done) if op.fused else None
     scr = vector.scratch(dev)
     st = torch.cuda.current_stream().cuda_stream
@@ -204,6 +208,8 @@ def _krylov(op: HeffOperator, x0: torch.Tensor, num_steps: int, tol: float, tol_
         if batch is not None:
             batch.apply([basis[k, :n]], [w[:n]])
         else:
+            if k > 0 and k % _GENERAL_DONE_POLL == 0 and int(done.item()) != 0:
+                break
             op.apply(basis[k, :n], w[:n])
         _capi.check(_capi.LIB.tnx_lanczos_step(
             w.data_ptr(), basis[k].data_ptr(), basis[k - 1].data_ptr() if k > 0 else 0,

@@ -48,6 +48,16 @@ def _out_keys(h):
     return [tuple(int(q) for q in r) for r in buf[: 4 * n.value].reshape(-1, 4)]
 
 
+def problem_flops(p) -> float:
+    """Algorithmic FLOPs of one H_eff application on a problem's own theta
+    key set (host planning only; no operator images are built)."""
+    h, _hold = _create(p.L, p.theta.indices, p.theta.keys, p.Wl, p.Wr, p.R)
+    try:
+        return float(_capi.LIB.tnx_heff_flops(h))
+    finally:
+        _capi.LIB.tnx_heff_destroy(h)
+
+
 def heff_key_closure(L, th_indices, th_keys, Wl, Wr, R, max_iter: int = 64):
     """Key sets K_0 = theta's keys, K_{k+1} = K_k | out(K_k), up to the fixed point.
 

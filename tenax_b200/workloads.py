@@ -19,51 +19,10 @@ import torch
 
 from tenax_b200.auto_mpo import heisenberg_chain_sites, heisenberg_cylinder_sites, to_symmetric
 from tenax_b200.core import FlowDirection, TensorIndex, U1Symmetry
+from tenax_b200.sectors import PHYS, bond_charges, env_keys, sector_sizes, theta_keys  # noqa: F401
 from tenax_b200.tensor import SymmetricTensor, _device, block_shape
 
 U1 = U1Symmetry()
-PHYS = np.array([1, -1], np.int32)
-
-
-def sector_sizes(chi: int, n_sectors: int = 30, sigma: float = 3.0, lo: int = 4, hi: int = 256,
-                 parity: int = 1) -> tuple:
-    """(charges, sizes) of one bond; deterministic integer rounding."""
-    k = np.arange(n_sectors) - n_sectors // 2
-    q = (parity % 2) + 2 * k
-    g = np.exp(-(q.astype(np.float64) ** 2) / (2 * sigma * sigma))
-    if chi < n_sectors * lo or chi > n_sectors * hi:
-        raise ValueError(f"chi={chi} cannot be split into {n_sectors} sectors of size [{lo},{hi}]")
-
-    def sizes(s):
-        return np.clip(np.rint(s * g), lo, hi).astype(np.int64)
-
-    a, b = 0.0, float(chi) * 1e6
-    for _ in range(200):
-        m = 0.5 * (a + b)
-        if sizes(m).sum() < chi:
-            a = m
-        else:
-            b = m
-    sz = sizes(b)
-    order = np.argsort(-g, kind="stable")
-    while sz.sum() > chi:
-        for i in order[::-1]:
-            if sz.sum() <= chi:
-                break
-            if sz[i] > lo:
-                sz[i] -= 1
-    while sz.sum() < chi:
-        for i in order:
-            if sz.sum() >= chi:
-                break
-            if sz[i] < hi:
-                sz[i] += 1
-    return q.astype(np.int32), sz
-
-
-def bond_charges(chi: int, parity: int = 1, **kw) -> np.ndarray:
-    q, sz = sector_sizes(chi, parity=parity, **kw)
-    return np.concatenate([np.full(int(s), int(c), np.int32) for c, s in zip(q, sz)])
 
 
 @dataclass
@@ -74,17 +33,6 @@ class HeffProblem:
     Wr: SymmetricTensor
     R: SymmetricTensor
     chi: int
-
-
-def _env_keys(leg0, mpo, leg2):
-    """Keys (q0, qb, q2) with q0 = qb + q2."""
-    s0 = set(np.unique(leg0).tolist())
-    keys = []
-    for qb in np.unique(mpo):
-        for q2 in np.unique(leg2):
-            if int(qb + q2) in s0:
-                keys.append((int(qb + q2), int(qb), int(q2)))
-    return sorted(keys)
 
 
 def _fill(indices, keys, gen, dtype=torch.float64):
@@ -110,12 +58,9 @@ def make_heff_problem(chi_l: int, chi_r: int, Wl: SymmetricTensor, Wr: Symmetric
             TensorIndex(U1, vr, FlowDirection.IN, "vr_c"))
     Tidx = (TensorIndex(U1, vl, FlowDirection.IN, "vl"), TensorIndex(U1, PHYS, FlowDirection.IN, "p1"),
             TensorIndex(U1, PHYS, FlowDirection.IN, "p2"), TensorIndex(U1, vr, FlowDirection.OUT, "vr"))
-    L = _fill(Lidx, _env_keys(vl, mpo_l, vl), gen)
-    R = _fill(Ridx, _env_keys(vr, mpo_r, vr), gen)
-    sr = set(np.unique(vr).tolist())
-    tkeys = sorted((int(a), int(p), int(q), int(a + p + q)) for a in np.unique(vl) for p in PHYS for q in PHYS
-                   if int(a + p + q) in sr)
-    th = _fill(Tidx, tkeys, gen)
+    L = _fill(Lidx, env_keys(vl, mpo_l, vl), gen)
+    R = _fill(Ridx, env_keys(vr, mpo_r, vr), gen)
+    th = _fill(Tidx, theta_keys(vl, vr), gen)
     return HeffProblem(L, th, Wl, Wr, R, chi_l)
 
 

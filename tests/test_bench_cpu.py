@@ -47,3 +47,47 @@ def test_clock_summary_without_samples():
     c.mark_start()
     c.mark_end()
     assert c.summary() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+
+
+def test_cpu_chi_schedule():
+    b = _bench()
+    for n in (1, 4, 5, 20, 100):
+        s = b.cpu_chi_schedule(n)
+        assert len(s) == n
+        assert s.count(2048) == 1
+        if n >= 4:
+            assert set(s) == {256, 512, 1024, 2048}
+    assert b.cpu_chi_schedule(20, n_top=2).count(2048) == 2
+
+
+def test_batch_rate_weights_by_chi_counts():
+    b = _bench()
+    tm = {"seconds": {256: [1.0, 3.0, 2.0], 2048: [10.0]}, "flops": {256: 1e12, 2048: 8e12}}
+    rate, per = b.batch_rate(tm, {256: 3, 2048: 1})
+    # 3 x 1 TFLOP in 3 x 2 s (median) + 8 TFLOP in 10 s
+    assert abs(rate - 11.0 / 16.0) < 1e-12
+    assert per[256]["s_per_matvec"] == 2.0 and per[2048]["timed"] == 1
+
+
+def test_reference_arm_never_loads_the_library():
+    """The CPU arm builds its structures and FLOP counts without importing
+    the package: no tenax_b200 module and no libtenax_b200.so in the
+    process after a chi=256 problem is built and one oracle matvec runs."""
+    import subprocess
+    import sys
+
+    code = (
+        "import sys, importlib.util\n"
+        f"sys.path.insert(0, {ROOT!r})\n"
+        f"spec = importlib.util.spec_from_file_location('b', {os.path.join(ROOT, 'bench.py')!r})\n"
+        "b = importlib.util.module_from_spec(spec); spec.loader.exec_module(b)\n"
+        "hp = b.HostProblems(1)\n"
+        "tm = b.time_cpu_schedule(hp, [256], warmup=0)\n"
+        "assert tm['flops'][256] > 0\n"
+        "assert not [m for m in sys.modules if m.startswith('tenax_b200')], 'package imported'\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "assert 'libtenax_b200' not in maps, 'library mapped'\n"
+        "print('OK')\n"
+    )
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "OK" in r.stdout, r.stderr[-2000:]

@@ -1,0 +1,90 @@
+"""Parity on the benchmarked structure itself.
+
+The throughput workload is 64 two-site H_eff problems of the width-6
+Heisenberg cylinder (AutoMPO, uncompressed, bulk Dw = 26), chi drawn from
+{256, 512, 1024, 2048}, 30 U(1) sectors per bond (Gaussian sizes, 4..256).
+Here the first problem of each chi of that very batch (same generator, same
+seed) is applied on the device in FP64, split-BF16x3 and TF32 and compared
+with the oracle's per-block-combination H_eff ("abc,apqd,bpse,eqtf,dfg->
+cstg", algorithms/dmrg.py:1282-1289) on the same inputs:
+  * the keys H_eff writes equal the oracle's output keys exactly (the output
+    keys grow beyond theta's; the Krylov layout holds them), and every other
+    key of the layout comes out zero;
+  * relative Frobenius error: FP64 <= 1e-12, split-BF16x3 <= 2e-5, TF32 <= 5e-3.
+The oracle matvec takes about 0.3 / 1 / 6 / 25 s on 8 host cores at chi =
+256 / 512 / 1024 / 2048; the chi=2048 case is a test of its own.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import tenax_b200 as tb  # noqa: E402
+from oracle import dmrg as odmrg  # noqa: E402
+from oracle.blocksparse import Leg, OTensor  # noqa: E402
+from tenax_b200 import replicas  # noqa: E402
+from tenax_b200.heff import _out_keys  # noqa: E402
+from tenax_b200.tensor import SymmetricTensor, embed_in_keys  # noqa: E402
+
+CHIS = (256, 512, 1024, 2048)
+TOL = {"fp64": 1e-12, "bf16x3": 2e-5, "tf32": 5e-3}
+
+
+def _host(t):
+    return OTensor(tuple(Leg(i.charges, int(i.flow), i.label) for i in t.indices), t.numpy_blocks())
+
+
+@pytest.fixture(scope="module")
+def first_of_each_chi():
+    from tenax_b200.workloads import batched_problems
+
+    probs = batched_problems(64, CHIS, seed=replicas.rank_seed(0, 0))
+    firsts = {}
+    for p in probs:
+        firsts.setdefault(int(p.chi), p)
+    del probs
+    torch.cuda.empty_cache()
+    return firsts
+
+
+def _check(p):
+    ops = {prec: tb.HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, prec) for prec in TOL}
+    keys = ops["fp64"].keys
+    for o in ops.values():
+        assert o.fused and o.keys == keys
+    x = embed_in_keys(p.theta, keys)
+    ref = odmrg.heff_matvec(*[_host(t) for t in (p.L, x, p.Wl, p.Wr, p.R)]).blocks
+    assert ref
+    written = set(_out_keys(ops["fp64"].handle))
+    assert written == set(ref), "output key set differs from the oracle's"
+    assert set(ref) <= set(keys)
+    den = np.sqrt(sum(float(np.sum(v * v)) for v in ref.values()))
+    errs = {}
+    for prec, op in ops.items():
+        y = op.apply(x.data)
+        torch.cuda.synchronize()
+        assert op.device_error() == 0
+        got = SymmetricTensor.from_flat(p.theta.indices, keys, y).numpy_blocks()
+        for k in got:
+            if k not in ref:
+                assert np.all(got[k] == 0.0), (prec, k)
+        num = np.sqrt(sum(float(np.sum((got[k] - ref[k]) ** 2)) for k in ref))
+        errs[prec] = num / den
+    for prec, e in errs.items():
+        assert e <= TOL[prec], (p.chi, prec, e)
+    return errs
+
+
+@pytest.mark.parametrize("chi", [256, 512, 1024])
+def test_bench_structure_parity(first_of_each_chi, chi):
+    _check(first_of_each_chi[chi])
+
+
+def test_bench_structure_parity_chi2048(first_of_each_chi):
+    """The chi=2048 problem of the batch (oracle matvec about 25 s on 8 cores)."""
+    _check(first_of_each_chi[2048])

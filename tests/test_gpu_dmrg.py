@@ -78,3 +78,57 @@ def test_dmrg_config1_energy(golden_dir):
     # the same inputs also lands 5e-5 away from the reference after sweep 1.
     assert abs(res.energies_per_sweep[0] - z["energies_per_sweep"][0]) < 5e-4
     assert len(res.truncation_errors) == len(z["truncation_errors"])
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "tf32"])
+def test_dmrg_config1_energy_mixed(golden_dir, precision):
+    """Config-1 DMRG with the H_eff sector GEMMs in split-BF16x3 or TF32
+    (Lanczos recurrence, polish, SVD and energies in FP64): the converged
+    energy within 1e-9 of the reference's FP64 run, the stated bar."""
+    z = np.load(os.path.join(golden_dir, "dmrg_c1_L20.npz"))
+    L = 20
+    mps, mpo = TensorNetwork("mps"), TensorNetwork("mpo")
+    for i in range(L):
+        mps.add_node(i, to_dev(unpack_tensor(z, f"mps{i}")))
+        mpo.add_node(i, to_dev(unpack_tensor(z, f"mpo{i}")))
+    cfg = gd.DMRGConfig(max_bond_dim=64, num_sweeps=2, lanczos_max_iter=10, two_site=True, precision=precision)
+    res = gd.dmrg(mpo, mps, cfg)
+    e_ref = float(z["energy"])
+    assert abs(res.energy - e_ref) <= 1e-9, (precision, res.energy, e_ref)
+    assert abs(res.energies_per_sweep[-1] - z["energies_per_sweep"][-1]) <= 1e-9
+    assert len(res.truncation_errors) == len(z["truncation_errors"])
+
+
+def _assert_same_blocks(got: dict, ref: dict, rtol=1e-12, atol=1e-13):
+    assert sorted(got) == sorted(ref)
+    for k in got:
+        np.testing.assert_allclose(got[k], ref[k], rtol=rtol, atol=atol, err_msg=str(k))
+
+
+def test_env_updates_match_reference(golden_dir):
+    """Left/right environment updates on the contraction engine
+    (dmrg.py:1165-1232, "abc,apd,bpxe,cxf->def" / "abc,dpa,epxb,fxc->def")
+    against the reference's own outputs: exact key sets, FP64 at 1e-12."""
+    z = np.load(os.path.join(golden_dir, "dmrg_pieces.npz"))
+    L, Wl, Wr, R = (to_dev(unpack_tensor(z, f"heff.{n}")) for n in ("L", "Wl", "Wr", "R"))
+    newL = gd.update_left_env(L, to_dev(unpack_tensor(z, "envl.A")), Wl)
+    _assert_same_blocks(newL.numpy_blocks(), unpack_tensor(z, "envl.out").blocks)
+    newR = gd.update_right_env(R, to_dev(unpack_tensor(z, "envr.B")), Wr)
+    _assert_same_blocks(newR.numpy_blocks(), unpack_tensor(z, "envr.out").blocks)
+
+
+def test_scale_bond_axis_matches_oracle(golden_dir):
+    """scale_bond_axis (algorithms/_tensor_utils.py:17-62) on the fixture's
+    Lanczos vector, every leg in turn, against the oracle's restatement:
+    bit-exact (one multiply per element)."""
+    from oracle import dmrg as odmrg
+
+    z = np.load(os.path.join(golden_dir, "dmrg_pieces.npz"))
+    host = unpack_tensor(z, "lanczos.vec")
+    dev = to_dev(host)
+    rng = np.random.default_rng(4)
+    for axis, leg in enumerate(host.legs):
+        s = rng.standard_normal(len(leg.charges))
+        got = gd.scale_bond_axis(dev, dev.labels()[axis], s).numpy_blocks()
+        ref = odmrg.scale_bond_axis(host, host.labels()[axis], s).blocks
+        _assert_same_blocks(got, ref, rtol=0, atol=0)

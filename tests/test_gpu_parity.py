@@ -178,6 +178,9 @@ def test_heff_z3(precision, tol):
     Wr = z3_like(u.Wr, [mpo, phys, phys, mpo])
     dL, dth, dWl, dWr, dR = map(to_dev, (L, th, Wl, Wr, R))
     op = tb.HeffOperator(dL, dWl, dWr, dR, dth.indices, dth.keys, precision)
+    # this structure has stage-4 groups writing several output charges: it
+    # must take the general path, or the fallback goes untested
+    assert not op.fused
     x = embed_in_keys(dth, op.keys)
     y = op.apply(x.data)
     torch.cuda.synchronize()

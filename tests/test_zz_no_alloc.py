@@ -91,3 +91,25 @@ def test_static_multi_operand_and_size_limit():
     st = _capi.LIB.tnx_plan_execute_static(bplan.handle, ptrs, out.data_ptr(), torch.cuda.current_stream().cuda_stream)
     assert st == _capi.TNX_ERR_VALUE
     assert b"static arena" in _capi.LIB.tnx_last_error()
+
+
+def test_static_single_operand_transpose():
+    """A one-operand plan (a leg permutation, contracted with the library's
+    scalar 1.0): the caller passes a single input pointer, and the static
+    path must read nothing beyond it.  Two calls in a row, against the
+    regular entry point."""
+    u1 = U1Symmetry()
+    q = np.array([-2, -1, -1, 0, 0, 0, 1, 1, 2], np.int32)
+    idx = (TensorIndex(u1, q, FlowDirection.IN, "a"), TensorIndex(u1, np.array([-1, 1], np.int32),
+                                                                 FlowDirection.IN, "p"),
+           TensorIndex(u1, q, FlowDirection.OUT, "b"))
+    t = SymmetricTensor.random_normal(idx, key=5)
+    out_idx = (idx[2], idx[0], idx[1])
+    plan = get_plan([t], ["apb"], "bap", _capi.MATCH_FILTERED, out_idx)
+    ref = plan.execute([t], "fp64")
+    torch.cuda.synchronize()
+    dense = t.todense().cpu().numpy().transpose(2, 0, 1)
+    got_t = SymmetricTensor.from_flat(out_idx, plan.out_keys, ref)
+    np.testing.assert_allclose(got_t.todense().cpu().numpy(), dense, rtol=0, atol=0)
+    for _ in range(2):
+        torch.testing.assert_close(_run_static(plan, [t]), ref, rtol=1e-12, atol=1e-14)
