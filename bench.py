@@ -186,21 +186,26 @@ def run_ours(args):
         st = torch.cuda.current_stream()
         if sampler:
             sampler.__enter__()
+        # one step = one batched apply, replayed from a captured CUDA graph
+        # (every stage of every problem in one graph launch) unless --no-graph
+        graph = batch.capture(xs, ys) if not args.no_graph else None
+        step = graph.replay if graph is not None else (lambda: batch.apply(xs, ys))
         for _ in range(args.warmup):
-            batch.apply(xs, ys)
+            step()
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         if sampler:
             sampler.mark_start()
         e0.record(st)
         for _ in range(args.steps):
-            batch.apply(xs, ys)
+            step()
         e1.record(st)
         barrier()
         if sampler:
             sampler.mark_end()
             sampler.__exit__()
         ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        del graph
         err = batch.device_error()
         # per-stage timing (each stage re-run alone, same buffers)
         stage_ms = []
@@ -291,7 +296,7 @@ def run_ours(args):
                     "ms_per_step": round(rmx["e2e_ms"], 4), "api": "HeffBatch.apply_host (pinned host buffers; "
                     "step s+1 copied in and step s-1 copied out while step s computes)",
                     "max_abs_diff_vs_device_apply": rmx["e2e_max_abs_diff_vs_device"]},
-            "gpu_launches": rmx["launches"] * args.steps,
+            "gpu_launches": rmx["launches"] * args.steps, "cuda_graph": not args.no_graph,
             "device_error_flag": rmx["err"],
             "clocks": clocks,
         }
@@ -1008,6 +1013,7 @@ def main():
     ap.add_argument("--split-chi", type=int, default=150)
     ap.add_argument("--split-iters", type=int, default=40)
     ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--no-graph", action="store_true", help="time eager applies instead of CUDA-graph replays")
     ap.add_argument("--mode", default="partition", choices=["partition", "replicas"],
                     help="N>1: split one batch over the ranks (partition, strong scaling) or give every rank its "
                          "own batch (replicas, weak scaling)")

@@ -62,6 +62,8 @@ class DMRGConfig:
     # (polar decomposition for every sector, 8 workers).
     svd_driver: str | None = "native"
     svd_streams: int = 8
+    # run each Krylov loop of a fused H_eff as one captured CUDA graph
+    cuda_graph: bool = False
 
 
 NOISE_REL = {"fp64": 0.0, "bf16x3": 1e-5, "tf32": 2e-3}
@@ -145,7 +147,7 @@ class LanczosStats(NamedTuple):
 
 
 def lanczos(op: HeffOperator, theta: SymmetricTensor, num_steps: int, tol: float, fp64_op: HeffOperator | None = None,
-            tol_rel: float = 0.0, polish_steps: int = 0):
+            tol_rel: float = 0.0, polish_steps: int = 0, graph: bool = False):
     """Plain three-term Lanczos without reorthogonalisation (dmrg.py:978-1045).
 
     Krylov vectors live on the operator's closed key layout; alpha/beta and
@@ -153,8 +155,10 @@ def lanczos(op: HeffOperator, theta: SymmetricTensor, num_steps: int, tol: float
     the loop.  ``fp64_op`` may also be a zero-argument callable returning
     the FP64 operator: it is then called after the first loop is queued on
     the device and before its read-back, so that the operator's host-side
-    planning overlaps the device work.  Returns (eigenvalue, eigenvector
-    SymmetricTensor with the reference's key set, LanczosStats).
+    planning overlaps the device work.  ``graph``: each Krylov loop of a
+    fused operator runs as one captured CUDA graph (see ``_krylov``).
+    Returns (eigenvalue, eigenvector SymmetricTensor with the reference's key
+    set, LanczosStats).
     """
     t0 = time.perf_counter()
     x0 = embed_in_keys(theta, op.keys).data
@@ -164,13 +168,13 @@ def lanczos(op: HeffOperator, theta: SymmetricTensor, num_steps: int, tol: float
         if fp64_op is not None and not isinstance(fp64_op, HeffOperator):
             built["op"] = fp64_op()
 
-    energy, vec, m, a, b = _krylov(op, x0, num_steps, tol, tol_rel, between=build)
+    energy, vec, m, a, b = _krylov(op, x0, num_steps, tol, tol_rel, between=build, graph=graph)
     fp64_op = built.get("op", fp64_op)
     key_seq = op.key_seq
     keys = key_seq[0] if m <= 1 else key_seq[min(m - 1, len(key_seq) - 1)]
     if fp64_op is not None and polish_steps > 0:
         # FP64 polish: a short FP64 Lanczos started from the mixed Ritz vector
-        energy, vec, m2, _, _ = _krylov(fp64_op, vec, polish_steps, tol, 0.0)
+        energy, vec, m2, _, _ = _krylov(fp64_op, vec, polish_steps, tol, 0.0, graph=graph)
         keys = op.keys
     elif fp64_op is not None:
         # Rayleigh quotient of the Ritz vector with the FP64 operator
@@ -182,13 +186,30 @@ def lanczos(op: HeffOperator, theta: SymmetricTensor, num_steps: int, tol: float
 
 
 _GENERAL_DONE_POLL = 4  # steps between early-exit checks of a general-path operator
+_CAPTURE_STREAMS: dict = {}
+_GRAPH_KEEP: list = [None]
 
 
-def _krylov(op: HeffOperator, x0: torch.Tensor, num_steps: int, tol: float, tol_rel: float, between=None):
+def _capture_stream(dev: torch.device) -> torch.cuda.Stream:
+    """One side stream per device for graph capture (its reduction scratch is
+    created before capture, so nothing is allocated inside a graph)."""
+    s = _CAPTURE_STREAMS.get(dev.index)
+    if s is None:
+        with torch.cuda.device(dev):
+            s = torch.cuda.Stream()
+        _CAPTURE_STREAMS[dev.index] = s
+    return s
+
+
+def _krylov(op: HeffOperator, x0: torch.Tensor, num_steps: int, tol: float, tol_rel: float, between=None,
+            graph: bool = False):
     """Device Lanczos loop from x0 on op's key layout: returns
     (Ritz value, normalised Ritz vector, steps used, alphas, betas).
     ``between`` (if given) runs on the host once the loop is queued, before
-    the read-back waits for it."""
+    the read-back waits for it.  ``graph`` (fused operators only) captures the
+    whole loop -- start vector, every matvec and orthogonalisation step with
+    its early-exit flag -- in one CUDA graph and launches that instead of the
+    individual kernels."""
     dev = x0.device
     n = op.size
     basis = torch.empty((num_steps + 1, max(n, 1)), dtype=torch.float64, device=dev)
@@ -196,25 +217,52 @@ def _krylov(op: HeffOperator, x0: torch.Tensor, num_steps: int, tol: float, tol_
     beta = torch.zeros(num_steps + 2, dtype=torch.float64, device=dev)
     done = torch.zeros(1, dtype=torch.int32, device=dev)
     w = torch.empty(max(n, 1), dtype=torch.float64, device=dev)
-    nrm = vector.nrm2(x0)
-    vector.scale(x0, nrm, 2, out=basis[0, :n])
     # fused operators skip their kernels once the early-exit flag is set; a
     # general-path operator (planning and allocating per apply) reads the flag
     # back every few steps and stops issuing applies once it is set
     batch = HeffBatch([op], skip_flag=done) if op.fused else None
-    scr = vector.scratch(dev)
+    graph = graph and batch is not None
+
+    def issue(x_in, scr, nrm):
+        st = torch.cuda.current_stream().cuda_stream
+        _capi.check(_capi.LIB.tnx_nrm2(x0.data_ptr(), n, nrm.data_ptr(), scr.data_ptr(), st))
+        _capi.check(_capi.LIB.tnx_scale(x0.data_ptr(), basis[0].data_ptr(), n, nrm.data_ptr(), 2, st))
+        for k in range(num_steps):
+            if batch is not None:
+                if x_in is not None:
+                    # fixed matvec input: the batch's pointer tables never change inside a graph
+                    x_in[:n].copy_(basis[k, :n])
+                    batch.apply([x_in[:n]], [w[:n]])
+                else:
+                    batch.apply([basis[k, :n]], [w[:n]])
+            else:
+                if k > 0 and k % _GENERAL_DONE_POLL == 0 and int(done.item()) != 0:
+                    break
+                op.apply(basis[k, :n], w[:n])
+            _capi.check(_capi.LIB.tnx_lanczos_step(
+                w.data_ptr(), basis[k].data_ptr(), basis[k - 1].data_ptr() if k > 0 else 0,
+                basis[k + 1].data_ptr(), n, alpha.data_ptr(), beta.data_ptr(), k, float(tol), float(tol_rel),
+                done.data_ptr(), scr.data_ptr(), st))
+
+    if graph:
+        cap = _capture_stream(dev)
+        cap.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(cap):
+            scr = vector.scratch(dev)
+            nrm = torch.empty((), dtype=torch.float64, device=dev)
+            x_in = torch.empty(max(n, 1), dtype=torch.float64, device=dev)
+            # bind the batch's pointer tables to (x_in, w) before capture
+            batch.apply([x_in[:n]], [w[:n]])
+            done.zero_()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=cap):
+            issue(x_in, scr, nrm)
+        g.replay()
+        torch.cuda.current_stream().wait_stream(cap)
+        _GRAPH_KEEP[0] = (g, x_in, nrm)  # alive until the read-back below completes
+    else:
+        issue(None, vector.scratch(dev), torch.empty((), dtype=torch.float64, device=dev))
     st = torch.cuda.current_stream().cuda_stream
-    for k in range(num_steps):
-        if batch is not None:
-            batch.apply([basis[k, :n]], [w[:n]])
-        else:
-            if k > 0 and k % _GENERAL_DONE_POLL == 0 and int(done.item()) != 0:
-                break
-            op.apply(basis[k, :n], w[:n])
-        _capi.check(_capi.LIB.tnx_lanczos_step(
-            w.data_ptr(), basis[k].data_ptr(), basis[k - 1].data_ptr() if k > 0 else 0,
-            basis[k + 1].data_ptr(), n, alpha.data_ptr(), beta.data_ptr(), k, float(tol), float(tol_rel),
-            done.data_ptr(), scr.data_ptr(), st))
     if between is not None:
         between()
     a = alpha.cpu().numpy()
@@ -511,7 +559,7 @@ def two_site_update(site_l, site_r, L, Wl, Wr, R, config, stats: list | None = N
     tol_rel = NOISE_REL.get(config.precision, 0.0) if config.lanczos_tol_rel is None else config.lanczos_tol_rel
     energy, th, ls = lanczos(op, theta, config.lanczos_max_iter, config.lanczos_tol,
                              make_fp64 if need_fp64 else None, tol_rel,
-                             config.fp64_polish_steps if need_fp64 else 0)
+                             config.fp64_polish_steps if need_fp64 else 0, graph=config.cuda_graph)
     t1 = _tick(phases, "lanczos", t1)
     rel = None
     diag_s = 0.0

@@ -188,6 +188,22 @@ class HeffBatch:
         op = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
         _capi.check(_capi.LIB.tnx_heff_batch_apply(self.handle, tp, op, torch.cuda.current_stream().cuda_stream))
 
+    def capture(self, thetas, outs) -> "torch.cuda.CUDAGraph":
+        """A CUDA graph of one apply with these buffers: the batch's pointer
+        tables are bound by an eager apply first, so the captured apply
+        issues kernels only.  ``graph.replay()`` then runs the whole batched
+        matvec (every stage, every problem) as one launch on the current
+        stream."""
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            self.apply(thetas, outs)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            self.apply(thetas, outs)
+        torch.cuda.current_stream().wait_stream(side)
+        return g
+
     def apply_host(self, host_inputs, host_outputs):
         """Stream independent applications from host memory: host_inputs[s]
         and host_outputs[s] are CPU float64 tensors of ``total`` elements

@@ -132,3 +132,41 @@ def test_scale_bond_axis_matches_oracle(golden_dir):
         got = gd.scale_bond_axis(dev, dev.labels()[axis], s).numpy_blocks()
         ref = odmrg.scale_bond_axis(host, host.labels()[axis], s).blocks
         _assert_same_blocks(got, ref, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+def test_lanczos_graph_equals_eager(golden_dir, precision):
+    """The Krylov loop captured in one CUDA graph (matvecs, orthogonalisation
+    steps and the early-exit flag) gives bit for bit the eager loop's
+    alphas, betas, eigenvalue and vector, on the fixture's H_eff and on a
+    multi-tile cylinder problem; the graph is built and replayed twice."""
+    z = np.load(os.path.join(golden_dir, "dmrg_pieces.npz"))
+    L, th, Wl, Wr, R = (to_dev(unpack_tensor(z, f"heff.{n}")) for n in ("L", "theta", "Wl", "Wr", "R"))
+    from tenax_b200 import workloads as W
+
+    Wl2, Wr2 = W.cylinder_bulk_w()
+    p = W.make_heff_problem(300, 300, Wl2, Wr2, np.random.default_rng(5), n_sectors=12, hi=64)
+    for (L_, Wl_, Wr_, R_, th_) in ((L, Wl, Wr, R, th), (p.L, p.Wl, p.Wr, p.R, p.theta)):
+        op = tb.HeffOperator(L_, Wl_, Wr_, R_, th_.indices, th_.keys, precision)
+        assert op.fused
+        e0, v0, s0 = gd.lanczos(op, th_, 12, 1e-12)
+        for _ in range(2):
+            e1, v1, s1 = gd.lanczos(op, th_, 12, 1e-12, graph=True)
+            assert s1.steps == s0.steps
+            np.testing.assert_array_equal(s1.alphas, s0.alphas)
+            np.testing.assert_array_equal(s1.betas, s0.betas)
+            assert e1 == e0
+            torch.testing.assert_close(v1.data, v0.data, rtol=0, atol=0)
+
+
+def test_dmrg_config1_graph(golden_dir):
+    """Config-1 DMRG with every Krylov loop in a CUDA graph: the reference's
+    energy within 1e-9."""
+    z = np.load(os.path.join(golden_dir, "dmrg_c1_L20.npz"))
+    mps, mpo = TensorNetwork("mps"), TensorNetwork("mpo")
+    for i in range(20):
+        mps.add_node(i, to_dev(unpack_tensor(z, f"mps{i}")))
+        mpo.add_node(i, to_dev(unpack_tensor(z, f"mpo{i}")))
+    cfg = gd.DMRGConfig(max_bond_dim=64, num_sweeps=2, lanczos_max_iter=10, two_site=True, cuda_graph=True)
+    res = gd.dmrg(mpo, mps, cfg)
+    assert abs(res.energy - float(z["energy"])) <= 1e-9
