@@ -171,8 +171,9 @@ def run_ours(args):
     def max_over_ranks(x: float) -> float:
         return replicas.max_over_ranks(x, dist, dev)
 
-    def run_precision(prec, with_e2e=False, sampler=None):
-        ops = [HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, prec) for p in problems]
+    def run_precision(prec, with_e2e=False, sampler=None, schedule=None):
+        ops = [HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, prec, schedule=schedule)
+               for p in problems]
         sizes = [o.size for o in ops]
         offs = np.concatenate([[0], np.cumsum(sizes)])
         x_all = torch.empty(int(offs[-1]), dtype=torch.float64, device=dev)
@@ -225,7 +226,8 @@ def run_ours(args):
             _capi.check(_capi.LIB.tnx_heff_stage_flops(o.handle, sf.ctypes.data))
             tot_sf += sf
         res = {"ms": ms, "flops": flops, "stage_ms": stage_ms, "stage_flops": tot_sf.tolist(), "err": err,
-               "per_problem_flops": [o.flops for o in ops], "launches": batch.launches_per_apply}
+               "per_problem_flops": [o.flops for o in ops], "launches": batch.launches_per_apply,
+               "schedule": ops[0].schedule}
         if with_e2e:
             # end to end through HeffBatch.apply_host: every step copies its
             # inputs in from pinned host memory and its outputs back; step
@@ -254,8 +256,9 @@ def run_ours(args):
         return res
 
     r64 = run_precision("fp64")
+    schedule = {"fuse_mpo": 0 if args.unfused else 1, "c_per_tile": args.c_per_tile}
     sampler = ClockSampler(local)
-    rmx = run_precision(args.precision, with_e2e=True, sampler=sampler)
+    rmx = run_precision(args.precision, with_e2e=True, sampler=sampler, schedule=schedule)
     clocks = sampler.summary()
 
     # ranks draw different problems: the job's work is the sum over ranks, its
@@ -266,15 +269,23 @@ def run_ours(args):
     peaks, peak_src = _peaks()
     # dominant GEMM stage of the mixed step
     st_ms = rmx["stage_ms"]
-    gemm = {1: rmx["stage_flops"][0], 3: rmx["stage_flops"][2]}
+    fused = bool(rmx["schedule"]["fuse_mpo"])
+    # the fused kernel does stage 1 and the MPO; its tensor work is stage 1's
+    gemm = {1: rmx["stage_flops"][0] + (rmx["stage_flops"][1] if fused else 0.0), 3: rmx["stage_flops"][2]}
     dom = max((1, 3), key=lambda s: st_ms[s])
+    stage_names = (["pack theta panels", "fused stages 1-3 (L.theta in TMEM, W_l W_r epilogue)",
+                    "none (MPO inside the fused kernel)", "stage-4 GEMM .R"] if fused else
+                   ["pack theta", "stage-1 GEMM L.theta", "fused MPO (W_l W_r)", "stage-4 GEMM .R"])
+    dom_name = ("fused stages 1-3 (tcgen05 + W_l W_r epilogue)" if fused and dom == 1
+                else f"{STAGE_GEMM[dom]} tcgen05 grouped GEMM")
     split = 3.0 if args.precision == "bf16x3" else 1.0
     peak = peaks["bf16_tflops"] / split if args.precision == "bf16x3" else peaks["bf16_tflops"] / 2.0
     achieved = gemm[dom] / (st_ms[dom] * 1e-3) / 1e12
     traffic = None
     tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(f"{args.precision}_stage{dom}")
+        key = f"{args.precision}_fused1" if fused and dom == 1 else f"{args.precision}_stage{dom}"
+        traffic = json.load(open(tp)).get(key)
     if rank == 0:
         out = {
             "metric": METRIC, "value": round(value, 3), "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -286,8 +297,8 @@ def run_ours(args):
                      "stage_ms": [round(x, 4) for x in r64["stage_ms"]]},
             "mixed_over_fp64": round(value / fp64_value, 3),
             "stage_ms": [round(x, 4) for x in st_ms],
-            "stage_names": ["pack theta", "stage-1 GEMM L.theta", "fused MPO (W_l W_r)", "stage-4 GEMM .R"],
-            "roofline": {"bound": "tensor", "kernel": f"{STAGE_GEMM[dom]} tcgen05 grouped GEMM", "achieved":
+            "stage_names": stage_names, "schedule": rmx["schedule"],
+            "roofline": {"bound": "tensor", "kernel": dom_name, "achieved":
                          round(achieved, 2), "peak": round(peak, 1), "unit": "TFLOP/s",
                          "frac": round(achieved / peak, 4), "peak_source": f"{peak_src} bf16 burst"
                          + (" / 3 (three products)" if split == 3 else " / 2 (tf32)"), "traffic": traffic},
@@ -1014,6 +1025,9 @@ def main():
     ap.add_argument("--split-iters", type=int, default=40)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--no-graph", action="store_true", help="time eager applies instead of CUDA-graph replays")
+    ap.add_argument("--unfused", action="store_true",
+                    help="mixed stages 1-3 as stage-1 GEMM + X1 in HBM + MPO kernel instead of the fused kernel")
+    ap.add_argument("--c-per-tile", type=int, default=0, help="fused kernel: c values per tile (0 = largest that fits)")
     ap.add_argument("--mode", default="partition", choices=["partition", "replicas"],
                     help="N>1: split one batch over the ranks (partition, strong scaling) or give every rank its "
                          "own batch (replicas, weak scaling)")

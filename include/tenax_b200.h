@@ -124,6 +124,24 @@ int tnx_heff_create(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, cons
  * precision re-plans, so either create works with any precision. */
 int tnx_heff_create_for(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, const tnx_tensor_desc* Wl,
                         const tnx_tensor_desc* Wr, const tnx_tensor_desc* R, int32_t precision, tnx_heff** h);
+/* Schedule of a mixed-precision operator's stages 1-3 (no counterpart in the
+ * reference, which evaluates H_eff one block combination at a time).
+ * fuse_mpo = 1: one tcgen05 kernel accumulates L.theta in tensor memory per
+ * (q_c, q_d) sector pair and applies W_l W_r in its epilogue, writing the
+ * stage-4 operand directly (no X1 in HBM), wherever the structure fits (at
+ * most 48 input slots per sector pair, every pair's blocks side by side in
+ * 256 accumulator columns); c_per_tile c values per tile, 0 = the largest
+ * that fits.  fuse_mpo = 0: stage-1 GEMM, X1 in HBM, MPO kernel.  Takes
+ * effect at the next tnx_heff_set_operators; FP64 operators always run
+ * unfused.  tnx_heff_get_schedule reports the schedule in effect (fuse_mpo =
+ * 1 only if the operator runs fused); before tnx_heff_set_operators, the one
+ * the precision given to tnx_heff_create_for would get (host planning only). */
+typedef struct tnx_heff_schedule {
+  int32_t fuse_mpo;
+  int32_t c_per_tile;
+} tnx_heff_schedule;
+int tnx_heff_set_schedule(tnx_heff* h, const tnx_heff_schedule* sched);
+int tnx_heff_get_schedule(const tnx_heff* h, tnx_heff_schedule* sched);
 int tnx_heff_closed(const tnx_heff* h, int32_t* closed);
 /* Output keys of H_eff applied to theta's key set (structure only). */
 int tnx_heff_out_keys(const tnx_heff* h, int64_t* n_keys, int32_t* keys);
@@ -136,7 +154,9 @@ int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const
 void tnx_heff_destroy(tnx_heff* h);
 
 /* Many independent H_eff problems applied in one launch per stage
- * (persistent grouped GEMMs over all sectors of all problems). */
+ * (persistent grouped GEMMs over all sectors of all problems).  The
+ * operators of one batch must all run fused stages 1-3 or all unfused
+ * (tnx_heff_get_schedule); otherwise TNX_ERR_VALUE. */
 int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx_heff_batch** b);
 int tnx_heff_batch_apply(tnx_heff_batch* b, const double* const* thetas, double* const* outs, void* stream);
 /* Host-resident streaming (no counterpart in the reference, which applies one
@@ -153,7 +173,8 @@ int tnx_heff_batch_apply_host(tnx_heff_batch* b, const double* const* host_in, d
  * (offsets: n doubles' worth of int64, or NULL). */
 int tnx_heff_batch_size(const tnx_heff_batch* b, int64_t* total, int64_t* offsets);
 /* Re-run one stage of the last apply (0 pack theta, 1 stage-1 GEMM, 2 fused
- * MPO, 3 stage-4 GEMM) with the same buffers -- per-kernel timing. */
+ * MPO, 3 stage-4 GEMM; with fused stages 1-3: 0 theta panels, 1 the fused
+ * kernel, 2 nothing) with the same buffers -- per-kernel timing. */
 int tnx_heff_batch_apply_stage(tnx_heff_batch* b, int32_t stage, void* stream);
 /* Algorithmic flops of stage 1 (L.theta), stages 2+3 (MPO), stage 4 (.R). */
 int tnx_heff_stage_flops(const tnx_heff* h, double* flops3);

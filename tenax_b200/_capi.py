@@ -35,6 +35,12 @@ class TnxUnsupported(NotImplementedError):
     """Valid input outside what this build implements."""
 
 
+class HeffSchedule(C.Structure):
+    """tnx_heff_schedule: fused stages 1-3 on/off and c values per tile (0 = auto)."""
+
+    _fields_ = [("fuse_mpo", C.c_int32), ("c_per_tile", C.c_int32)]
+
+
 class TensorDesc(C.Structure):
     _fields_ = [
         ("n_legs", C.c_int32),
@@ -70,6 +76,8 @@ def _load():
         "tnx_heff_create": (C.c_int, [P, P, P, P, P, P]),
         "tnx_heff_create_for": (C.c_int, [P, P, P, P, P, i32, P]),
         "tnx_heff_closed": (C.c_int, [P, P]),
+        "tnx_heff_set_schedule": (C.c_int, [P, P]),
+        "tnx_heff_get_schedule": (C.c_int, [P, P]),
         "tnx_heff_out_keys": (C.c_int, [P, P, P]),
         "tnx_heff_flops": (dbl, [P]),
         "tnx_heff_set_operators": (C.c_int, [P, P, P, P, P, i32, P]),
@@ -113,7 +121,7 @@ EXPORTED = [
     "tnx_last_error", "tnx_version", "tnx_valid_blocks", "tnx_plan_create", "tnx_plan_output",
     "tnx_plan_workspace", "tnx_plan_flops", "tnx_plan_execute", "tnx_plan_destroy", "tnx_plan_execute_static",
     "tnx_heff_create", "tnx_heff_create_for",
-    "tnx_heff_closed", "tnx_heff_out_keys", "tnx_heff_flops", "tnx_heff_set_operators", "tnx_heff_destroy",
+    "tnx_heff_closed", "tnx_heff_set_schedule", "tnx_heff_get_schedule", "tnx_heff_out_keys", "tnx_heff_flops", "tnx_heff_set_operators", "tnx_heff_destroy",
     "tnx_heff_batch_create", "tnx_heff_batch_apply", "tnx_heff_batch_apply_host", "tnx_heff_batch_size",
     "tnx_heff_batch_apply_stage", "tnx_heff_stage_flops",
     "tnx_heff_batch_launches", "tnx_heff_batch_error",

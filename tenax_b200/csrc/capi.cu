@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -855,11 +856,144 @@ extern "C" int tnx_plan_execute_static(const tnx_plan* plan, const double* const
   })
 }
 
+namespace {
+// ---------------------------------------------------------------------------
+// Fused H_eff stages 1-3 (heff_fused.cu): the per-operator layout.  A tile is
+// (MPO pair (q_c, q_d), c-tile of cc values, d-tile of 128); every input
+// block (q_b, q_p, q_q) and physical element pair (p, q) of the pair is one
+// MMA chain: A = the theta block's (p, q) slice as rows d, B = the L block's
+// rows (c, b) of the tile's c values, both K = a.
+// ---------------------------------------------------------------------------
+struct FusedBlk {
+  int32_t th_blk, pp, qq, l_blk, mb, ma, n_mma, col, slot0, slot_stride;
+};
+struct FusedLayout {
+  int32_t cc = 0;
+  std::vector<std::vector<FusedBlk>> blocks;  // per MPO pair
+  std::vector<int64_t> lp_off;                // per L block: byte offset of its panels in one plane (-1: unused)
+  std::vector<int32_t> lp_nmma, lp_nKt;
+  int64_t lp_bytes = 0;                       // bytes of one plane (hi; lo follows for BF16x3)
+  std::map<std::array<int32_t, 3>, int64_t> thp_tile0;  // (theta block, p, q) -> first 16 KB tile
+  int64_t thp_tiles = 0;
+  std::string why_not;  // non-empty: the structure does not fit the fused kernel
+};
+
+int32_t round16(int64_t x) { return static_cast<int32_t>((x + 15) / 16 * 16); }
+
+FusedLayout fused_layout(const HeffPlan& H, int mode, int32_t cc_req) {
+  FusedLayout F;
+  const int tk = img_geom(mode).tk;
+  std::map<std::pair<int32_t, int32_t>, int> l_by_bc;  // (q_b, q_c) -> L block
+  for (size_t i = 0; i < H.L.keys.size(); ++i) {
+    auto key = std::make_pair(H.L.keys[i][1], H.L.keys[i][2]);
+    if (l_by_bc.count(key)) {
+      F.why_not = "an L block is not determined by its (q_b, q_c)";
+      return F;
+    }
+    l_by_bc[key] = static_cast<int>(i);
+  }
+  std::map<Key, int> th_by_key;
+  for (size_t i = 0; i < H.th.keys.size(); ++i) th_by_key[H.th.keys[i]] = static_cast<int>(i);
+  F.blocks.resize(H.pairs.size());
+  for (size_t p = 0; p < H.pairs.size(); ++p) {
+    const MpoPair& mp = H.pairs[p];
+    if (mp.n_in_slots > kFusedMaxSlots) {
+      F.why_not = "an MPO pair has more than " + std::to_string(kFusedMaxSlots) + " input slots";
+      return F;
+    }
+    for (size_t ii = 0; ii < mp.ins.size(); ++ii) {
+      const MpoIn& in = mp.ins[ii];
+      const Key& ik = H.mpo_in_keys[p][ii];  // (q_b, q_p, q_q)
+      auto lit = l_by_bc.find({ik[0], mp.qc});
+      if (lit == l_by_bc.end()) {
+        F.why_not = "internal: no L block for an X1 block";
+        return F;
+      }
+      const int lb = lit->second;
+      const int32_t qa = H.L.keys[lb][0];
+      auto tit = th_by_key.find(Key{qa, ik[1], ik[2], mp.qd});
+      if (tit == th_by_key.end()) {
+        F.why_not = "internal: no theta block for an X1 block";
+        return F;
+      }
+      const int tb = tit->second;
+      const auto& ld = H.L.dims[lb];
+      const auto& td = H.th.dims[tb];
+      if (ld[0] != td[0] || ld[1] != in.mb || ld[2] != mp.mc || td[1] != in.mp || td[2] != in.mq || td[3] != mp.md) {
+        F.why_not = "internal: inconsistent block dims";
+        return F;
+      }
+      for (int pp = 0; pp < in.mp; ++pp)
+        for (int qq = 0; qq < in.mq; ++qq)
+          F.blocks[p].push_back(FusedBlk{tb, pp, qq, lb, in.mb, static_cast<int32_t>(ld[0]), 0, 0,
+                                         mp.in_slot0[ii] + pp * in.mq + qq, in.mp * in.mq});
+    }
+  }
+  // c values per tile: the largest that fits every pair's blocks side by side
+  // in one accumulator, each block's panel within the kernel's operand stage
+  int64_t max_mc = 1;
+  for (auto& mp : H.pairs) max_mc = std::max<int64_t>(max_mc, mp.mc);
+  auto fits = [&](int32_t cc) {
+    for (auto& bl : F.blocks) {
+      int64_t cols = 0;
+      for (auto& b : bl) {
+        const int32_t n = round16(static_cast<int64_t>(b.mb) * cc);
+        if (n > kFusedMaxN) return false;
+        cols += n;
+      }
+      if (cols > kFusedAccCols) return false;
+    }
+    return true;
+  };
+  int32_t cc = 0;
+  if (cc_req > 0) {
+    if (fits(cc_req)) cc = cc_req;
+  } else {
+    for (int32_t c = 1; c <= std::min<int64_t>(32, max_mc); ++c)
+      if (fits(c)) cc = c;
+  }
+  if (cc == 0) {
+    F.why_not = "no c-tile fits the tensor-memory accumulator";
+    return F;
+  }
+  F.cc = cc;
+  // TMEM columns, the L panel layout and the theta panel tiles
+  F.lp_off.assign(H.L.keys.size(), -1);
+  F.lp_nmma.assign(H.L.keys.size(), 0);
+  F.lp_nKt.assign(H.L.keys.size(), 0);
+  for (auto& bl : F.blocks) {
+    int32_t col = 0;
+    for (auto& b : bl) {
+      b.n_mma = round16(static_cast<int64_t>(b.mb) * cc);
+      b.col = col;
+      col += b.n_mma;
+      if (F.lp_off[b.l_blk] < 0) {
+        const auto& ld = H.L.dims[b.l_blk];
+        F.lp_nmma[b.l_blk] = b.n_mma;
+        F.lp_nKt[b.l_blk] = static_cast<int32_t>(cdiv(ld[0], tk));
+        F.lp_off[b.l_blk] = F.lp_bytes;
+        F.lp_bytes += cdiv(ld[2], cc) * F.lp_nKt[b.l_blk] * static_cast<int64_t>(b.n_mma) * 128;
+      }
+      const std::array<int32_t, 3> tkey{b.th_blk, b.pp, b.qq};
+      if (!F.thp_tile0.count(tkey)) {
+        const auto& td = H.th.dims[b.th_blk];
+        F.thp_tile0[tkey] = F.thp_tiles;
+        F.thp_tiles += cdiv(td[3], 128) * cdiv(td[0], tk);
+      }
+    }
+  }
+  return F;
+}
+}  // namespace
+
 extern "C" {
 
 // ---------------------------------------------------------------------------
 // H_eff
 // ---------------------------------------------------------------------------
+// default of tnx_heff_schedule.fuse_mpo for mixed-precision operators
+constexpr int32_t kDefaultFuse = 0;
+
 struct tnx_heff {
   HeffPlan H;
   int prec = -1;
@@ -868,6 +1002,13 @@ struct tnx_heff {
   PairGeom g1, g4;
   bool terms_ready = false;
   double out_scale = 1.0;  // 2^(eL + eR): undoes the operator range scaling
+  // schedule requested by tnx_heff_set_schedule, applied by tnx_heff_set_operators
+  int32_t sched_fuse = kDefaultFuse, sched_cc = 0;
+  int32_t plan_prec = TNX_PREC_FP64;  // precision given to tnx_heff_create_for
+  // fused stages 1-3 (mixed precisions): layout and L panels (hi plane, then lo)
+  bool fused = false;
+  FusedLayout fl;
+  DevMem lp_img;
 };
 
 int tnx_heff_create(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, const tnx_tensor_desc* Wl,
@@ -888,7 +1029,39 @@ int tnx_heff_create_for(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, 
     tR.subs = "dfg";
     // the mixed precisions read X1 with aligned 32-byte loads (see tnx_heff_set_operators)
     x->H = plan_heff(tL, tT, tWl, tWr, tR, img_mode_of(precision) == IMG_F64 ? 1 : kMpoKAlign);
+    x->plan_prec = precision;
     *h = x.release();
+    return TNX_OK;
+  })
+}
+
+int tnx_heff_set_schedule(tnx_heff* h, const tnx_heff_schedule* sched) {
+  if (!h || !sched) return set_err(TNX_ERR_VALUE, "null argument");
+  if (sched->c_per_tile < 0 || sched->c_per_tile > 32) return set_err(TNX_ERR_VALUE, "c_per_tile must be in [0, 32]");
+  h->sched_fuse = sched->fuse_mpo ? 1 : 0;
+  h->sched_cc = sched->c_per_tile;
+  return TNX_OK;
+}
+
+int tnx_heff_get_schedule(const tnx_heff* h, tnx_heff_schedule* sched) {
+  if (!h || !sched) return set_err(TNX_ERR_VALUE, "null argument");
+  TNX_TRY({
+    if (h->prec < 0) {
+      // before tnx_heff_set_operators: the schedule the planned precision would get
+      const int mode = img_mode_of(h->plan_prec);
+      bool fz = false;
+      int32_t cc = 0;
+      if (mode != IMG_F64 && h->sched_fuse && h->H.closed && h->H.s4_separable) {
+        const FusedLayout fl = fused_layout(h->H, mode, h->sched_cc);
+        fz = fl.why_not.empty();
+        cc = fl.cc;
+      }
+      sched->fuse_mpo = fz ? 1 : 0;
+      sched->c_per_tile = fz ? cc : 0;
+      return TNX_OK;
+    }
+    sched->fuse_mpo = h->fused ? 1 : 0;
+    sched->c_per_tile = h->fused ? h->fl.cc : 0;
     return TNX_OK;
   })
 }
@@ -934,11 +1107,19 @@ int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const
     h->terms_ready = true;
     h->g1 = pair_geom(H.s1, mode);
     h->g4 = pair_geom(H.s4, mode);
-    h->l_img.alloc(std::max<int64_t>(1, h->g1.a_tiles) * ig.tile_bytes * split);
+    // fused stages 1-3 where the schedule asks for it and the structure fits
+    h->fused = false;
+    h->fl = FusedLayout{};
+    if (mode != IMG_F64 && h->sched_fuse) {
+      h->fl = fused_layout(H, mode, h->sched_cc);
+      h->fused = h->fl.why_not.empty();
+    }
+    // the stage-1 A image (L) only serves the unfused path
+    h->l_img.alloc(h->fused ? 0 : std::max<int64_t>(1, h->g1.a_tiles) * ig.tile_bytes * split);
     h->r_img.alloc(std::max<int64_t>(1, h->g4.b_tiles) * ig.tile_bytes * split);
     h->l_lo = h->g1.a_tiles * ig.tile_bytes;
     h->r_lo = h->g4.b_tiles * ig.tile_bytes;
-    CUDA_OK(cudaMemsetAsync(h->l_img.p, 0, h->l_img.n, st));
+    if (h->l_img.n) CUDA_OK(cudaMemsetAsync(h->l_img.p, 0, h->l_img.n, st));
     CUDA_OK(cudaMemsetAsync(h->r_img.p, 0, h->r_img.n, st));
     // Environments can sit far outside the FP32/BF16 range (a random MPS's
     // environments shrink geometrically with length): pack L and R divided by
@@ -955,10 +1136,44 @@ int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const
     auto pow2_of = [](double m) { return (m > 0.0 && std::isfinite(m)) ? std::ldexp(1.0, std::ilogb(m)) : 1.0; };
     const double sL = pow2_of(mx[0]), sR = pow2_of(mx[1]);
     h->out_scale = sL * sR;
+    if (h->fused) {
+      h->lp_img.alloc(std::max<int64_t>(1, h->fl.lp_bytes) * split);
+      CUDA_OK(cudaMemsetAsync(h->lp_img.p, 0, h->lp_img.n, st));
+      std::vector<DevLPanelSeg> segs;
+      std::vector<int4> chunks;
+      for (size_t lb = 0; lb < H.L.keys.size(); ++lb) {
+        if (h->fl.lp_off[lb] < 0) continue;
+        const auto& ld = H.L.dims[lb];
+        DevLPanelSeg g{};
+        g.src_off = H.L.offs[lb];
+        g.img_addr = reinterpret_cast<uint64_t>(h->lp_img.p) + static_cast<uint64_t>(h->fl.lp_off[lb]);
+        g.lo_off = h->fl.lp_bytes;
+        g.ma = static_cast<int32_t>(ld[0]);
+        g.mb = static_cast<int32_t>(ld[1]);
+        g.mc = static_cast<int32_t>(ld[2]);
+        g.cc = h->fl.cc;
+        g.n_mma = h->fl.lp_nmma[lb];
+        g.nKt = h->fl.lp_nKt[lb];
+        g.scale = 1.0 / sL;
+        const int id = static_cast<int>(segs.size());
+        segs.push_back(g);
+        const int64_t n = ld[0] * ld[1] * ld[2];
+        for (int64_t e0 = 0; e0 < n; e0 += 256) chunks.push_back(make_int4(id, static_cast<int>(e0 / 256), 0, 0));
+      }
+      DevMem dseg, dch;
+      upload(dseg, segs, st);
+      upload(dch, chunks, st);
+      launch_pack_lpanels(mode, L, dseg.as<DevLPanelSeg>(), dch.as<int4>(), static_cast<int>(chunks.size()), st);
+      CUDA_OK(cudaGetLastError());
+      CUDA_OK(cudaStreamSynchronize(st));
+    } else {
+      h->lp_img.alloc(0);
+    }
     std::vector<DevPackSeg> pl, pr;
     std::vector<DevChunk> cl, cr;
-    build_pack(H.s1.packA, h->g1, true, reinterpret_cast<uint64_t>(h->l_img.p), h->l_lo, ig.tile_bytes, 0, pl, cl,
-               1.0 / sL);
+    if (!h->fused)
+      build_pack(H.s1.packA, h->g1, true, reinterpret_cast<uint64_t>(h->l_img.p), h->l_lo, ig.tile_bytes, 0, pl, cl,
+                 1.0 / sL);
     build_pack(H.s4.packB, h->g4, false, reinterpret_cast<uint64_t>(h->r_img.p), h->r_lo, ig.tile_bytes, 1, pr, cr,
                1.0 / sR);
     DevMem dpl, dcl, dpr, dcr, tab;
@@ -1004,6 +1219,12 @@ struct tnx_heff_batch {
   DevMem zero_chunks;  // theta-layout blocks H_eff never writes (slot = problem + 1)
   int n_zero_chunks = 0;
   DevMem err, src_tab, out_tab1, out_tab4;
+  // fused stages 1-3: theta panels (hi plane, then lo) and the kernel's tables
+  bool fused = false;
+  DevMem thp_img, thp_rows, thp_row_chunks;
+  int n_thp_row_chunks = 0;
+  DevMem f_pairs, f_blocks, f_tb, f_terms, f_tiles;
+  int n_f_tiles = 0;
   const int32_t* skip = nullptr;
   int n_launches = 0;
   std::vector<uint64_t> last_src, last_out;
@@ -1044,8 +1265,11 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     const bool f32 = mode != IMG_F64;
     for (int i = 0; i < n; ++i) {
       if (hs[i]->prec != precision) return set_err(TNX_ERR_VALUE, "operators were packed for another precision");
+      if (hs[i]->fused != hs[0]->fused)
+        return set_err(TNX_ERR_VALUE, "operators of one batch must all run fused stages 1-3 or all unfused");
       b->hs.push_back(hs[i]);
     }
+    b->fused = hs[0]->fused;
     for (int i = 0; i < n; ++i) {
       b->th_off.push_back(b->th_total);
       b->th_total += hs[i]->H.th.total;
@@ -1062,13 +1286,34 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
       x3_tiles += hs[i]->g4.a_tiles;
       for (auto& g : H.s1.groups) x1_elems += g.M * x1_ld(g.N);
     }
-    b->th_img.alloc(std::max<int64_t>(1, th_tiles) * ig.tile_bytes * split);
+    // the unfused path's stage-1 B image and X1 result; the fused path's theta panels
+    const bool fz = b->fused;
+    b->th_img.alloc(fz ? 16 : std::max<int64_t>(1, th_tiles) * ig.tile_bytes * split);
     b->x3_img.alloc(std::max<int64_t>(1, x3_tiles) * ig.tile_bytes * split);
     b->th_lo = th_tiles * ig.tile_bytes;
     b->x3_lo = x3_tiles * ig.tile_bytes;
-    b->x1.alloc(std::max<int64_t>(1, x1_elems) * (f32 ? 4 : 8));
+    b->x1.alloc(fz ? 16 : std::max<int64_t>(1, x1_elems) * (f32 ? 4 : 8));
     CUDA_OK(cudaMemset(b->th_img.p, 0, b->th_img.n));
     CUDA_OK(cudaMemset(b->x3_img.p, 0, b->x3_img.n));
+    std::vector<int64_t> thp_t0(n, 0);
+    int64_t thp_tiles = 0;
+    if (fz) {
+      for (int i = 0; i < n; ++i) {
+        thp_t0[i] = thp_tiles;
+        thp_tiles += hs[i]->fl.thp_tiles;
+      }
+      b->thp_img.alloc(std::max<int64_t>(1, thp_tiles) * ig.tile_bytes * split);
+      CUDA_OK(cudaMemset(b->thp_img.p, 0, b->thp_img.n));
+    }
+    const uint64_t thp_base = reinterpret_cast<uint64_t>(b->thp_img.p);
+    const int64_t thp_lo = thp_tiles * ig.tile_bytes;
+    std::vector<DevRowPackSeg> fth;
+    std::vector<int4> fthc;
+    std::vector<DevFPair> FP;
+    std::vector<DevFBlock> FB;
+    std::vector<int32_t> FTB;
+    std::vector<DevFTerm> FT;
+    std::vector<std::pair<int64_t, DevFTile>> FTL;
     const uint64_t th_base = reinterpret_cast<uint64_t>(b->th_img.p);
     const uint64_t x3_base = reinterpret_cast<uint64_t>(b->x3_img.p);
     const uint64_t x1_base = reinterpret_cast<uint64_t>(b->x1.p);
@@ -1118,11 +1363,37 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         rs.rows = static_cast<int32_t>(ps.count / ps.dims[0]);
         rs.src_slot = i;
         rs.scale = 1.0;
+        rs.kstride = rs.rows;
         const int id = static_cast<int>(trs.size());
         trs.push_back(rs);
         const int nkc = (rs.kval + kMpoKAlign - 1) / kMpoKAlign, cpt = pack_rows_chunks_per_thread();
         for (int r0 = 0; r0 < rs.rows; r0 += 256)
           for (int kc = 0; kc < nkc; kc += cpt) trc.push_back(make_int4(id, r0, kc, 0));
+      }
+      if (fz) {
+        // theta panels: each referenced (theta block, p, q) slice as rows d, K = a
+        const int tk = ig.tk;
+        for (const auto& kv : h->fl.thp_tile0) {
+          const int tb = kv.first[0], pp = kv.first[1], qq = kv.first[2];
+          const auto& td = H.th.dims[tb];
+          DevRowPackSeg rs{};
+          rs.src_off = H.th.offs[tb] + (static_cast<int64_t>(pp) * td[2] + qq) * td[3];
+          rs.img_addr = thp_base + static_cast<uint64_t>(thp_t0[i] + kv.second) * ig.tile_bytes;
+          rs.lo_off = thp_lo;
+          rs.row0 = 0;
+          rs.k0 = 0;
+          rs.nKt = static_cast<int32_t>(cdiv(td[0], tk));
+          rs.rows = static_cast<int32_t>(td[3]);
+          rs.kval = static_cast<int32_t>(td[0]);
+          rs.src_slot = i;
+          rs.scale = 1.0;
+          rs.kstride = td[1] * td[2] * td[3];
+          const int id = static_cast<int>(fth.size());
+          fth.push_back(rs);
+          const int nkc = (rs.kval + kMpoKAlign - 1) / kMpoKAlign, cpt = pack_rows_chunks_per_thread();
+          for (int r0 = 0; r0 < rs.rows; r0 += 256)
+            for (int kc = 0; kc < nkc; kc += cpt) fthc.push_back(make_int4(id, r0, kc, 0));
+        }
       }
       // stage-1 groups
       std::vector<int64_t> x1_goff;
@@ -1209,7 +1480,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
                                         esz;
                 sl.ld = ld;
                 // the FP32 MPO kernel loads 8 consecutive d (padding included) with 16-byte loads
-                if (f32 && (H.x1_align != kMpoKAlign || sl.base % 32 != 0 || ld % 8 != 0))
+                if (f32 && !fz && (H.x1_align != kMpoKAlign || sl.base % 32 != 0 || ld % 8 != 0))
                   return set_err(TNX_ERR_RUNTIME, "internal: X1 slot not aligned for the vector MPO loads");
                 MI.push_back(sl);
               }
@@ -1236,6 +1507,52 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         for (auto& t : mp.terms) MT.push_back({t.out_slot, t.in_slot, t.w});
         const int pair_id = static_cast<int>(MP.size());
         MP.push_back(dp);
+        if (fz) {
+          // fused tables of this pair: its MMA blocks, its terms by output slot, its tiles
+          const FusedLayout& fl = h->fl;
+          const int tk = ig.tk;
+          DevFPair fp{};
+          fp.blk0 = static_cast<int32_t>(FB.size());
+          fp.n_blk = static_cast<int32_t>(fl.blocks[pi].size());
+          fp.tb0 = static_cast<int32_t>(FTB.size());
+          fp.n_out = mp.n_out_slots;
+          fp.out0 = dp.out0;
+          fp.n_in = mp.n_in_slots;
+          fp.mc = mp.mc;
+          fp.md = mp.md;
+          fp.cc = fl.cc;
+          int64_t work = 0;
+          for (const FusedBlk& fb : fl.blocks[pi]) {
+            DevFBlock d{};
+            d.a_addr = thp_base + static_cast<uint64_t>(thp_t0[i] + fl.thp_tile0.at({fb.th_blk, fb.pp, fb.qq})) *
+                                      ig.tile_bytes;
+            d.b_addr = reinterpret_cast<uint64_t>(h->lp_img.p) + static_cast<uint64_t>(fl.lp_off[fb.l_blk]);
+            d.a_lo = thp_lo;
+            d.b_lo = fl.lp_bytes;
+            d.nKt = static_cast<int32_t>(cdiv(fb.ma, tk));
+            d.kk_last = kk_last_of(fb.ma, b->mode);
+            d.n_mma = fb.n_mma;
+            d.col = fb.col;
+            d.mb = fb.mb;
+            d.slot0 = fb.slot0;
+            d.slot_stride = fb.slot_stride;
+            FB.push_back(d);
+            work += static_cast<int64_t>(fb.n_mma) * d.nKt;
+          }
+          size_t u = 0;
+          for (int32_t o = 0; o < mp.n_out_slots; ++o) {
+            FTB.push_back(static_cast<int32_t>(FT.size()));
+            for (; u < mp.terms.size() && mp.terms[u].out_slot == o; ++u)
+              FT.push_back(DevFTerm{mp.terms[u].in_slot, static_cast<float>(mp.terms[u].w)});
+          }
+          FTB.push_back(static_cast<int32_t>(FT.size()));
+          if (u != mp.terms.size()) return set_err(TNX_ERR_RUNTIME, "internal: MPO terms not sorted by output slot");
+          const int fpair = static_cast<int>(FP.size());
+          FP.push_back(fp);
+          for (int64_t dt = 0; dt < cdiv(mp.md, 128); ++dt)
+            for (int64_t ct = 0; ct < cdiv(mp.mc, fl.cc); ++ct)
+              FTL.push_back({work, DevFTile{fpair, static_cast<int32_t>(ct), static_cast<int32_t>(dt), 0}});
+        }
         const int ppc = mpo_points_per_cta();
         const int dpt = mpo_d_per_thread(b->mode);
         const int npts = mp.mc * ((mp.md + dpt - 1) / dpt);
@@ -1270,6 +1587,55 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     upload(b->mpo_chunks, MC);
     upload(b->zero_chunks, ZC);
     b->n_zero_chunks = static_cast<int>(ZC.size());
+    if (fz) {
+      // every access of the fused kernel stays inside its buffers: theta panel
+      // tiles, L panels, TMEM columns, staging rows, terms and output slots
+      const uint64_t thp_end = thp_base + static_cast<uint64_t>(thp_tiles) * ig.tile_bytes;
+      for (const DevFPair& fp : FP) {
+        if (fp.n_blk < 1 || fp.n_in > kFusedMaxSlots || fp.out0 < 0 ||
+            fp.out0 + fp.n_out > static_cast<int64_t>(MO.size()) ||
+            fp.tb0 + fp.n_out + 1 > static_cast<int64_t>(FTB.size()) || fp.cc < 1)
+          return set_err(TNX_ERR_RUNTIME, "internal: fused pair table out of range");
+        for (int o = 0; o < fp.n_out; ++o)
+          for (int u = FTB[fp.tb0 + o]; u < FTB[fp.tb0 + o + 1]; ++u)
+            if (FT[u].in_slot < 0 || FT[u].in_slot >= fp.n_in)
+              return set_err(TNX_ERR_RUNTIME, "internal: fused term reads outside its pair's input slots");
+        const int64_t n_dt = cdiv(fp.md, 128);
+        for (int j = 0; j < fp.n_blk; ++j) {
+          const DevFBlock& d = FB[fp.blk0 + j];
+          if (d.n_mma < 16 || d.n_mma % 16 || d.n_mma > kFusedMaxN || d.col < 0 || d.col + d.n_mma > kFusedAccCols ||
+              d.mb * fp.cc > d.n_mma || d.nKt < 1 || d.slot0 < 0 || d.slot0 + (d.mb - 1) * d.slot_stride >= fp.n_in)
+            return set_err(TNX_ERR_RUNTIME, "internal: fused block geometry out of range");
+          const uint64_t a_last = d.a_addr + static_cast<uint64_t>(n_dt * d.nKt) * ig.tile_bytes;
+          if (d.a_addr < thp_base || a_last > thp_end)
+            return set_err(TNX_ERR_RUNTIME, "internal: fused theta panel outside its image");
+        }
+      }
+      for (int i = 0; i < n; ++i) {
+        const tnx_heff* h = hs[i];
+        const uint64_t lp0 = reinterpret_cast<uint64_t>(h->lp_img.p);
+        for (size_t lb = 0; lb < h->H.L.keys.size(); ++lb) {
+          if (h->fl.lp_off[lb] < 0) continue;
+          const int64_t bytes = cdiv(h->H.L.dims[lb][2], h->fl.cc) * h->fl.lp_nKt[lb] *
+                                static_cast<int64_t>(h->fl.lp_nmma[lb]) * 128;
+          if (h->fl.lp_off[lb] + bytes > h->fl.lp_bytes || lp0 == 0)
+            return set_err(TNX_ERR_RUNTIME, "internal: L panels outside their image");
+        }
+      }
+      upload(b->thp_rows, fth);
+      upload(b->thp_row_chunks, fthc);
+      b->n_thp_row_chunks = static_cast<int>(fthc.size());
+      upload(b->f_pairs, FP);
+      upload(b->f_blocks, FB);
+      upload(b->f_tb, FTB);
+      upload(b->f_terms, FT);
+      std::stable_sort(FTL.begin(), FTL.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+      std::vector<DevFTile> ftl;
+      ftl.reserve(FTL.size());
+      for (auto& x : FTL) ftl.push_back(x.second);
+      upload(b->f_tiles, ftl);
+      b->n_f_tiles = static_cast<int>(ftl.size());
+    }
     b->n_mpo_chunks = static_cast<int>(MC.size());
     b->err.alloc(sizeof(int32_t));
     CUDA_OK(cudaMemset(b->err.p, 0, sizeof(int32_t)));
@@ -1281,7 +1647,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     t1tab.p[0] = x1_base;
     CUDA_OK(cudaMemcpy(b->out_tab1.p, &t1tab, sizeof(PtrTab), cudaMemcpyHostToDevice));
     CUDA_OK(cudaDeviceSynchronize());
-    b->n_launches = 4 + (b->n_zero_chunks > 0 ? 1 : 0);
+    b->n_launches = (b->fused ? 3 : 4) + (b->n_zero_chunks > 0 ? 1 : 0);
     *out = b.release();
     return TNX_OK;
   })
@@ -1302,6 +1668,17 @@ int tnx_heff_batch_launches(const tnx_heff_batch* b, int32_t* n_launches) {
 static void heff_batch_stage(tnx_heff_batch* b, int stage, cudaStream_t st, const uint64_t* src_tab,
                              const uint64_t* out_tab4) {
   const bool f32 = b->mode != IMG_F64;
+  if (b->fused && stage < 3) {
+    // 0: theta panels; 1: fused stages 1-3 (X3 image); 2: nothing (the MPO ran inside stage 1)
+    if (stage == 0)
+      launch_pack_rows(src_tab, b->thp_rows.as<DevRowPackSeg>(), b->thp_row_chunks.as<int4>(), b->n_thp_row_chunks,
+                       b->mode, b->skip, st);
+    else if (stage == 1)
+      launch_heff_fused(b->mode, b->f_pairs.as<DevFPair>(), b->f_blocks.as<DevFBlock>(), b->f_tb.as<int32_t>(),
+                        b->f_terms.as<DevFTerm>(), b->mpo_oslots.as<DevMpoOutSlot>(), b->f_tiles.as<DevFTile>(),
+                        b->n_f_tiles, b->err.as<int32_t>(), b->skip, st);
+    return;
+  }
   switch (stage) {
     case 0:
       if (b->th_by_rows)

@@ -56,6 +56,9 @@ __host__ __device__ inline int64_t img_byte_offset(int mode, int64_t tile0, int 
 // ---------------------------------------------------------------------------
 constexpr int kMaxLegsDev = 12;  // equals kMaxLegs of the planner
 constexpr int kMpoKAlignDev = 8;  // equals kMpoKAlign of the planner (stage-4 d padding)
+constexpr int kFusedMaxN = 96;     // fused H_eff: largest L panel (MMA N) of one input block
+constexpr int kFusedMaxSlots = 48; // fused H_eff: input slots of one MPO pair (epilogue staging rows)
+constexpr int kFusedAccCols = 256; // fused H_eff: TMEM columns of one tile's accumulator
 
 struct DevPackSeg {
   int64_t src_off;    // element offset of the block in operand buffer src_tab[src_slot]
@@ -80,6 +83,7 @@ struct DevRowPackSeg {
   int64_t lo_off;     // byte offset of the low-part image (BF16 split)
   int32_t row0, k0, nKt, rows, kval, src_slot;
   double scale;
+  int64_t kstride;    // source elements between consecutive k (>= rows)
 };
 
 struct DevScatSeg {
@@ -144,6 +148,82 @@ struct DevMpoTerm {
   int32_t out_slot, in_slot;
   double w;
 };
+
+// Fused H_eff stages 1-3 (heff_fused.cu).  A tile is (MPO pair (q_c, q_d),
+// c-tile, d-tile): its TMEM accumulator holds X1[d, (c, b)] of every input
+// block of the pair side by side, and its epilogue applies W_l W_r to write
+// X3 straight into the stage-4 operand image.
+struct DevFPair {
+  int32_t blk0, n_blk;  // DevFBlock range (one per input block and physical element pair (p, q))
+  int32_t tb0, n_out;   // term_begin[tb0 + o] .. [tb0 + o + 1]: the terms of output slot o
+  int32_t out0, n_in;   // DevMpoOutSlot range start; input slots (per-warp staging rows)
+  int32_t mc, md, cc;   // c extent, d extent, c values per tile
+  int32_t pad;
+};
+struct DevFBlock {
+  uint64_t a_addr;  // theta panel image (128-row tiles; tile (dt, kt) at index dt * nKt + kt)
+  uint64_t b_addr;  // L panel image (panel (ct, kt) at index ct * nKt + kt, n_mma rows each)
+  int64_t a_lo, b_lo;
+  int32_t nKt, kk_last, n_mma, col;  // K slabs, MMA K steps of the last slab, MMA N, TMEM column
+  int32_t mb, slot0, slot_stride;    // b extent; staging slot of (b = 0) and its stride per b
+  int32_t pad;
+};
+struct DevFTerm {
+  int32_t in_slot;
+  float w;
+};
+struct DevFTile {
+  int32_t pair, ct, dt, pad;
+};
+// An L block (a, b, c) -> panel image: row (c % cc) * mb + b of panel c / cc, K = a.
+struct DevLPanelSeg {
+  int64_t src_off;    // element offset of the block in the L buffer
+  uint64_t img_addr;  // panel 0 of this block
+  int64_t lo_off;
+  int32_t ma, mb, mc, cc, n_mma, nKt;
+  double scale;
+};
+
+// One aligned chunk of kMpoVec consecutive K of one image row (k a multiple
+// of kMpoVec): a single 16-byte swizzle unit of a BF16 row (hi and lo
+// images), two for TF32, four double pairs for FP64.
+constexpr int kMpoVec = kMpoKAlignDev;
+
+template <int MODE, typename AccT>
+static __device__ __forceinline__ void img_store_chunk(uint8_t* img, int64_t lo_offset, int nKt, int64_t row, int64_t k,
+                                                const AccT (&v)[kMpoVec]) {
+  // k is a multiple of kMpoVec
+  if constexpr (MODE == IMG_BF16) {
+    const int64_t off = img_byte_offset(MODE, 0, nKt, row, k);
+    uint32_t hi[4], lo[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const float a = static_cast<float>(v[2 * u]), b = static_cast<float>(v[2 * u + 1]);
+      const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+      const __nv_bfloat162 l = __floats2bfloat162_rn(a - __low2float(h), b - __high2float(h));
+      hi[u] = *reinterpret_cast<const uint32_t*>(&h);
+      lo[u] = *reinterpret_cast<const uint32_t*>(&l);
+    }
+    *reinterpret_cast<uint4*>(img + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<uint4*>(img + lo_offset + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  } else if constexpr (MODE == IMG_TF32) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      uint32_t t[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t[u]) : "f"(static_cast<float>(v[4 * h + u])));
+      *reinterpret_cast<uint4*>(img + img_byte_offset(MODE, 0, nKt, row, k + 4 * h)) = make_uint4(t[0], t[1], t[2],
+                                                                                                   t[3]);
+    }
+  } else {
+    // FP64 tiles XOR bits 2-3 of the in-row index: element pairs (2u, 2u+1) stay adjacent
+#pragma unroll
+    for (int u = 0; u < kMpoVec; u += 2)
+      *reinterpret_cast<double2*>(img + img_byte_offset(MODE, 0, nKt, row, k + u)) =
+          make_double2(static_cast<double>(v[u]), static_cast<double>(v[u + 1]));
+  }
+}
 
 // ---------------------------------------------------------------------------
 // PTX wrappers (sm_100a)

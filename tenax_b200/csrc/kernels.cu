@@ -152,45 +152,7 @@ void launch_zero_ranges(const uint64_t* out_tab, const DevChunk* chunks, int n_c
 // terms' loads are kept in flight per thread.  FP64 uses the per-point kernel.
 // ---------------------------------------------------------------------------
 constexpr int kMpoThreads = 256;
-constexpr int kMpoVec = 8;
 constexpr int kMpoTerms = 4;
-static_assert(kMpoVec == kMpoKAlignDev, "thread chunk must equal the stage-4 d padding");
-
-template <int MODE, typename AccT>
-__device__ __forceinline__ void img_store_chunk(uint8_t* img, int64_t lo_offset, int nKt, int64_t row, int64_t k,
-                                                const AccT (&v)[kMpoVec]) {
-  // k is a multiple of kMpoVec
-  if constexpr (MODE == IMG_BF16) {
-    const int64_t off = img_byte_offset(MODE, 0, nKt, row, k);
-    uint32_t hi[4], lo[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const float a = static_cast<float>(v[2 * u]), b = static_cast<float>(v[2 * u + 1]);
-      const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-      const __nv_bfloat162 l = __floats2bfloat162_rn(a - __low2float(h), b - __high2float(h));
-      hi[u] = *reinterpret_cast<const uint32_t*>(&h);
-      lo[u] = *reinterpret_cast<const uint32_t*>(&l);
-    }
-    *reinterpret_cast<uint4*>(img + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-    *reinterpret_cast<uint4*>(img + lo_offset + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-  } else if constexpr (MODE == IMG_TF32) {
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      uint32_t t[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t[u]) : "f"(static_cast<float>(v[4 * h + u])));
-      *reinterpret_cast<uint4*>(img + img_byte_offset(MODE, 0, nKt, row, k + 4 * h)) = make_uint4(t[0], t[1], t[2],
-                                                                                                   t[3]);
-    }
-  } else {
-    // FP64 tiles XOR bits 2-3 of the in-row index: element pairs (2u, 2u+1) stay adjacent
-#pragma unroll
-    for (int u = 0; u < kMpoVec; u += 2)
-      *reinterpret_cast<double2*>(img + img_byte_offset(MODE, 0, nKt, row, k + u)) =
-          make_double2(static_cast<double>(v[u]), static_cast<double>(v[u + 1]));
-  }
-}
 
 template <int MODE>
 __global__ void __launch_bounds__(kMpoThreads) mpo_apply_kernel(
@@ -343,7 +305,7 @@ __global__ void __launch_bounds__(256) pack_rows_kernel(const uint64_t* __restri
 #pragma unroll
     for (int u = 0; u < kMpoVec; ++u) {
       const int a = (ch.z + j) * kMpoVec + u;
-      v[j][u] = a < s.kval ? static_cast<ValT>(src[static_cast<int64_t>(a) * s.rows] * s.scale) : ValT(0);
+      v[j][u] = a < s.kval ? static_cast<ValT>(src[static_cast<int64_t>(a) * s.kstride] * s.scale) : ValT(0);
     }
 #pragma unroll
   for (int j = 0; j < kChunks; ++j)

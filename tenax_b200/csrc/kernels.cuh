@@ -65,5 +65,12 @@ void launch_gemm_f64(const DevGroup* groups, const DevTile* tiles, int n_tiles, 
 void launch_gemm_tc(int mode, const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
                     const uint64_t* out_tab, bool out_f64, int32_t* err_flag, const int32_t* skip, cudaStream_t st);
 int device_sm_count();
+// fused H_eff stages 1-3 (tcgen05, mode IMG_BF16 or IMG_TF32): X3 image from theta and L panels
+void launch_heff_fused(int mode, const DevFPair* pairs, const DevFBlock* blocks, const int32_t* term_begin,
+                       const DevFTerm* terms, const DevMpoOutSlot* oslots, const DevFTile* tiles, int n_tiles,
+                       int32_t* err_flag, const int32_t* skip, cudaStream_t st);
+// L block -> panel image (chunks: (segment, 256-element block, -, -))
+void launch_pack_lpanels(int mode, const double* L, const DevLPanelSeg* segs, const int4* chunks, int n_chunks,
+                         cudaStream_t st);
 
 }  // namespace tnx

@@ -667,6 +667,8 @@ HeffPlan plan_heff(const TensorStruct& L, const TensorStruct& th, const TensorSt
       H.pairs.push_back({});
       H.mpo_in_keys.push_back({});
       H.mpo_out_keys.push_back({});
+      H.pairs.back().qc = k[1];
+      H.pairs.back().qd = k[4];
       H.pairs.back().mc = static_cast<int32_t>(d[1]);
       H.pairs.back().md = static_cast<int32_t>(d[4]);
     }

@@ -146,6 +146,7 @@ struct MpoTerm { // y[out_slot] += w * x[in_slot]
   double w;
 };
 struct MpoPair {
+  int32_t qc = 0, qd = 0;  // charges of the pair's c and d sectors
   int32_t mc, md;
   std::vector<MpoIn> ins;
   std::vector<MpoOut> outs;

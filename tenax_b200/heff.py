@@ -91,15 +91,19 @@ HEFF_SUBSCRIPTS = "abc,apqd,bpse,eqtf,dfg->cstg"  # algorithms/dmrg.py:1282-1289
 class HeffOperator:
     """H_eff of one two-site problem; theta/outputs live on a closed key set.
 
-    The fused path (four launches per apply, batchable) needs every stage-4
-    group to write a single output charge, which the sector structures of
-    U(1) MPS/MPO problems satisfy.  Other structures (``fused`` False) apply
+    The fused path (three or four launches per apply, batchable) needs every
+    stage-4 group to write a single output charge, which the sector
+    structures of U(1) MPS/MPO problems satisfy.  With a mixed precision,
+    ``schedule={"fuse_mpo": 1}`` runs stages 1-3 as one kernel that applies
+    W_l W_r straight from tensor memory (``c_per_tile`` sets the fused
+    tile's c extent), ``{"fuse_mpo": 0}`` the stage-1 GEMM, X1 in HBM and
+    the MPO kernel; ``self.schedule`` reports the schedule in effect.  Other structures (``fused`` False) apply
     H_eff through the general unfiltered contraction engine, the
     reference's ``_blockwise_contract`` semantics, one pairwise chain per
     apply: the same result, without the fused kernels."""
 
     def __init__(self, L: SymmetricTensor, Wl: SymmetricTensor, Wr: SymmetricTensor, R: SymmetricTensor,
-                 theta_indices, theta_keys, precision: str = "fp64"):
+                 theta_indices, theta_keys, precision: str = "fp64", schedule: dict | None = None):
         self.theta_indices = tuple(theta_indices)
         # the closure's last plan is the operator's plan (created for its precision)
         self.key_seq, self.handle, self._hold = _closure(L, theta_indices, theta_keys, Wl, Wr, R, precision)
@@ -109,11 +113,18 @@ class HeffOperator:
         self.fused = bool(closed.value)
         self.precision = precision
         self.flops = float(_capi.LIB.tnx_heff_flops(self.handle))
+        self.schedule = {"fuse_mpo": 0, "c_per_tile": 0}
         if self.fused:
+            if schedule is not None:
+                req = _capi.HeffSchedule(int(schedule.get("fuse_mpo", 1)), int(schedule.get("c_per_tile", 0)))
+                _capi.check(_capi.LIB.tnx_heff_set_schedule(self.handle, C.byref(req)))
             _capi.check(_capi.LIB.tnx_heff_set_operators(self.handle, L.data.data_ptr(), Wl.data.data_ptr(),
                                                          Wr.data.data_ptr(), R.data.data_ptr(),
                                                          _capi.PRECISIONS[precision],
                                                          torch.cuda.current_stream().cuda_stream))
+            got = _capi.HeffSchedule()
+            _capi.check(_capi.LIB.tnx_heff_get_schedule(self.handle, C.byref(got)))
+            self.schedule = {"fuse_mpo": int(got.fuse_mpo), "c_per_tile": int(got.c_per_tile)}
         else:
             self._operands = (L, Wl, Wr, R)
         sizes = [int(np.prod([int(np.count_nonzero(i.charges == q)) for i, q in zip(self.theta_indices, k)]))

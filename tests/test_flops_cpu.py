@@ -35,3 +35,34 @@ def test_oracle_flops_equal_planner(chi):
     _capi.LIB.tnx_heff_destroy(h)
     assert f_oracle == f_plan
     assert f_oracle > 0
+
+
+@pytest.mark.parametrize("chi", [256, 512, 1024, 2048])
+def test_benchmark_structures_plan_fused(chi):
+    """Host planning of the fused stages 1-3 on the benchmark's structures:
+    asked for, every split-BF16x3 and TF32 operator gets the fused kernel
+    (cylinder MPO: at most 36 input slots per sector pair), FP64 never does,
+    and out-of-range tile extents are rejected."""
+    from tenax_b200 import _capi
+
+    b = _bench()
+    args, _ = b.HostProblems(3).make(chi, fill=False)
+    hold = [_capi.DescHolder([l.charges for l in t.legs], [l.flow for l in t.legs], sorted(t.blocks), None)
+            for t in args]
+    for prec, want in (("bf16x3", 1), ("tf32", 1), ("fp64", 0)):
+        h = C.c_void_p()
+        _capi.check(_capi.LIB.tnx_heff_create_for(*[C.byref(x.desc) for x in hold], _capi.PRECISIONS[prec],
+                                                  C.byref(h)))
+        on = _capi.HeffSchedule(1, 0)
+        _capi.check(_capi.LIB.tnx_heff_set_schedule(h, C.byref(on)))
+        s = _capi.HeffSchedule()
+        _capi.check(_capi.LIB.tnx_heff_get_schedule(h, C.byref(s)))
+        assert s.fuse_mpo == want, (chi, prec)
+        assert (s.c_per_tile >= 1) == bool(want)
+        off = _capi.HeffSchedule(0, 0)
+        _capi.check(_capi.LIB.tnx_heff_set_schedule(h, C.byref(off)))
+        _capi.check(_capi.LIB.tnx_heff_get_schedule(h, C.byref(s)))
+        assert s.fuse_mpo == 0
+        bad = _capi.HeffSchedule(1, 99)
+        assert _capi.LIB.tnx_heff_set_schedule(h, C.byref(bad)) == _capi.TNX_ERR_VALUE
+        _capi.LIB.tnx_heff_destroy(h)
