@@ -72,6 +72,36 @@ int tnx_valid_blocks(int32_t n_legs, const int32_t* charges, const int64_t* leg_
                      int32_t modulus, int32_t has_target, int64_t target, int64_t* n_keys, int32_t* keys_out,
                      int64_t keys_cap);
 
+/* Device-side sector planning (no counterpart in the reference's API: the
+ * same integer results as the host planner, computed by kernels on `stream`
+ * from charge arrays and block keys in DEVICE memory; each call reads back
+ * only the counts it returns and synchronises `stream`).  Limits: at most 12
+ * legs, a charge range of at most 65536 per leg, at most 65536 valid output
+ * keys per contraction.
+ *   tnx_valid_blocks_dev: tnx_valid_blocks (_compute_valid_blocks,
+ *     core/tensor.py:53-165) with charges_dev (all legs concatenated) and
+ *     keys_dev (n_keys x n_legs) on the device; keys_dev may be NULL.
+ *   tnx_contract_structure_dev: the output structure of a two-operand
+ *     filtered contraction (_contract_symmetric, contraction/contractor.py:
+ *     344-441): a->charges, a->keys, b->charges, b->keys are device
+ *     pointers, subs are required.  Writes the output keys in sorted order
+ *     (n_out_blocks x len(out_subs)), their block offsets (n_out_blocks + 1
+ *     entries, the last one the total), and the matched block pairs (A block,
+ *     B block, output block; int32 triples) ordered by A block then B block;
+ *     any output pointer may be NULL (counts only).
+ *   tnx_fused_charges_dev: _compute_fused_charges (algorithms/
+ *     _tensor_utils.py:191-203): out[i*d_b + j] = fused_flow*(flow_a qa[i] +
+ *     flow_b qb[j]) (mod n for Z_n, modulus > 0), device arrays. */
+int tnx_valid_blocks_dev(int32_t n_legs, const int32_t* charges_dev, const int64_t* leg_dims, const int32_t* flows,
+                         int32_t modulus, int32_t has_target, int64_t target, int64_t* n_keys, int32_t* keys_dev,
+                         int64_t keys_cap, void* stream);
+int tnx_contract_structure_dev(const tnx_tensor_desc* a, const tnx_tensor_desc* b, const char* out_subs,
+                               int32_t modulus, int64_t* n_out_blocks, int32_t* out_keys_dev, int64_t* out_offsets_dev,
+                               int64_t out_cap, int64_t* n_pairs, int32_t* pairs_dev, int64_t pairs_cap,
+                               void* stream);
+int tnx_fused_charges_dev(const int32_t* qa_dev, int64_t da, int32_t fa, const int32_t* qb_dev, int64_t db,
+                          int32_t fb, int32_t fused_flow, int32_t modulus, int32_t* out_dev, void* stream);
+
 /* Plan a block-sparse contraction of n_ops operands with subscripts
  * ops[i].subs -> out_subs.  mode TNX_MATCH_FILTERED reproduces
  * _contract_symmetric (contractor.py:291-484, output-target inference and
@@ -82,6 +112,16 @@ int tnx_valid_blocks(int32_t n_legs, const int32_t* charges, const int64_t* leg_
 int tnx_plan_create(const tnx_tensor_desc* ops, int32_t n_ops, const char* out_subs, int32_t mode,
                     int32_t modulus, const int32_t* out_charges, const int64_t* out_leg_dims,
                     const int32_t* out_flows, tnx_plan** plan);
+/* tnx_plan_create for operands of a fermionic symmetry (FermionParity,
+ * FermionicU1 with a built-in grading: parity = charge mod 2): every block
+ * combination of a one- or two-operand contraction carries the reference's
+ * exchange sign of the leg reordering (contraction/contractor.py:206-285,
+ * :460-470); a one-operand plan is then the Koszul-signed transpose
+ * (core/tensor.py:32-50).  fermionic = 0 is tnx_plan_create.  Three or more
+ * operands: TNX_ERR_UNSUPPORTED (contract pairwise). */
+int tnx_plan_create_graded(const tnx_tensor_desc* ops, int32_t n_ops, const char* out_subs, int32_t mode,
+                           int32_t modulus, const int32_t* out_charges, const int64_t* out_leg_dims,
+                           const int32_t* out_flows, int32_t fermionic, tnx_plan** plan);
 /* Output structure: blocks in sorted-key order, contiguous. keys may be NULL. */
 int tnx_plan_output(const tnx_plan* plan, int64_t* n_blocks, int32_t* keys, int64_t* total_elems,
                     int32_t* has_target, int64_t* target);

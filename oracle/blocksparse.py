@@ -36,6 +36,9 @@ class OTensor:
     legs: tuple
     blocks: dict = field(default_factory=dict)
     modulus: int | None = None
+    # fermionic grading (FermionParity: Z2; FermionicU1: U(1)), parity q mod 2
+    # for the built-in gradings (core/symmetry.py:311-440)
+    fermionic: bool = False
 
     def labels(self):
         return tuple(l.label for l in self.legs)
@@ -210,6 +213,83 @@ def labels_to_subscripts(tensors, output_labels=None):
     return ",".join(subs) + "->" + out, tuple(first[l] for l in output_labels)
 
 
+def parity(q) -> int:
+    """Z2 grading of a charge: FermionParity ``q % 2`` and FermionicU1's
+    built-in gradings ``|q| % 2`` / ``q % 2`` (core/symmetry.py:345-346,
+    367-371) all equal q mod 2 on integers."""
+    return int(q) % 2
+
+
+def inversion_pairs(in_subs, outp):
+    """Character pairs whose exchange can flip a fermionic contraction's sign
+    (contraction/contractor.py:206-285): all input characters in order, each
+    mapped to its target slot (the output characters, then the contracted
+    characters by first appearance; the two occurrences of a contracted
+    character take consecutive half-slots), and every inverted pair kept."""
+    all_chars = [c for s in in_subs for c in s]
+    counts = Counter(all_chars)
+    contracted = {c for c, n in counts.items() if n >= 2}
+    target = list(outp)
+    seen = set()
+    for c in all_chars:
+        if c in contracted and c not in seen:
+            target.append(c)
+            seen.add(c)
+    slot = {}
+    for i, c in enumerate(target):
+        slot.setdefault(c, i)
+    used: Counter = Counter()
+    perm = []
+    for c in all_chars:
+        perm.append(slot[c] * 2 + (used[c] if c in contracted else 0))
+        used[c] += 1
+    return [(all_chars[i], all_chars[j]) for i in range(len(all_chars)) for j in range(i + 1, len(all_chars))
+            if perm[i] > perm[j]]
+
+
+def koszul_sign(parities, perm) -> int:
+    """(-1) per inverted pair of odd elements (core/tensor.py:32-50)."""
+    sign = 1
+    for i in range(len(perm)):
+        for j in range(i + 1, len(perm)):
+            if perm[i] > perm[j] and parities[perm[i]] and parities[perm[j]]:
+                sign = -sign
+    return sign
+
+
+def transpose(t: OTensor, axes) -> OTensor:
+    """Leg permutation with the Koszul sign of fermionic blocks
+    (core/tensor.py:836-862)."""
+    axes = tuple(axes)
+    out = {}
+    for key, blk in t.blocks.items():
+        v = np.transpose(blk, axes)
+        if t.fermionic and koszul_sign([parity(q) for q in key], axes) < 0:
+            v = -v
+        out[tuple(key[i] for i in axes)] = v
+    return OTensor(tuple(t.legs[i] for i in axes), out, t.modulus, t.fermionic)
+
+
+def dagger(t: OTensor) -> OTensor:
+    """Conjugate with dual charges and flows; fermionic blocks take the twist
+    phase (-1)^(sum of parities) (core/tensor.py:795-820)."""
+    legs = tuple(Leg(np.asarray(dual_charges(l.charges, t.modulus), np.int32), -int(l.flow), l.label)
+                 for l in t.legs)
+    out = {}
+    for key, blk in t.blocks.items():
+        v = np.conj(blk)
+        if t.fermionic and sum(parity(q) for q in key) % 2:
+            v = -v
+        out[tuple(int(q) for q in dual_charges(np.asarray(key), t.modulus))] = v
+    return OTensor(legs, out, t.modulus, t.fermionic)
+
+
+def dual_charges(q, modulus):
+    """-q (U1) or (-q) mod n (Z_n) (core/symmetry.py:197-204, 239-246)."""
+    q = np.asarray(q, dtype=np.int64)
+    return (-q) if modulus is None else np.mod(-q, modulus)
+
+
 def contract_symmetric(tensors, subscripts):
     """Block-sparse contraction with the reference's filtered semantics.
 
@@ -262,6 +342,8 @@ def contract_symmetric(tensors, subscripts):
     for m in sig_maps[1:]:
         common &= set(m.keys())
 
+    fermionic = any(t.fermionic for t in tensors)
+    pairs = inversion_pairs(in_subs, outp) if fermionic else []
     out_blocks: dict = {}
     for sig in common:
         for combo in itertools.product(*[m[sig] for m in sig_maps]):
@@ -286,11 +368,18 @@ def contract_symmetric(tensors, subscripts):
                 res = np.einsum(subscripts, *[a for _, a in combo])
             except ValueError:
                 continue
+            # exchange sign of the leg reordering (contractor.py:460-470)
+            sign = 1
+            for ci, cj in pairs:
+                if parity(c2q[ci]) and parity(c2q[cj]):
+                    sign = -sign
+            if sign < 0:
+                res = -res
             if okey in out_blocks:
                 out_blocks[okey] = out_blocks[okey] + res
             else:
                 out_blocks[okey] = res
-    return OTensor(out_legs, out_blocks, modulus), output_target
+    return OTensor(out_legs, out_blocks, modulus, fermionic), output_target
 
 
 def blockwise_contract(tensors, subscripts, out_legs=None):

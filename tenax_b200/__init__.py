@@ -12,6 +12,8 @@ package's sm_100a kernels through the C ABI in ``include/tenax_b200.h``.
 from tenax_b200 import _capi  # noqa: F401  (loads libtenax_b200.so or raises)
 from tenax_b200.core import (  # noqa: F401
     BaseSymmetry,
+    FermionicU1,
+    FermionParity,
     FlowDirection,
     Label,
     TensorIndex,

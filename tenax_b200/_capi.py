@@ -67,12 +67,16 @@ def _load():
         "tnx_version": (C.c_int, []),
         "tnx_valid_blocks": (C.c_int, [i32, P, P, P, i32, i32, i64, P, P, i64]),
         "tnx_plan_create": (C.c_int, [P, i32, C.c_char_p, i32, i32, P, P, P, P]),
+        "tnx_plan_create_graded": (C.c_int, [P, i32, C.c_char_p, i32, i32, P, P, P, i32, P]),
         "tnx_plan_output": (C.c_int, [P, P, P, P, P, P]),
         "tnx_plan_workspace": (C.c_int, [P, i32, P]),
         "tnx_plan_flops": (dbl, [P]),
         "tnx_plan_execute": (C.c_int, [P, P, P, i32, P, C.c_size_t, P]),
         "tnx_plan_destroy": (None, [P]),
         "tnx_plan_execute_static": (C.c_int, [P, P, P, P]),
+        "tnx_valid_blocks_dev": (C.c_int, [i32, P, P, P, i32, i32, i64, P, P, i64, P]),
+        "tnx_contract_structure_dev": (C.c_int, [P, P, C.c_char_p, i32, P, P, P, i64, P, P, i64, P]),
+        "tnx_fused_charges_dev": (C.c_int, [P, i64, i32, P, i64, i32, i32, i32, P, P]),
         "tnx_heff_create": (C.c_int, [P, P, P, P, P, P]),
         "tnx_heff_create_for": (C.c_int, [P, P, P, P, P, i32, P]),
         "tnx_heff_closed": (C.c_int, [P, P]),
@@ -118,8 +122,10 @@ def _load():
 
 LIB = _load()
 EXPORTED = [
-    "tnx_last_error", "tnx_version", "tnx_valid_blocks", "tnx_plan_create", "tnx_plan_output",
+    "tnx_last_error", "tnx_version", "tnx_valid_blocks", "tnx_plan_create", "tnx_plan_create_graded",
+    "tnx_plan_output",
     "tnx_plan_workspace", "tnx_plan_flops", "tnx_plan_execute", "tnx_plan_destroy", "tnx_plan_execute_static",
+    "tnx_valid_blocks_dev", "tnx_contract_structure_dev", "tnx_fused_charges_dev",
     "tnx_heff_create", "tnx_heff_create_for",
     "tnx_heff_closed", "tnx_heff_set_schedule", "tnx_heff_get_schedule", "tnx_heff_out_keys", "tnx_heff_flops", "tnx_heff_set_operators", "tnx_heff_destroy",
     "tnx_heff_batch_create", "tnx_heff_batch_apply", "tnx_heff_batch_apply_host", "tnx_heff_batch_size",

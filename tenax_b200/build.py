@@ -16,8 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtenax_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
-SOURCES = ["planner.cpp", "kernels.cu", "gemm_f64.cu", "gemm_tc.cu", "heff_fused.cu", "svd.cu", "capi.cu"]
-HEADERS = ["planner.hpp", "common.cuh", "kernels.cuh", "tcgen05.cuh", "svd.hpp"]
+SOURCES = ["planner.cpp", "kernels.cu", "gemm_f64.cu", "gemm_tc.cu", "heff_fused.cu", "planner_dev.cu", "svd.cu", "capi.cu"]
+HEADERS = ["planner.hpp", "common.cuh", "kernels.cuh", "tcgen05.cuh", "planner_dev.hpp", "svd.hpp"]
 
 NVCC_FLAGS = [
     "-std=c++17",

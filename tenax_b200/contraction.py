@@ -32,7 +32,7 @@ def _stream_ptr() -> int:
 class Plan:
     """An owned ``tnx_plan`` handle plus its output structure."""
 
-    def __init__(self, tensors, in_subs, out_subs, mode, out_indices):
+    def __init__(self, tensors, in_subs, out_subs, mode, out_indices, fermionic: bool = False):
         self.holders = [
             _capi.DescHolder([i.charges for i in t.indices], [int(i.flow) for i in t.indices], t.keys, s)
             for t, s in zip(tensors, in_subs)
@@ -41,9 +41,10 @@ class Plan:
         out_h = _capi.DescHolder([i.charges for i in out_indices], [int(i.flow) for i in out_indices], [], None)
         modulus = tensors[0].indices[0].symmetry.n_values() if tensors[0].indices else None
         h = C.c_void_p()
-        _capi.check(_capi.LIB.tnx_plan_create(descs, len(tensors), out_subs.encode(), mode,
-                                              0 if modulus is None else int(modulus), out_h.charges.ctypes.data,
-                                              out_h.leg_dims.ctypes.data, out_h.flows.ctypes.data, C.byref(h)))
+        _capi.check(_capi.LIB.tnx_plan_create_graded(descs, len(tensors), out_subs.encode(), mode,
+                                                     0 if modulus is None else int(modulus), out_h.charges.ctypes.data,
+                                                     out_h.leg_dims.ctypes.data, out_h.flows.ctypes.data,
+                                                     int(bool(fermionic)), C.byref(h)))
         self.handle = h
         nb, tot, has_t, tgt = C.c_int64(), C.c_int64(), C.c_int32(), C.c_int64()
         _capi.check(_capi.LIB.tnx_plan_output(h, C.byref(nb), None, C.byref(tot), C.byref(has_t), C.byref(tgt)))
@@ -69,8 +70,20 @@ class Plan:
             self.handle = None
 
 
-def _structure_key(tensors, in_subs, out_subs, mode, out_indices):
-    parts = [mode, out_subs]
+def _fermionic(tensors) -> bool:
+    """Whether the operands carry a fermionic grading the engine signs with
+    (parity = charge mod 2); other gradings are rejected."""
+    sym = tensors[0].indices[0].symmetry if tensors and tensors[0].indices else None
+    if sym is None or not sym.is_fermionic:
+        return False
+    if not getattr(sym, "builtin_grading", True):
+        raise _capi.TnxUnsupported("fermionic contraction with a custom grading function: only the built-in "
+                                   "gradings (parity = charge mod 2) are supported")
+    return True
+
+
+def _structure_key(tensors, in_subs, out_subs, mode, out_indices, fermionic=False):
+    parts = [mode, out_subs, bool(fermionic)]
     for t, s in zip(tensors, in_subs):
         parts.append((s, tuple(int(i.flow) for i in t.indices), tuple(i.charges.tobytes() for i in t.indices),
                       tuple(t.keys)))
@@ -78,13 +91,13 @@ def _structure_key(tensors, in_subs, out_subs, mode, out_indices):
     return tuple(parts)
 
 
-def get_plan(tensors, in_subs, out_subs, mode, out_indices) -> Plan:
-    key = _structure_key(tensors, in_subs, out_subs, mode, out_indices)
+def get_plan(tensors, in_subs, out_subs, mode, out_indices, fermionic: bool = False) -> Plan:
+    key = _structure_key(tensors, in_subs, out_subs, mode, out_indices, fermionic)
     p = _PLANS.get(key)
     if p is not None:
         _PLANS.move_to_end(key)
         return p
-    p = Plan(tensors, in_subs, out_subs, mode, out_indices)
+    p = Plan(tensors, in_subs, out_subs, mode, out_indices, fermionic)
     _PLANS[key] = p
     if len(_PLANS) > _PLAN_CACHE_SIZE:
         _PLANS.popitem(last=False)
@@ -137,7 +150,8 @@ def _contract_symmetric(tensors, subscripts, output_indices=None, precision=None
         for ch, idx in zip(s, t.indices):
             c2i[ch] = idx
     out_indices = tuple(c2i[c] for c in out_subs)
-    plan = get_plan(tensors, in_subs, out_subs, _capi.MATCH_FILTERED, out_indices)
+    # fermionic operands: the exchange sign of the leg reordering (contractor.py:460-470)
+    plan = get_plan(tensors, in_subs, out_subs, _capi.MATCH_FILTERED, out_indices, _fermionic(tensors))
     data = plan.execute(tensors, precision or DEFAULT_PRECISION)
     out = SymmetricTensor.from_flat(out_indices, plan.out_keys, data)
     if plan.target is None:
@@ -155,11 +169,15 @@ def blockwise_contract(tensors, subscripts, output_indices, precision=None) -> S
 
 
 def transpose_symmetric(t: SymmetricTensor, axes) -> SymmetricTensor:
-    """Leg permutation of every block (core/tensor.py:832-861)."""
+    """Leg permutation of every block (core/tensor.py:832-861); fermionic
+    blocks take the Koszul sign of the permutation (core/tensor.py:32-50)."""
     chars = string.ascii_letters[: t.ndim]
     sub = chars + "->" + "".join(chars[a] for a in axes)
     new_idx = tuple(t.indices[a] for a in axes)
-    return blockwise_contract([t], sub, new_idx)
+    lhs, out_subs = sub.split("->")
+    plan = get_plan([t], [lhs], out_subs, _capi.MATCH_UNFILTERED, new_idx, _fermionic([t]))
+    data = plan.execute([t], DEFAULT_PRECISION)
+    return SymmetricTensor.from_flat(new_idx, plan.out_keys, data)
 
 
 def contract_with_subscripts(tensors, subscripts, output_indices, optimize="auto", precision=None):
@@ -241,6 +259,9 @@ def contract_ad(a: SymmetricTensor, b: SymmetricTensor, output_labels=None, prec
     """``contract(a, b)`` (contractor.py:490-531, filtered semantics) whose
     result's flat ``data`` carries autograd history: gradients flow to
     ``a.data`` / ``b.data`` through the hand-written block-sparse adjoint."""
+    if _fermionic((a, b)):
+        raise TnxUnsupportedAD("contract_ad: the adjoint of a fermionic contraction carries exchange signs "
+                               "this engine does not apply to gradients")
     subscripts, out_idx = _labels_to_subscripts((a, b), output_labels)
     lhs, so = subscripts.split("->")
     sa, sb = lhs.split(",")

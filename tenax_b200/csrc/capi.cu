@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "planner.hpp"
+#include "planner_dev.hpp"
 #include "svd.hpp"
 
 using namespace tnx;
@@ -185,7 +186,7 @@ void build_pack(const std::vector<PackSeg>& segs, const PairGeom& G, bool a_side
     d.nlegs = s.nlegs;
     d.src_slot = src_slot;
     d.kcount = 1;
-    d.scale = scale;
+    d.scale = s.neg ? -scale : scale;
     for (int l = 0; l < s.nlegs; ++l) {
       d.dims[l] = s.dims[l];
       d.rstr[l] = s.rstr[l];
@@ -296,6 +297,97 @@ int tnx_valid_blocks(int32_t n_legs, const int32_t* charges, const int64_t* leg_
 int tnx_plan_create(const tnx_tensor_desc* ops, int32_t n_ops, const char* out_subs, int32_t mode,
                     int32_t modulus, const int32_t* out_charges, const int64_t* out_leg_dims,
                     const int32_t* out_flows, tnx_plan** plan) {
+  return tnx_plan_create_graded(ops, n_ops, out_subs, mode, modulus, out_charges, out_leg_dims, out_flows, 0, plan);
+}
+
+}  // extern "C"
+
+namespace {
+// Character pairs whose exchange can flip a fermionic contraction's sign
+// (contraction/contractor.py:206-285): the input characters in order, each
+// mapped to its target slot -- the output characters, then the contracted
+// characters by first appearance, a contracted character's two occurrences
+// taking consecutive half-slots -- and every inverted pair kept.
+std::vector<std::pair<char, char>> inversion_pairs(const std::vector<std::string>& in_subs, const std::string& out) {
+  std::string all;
+  for (auto& s : in_subs) all += s;
+  std::map<char, int> cnt;
+  for (char c : all) cnt[c]++;
+  std::string target = out;
+  for (char c : all)
+    if (cnt[c] >= 2 && target.find(c) == std::string::npos) target.push_back(c);
+  std::map<char, int> used;
+  std::vector<int> perm;
+  for (char c : all) {
+    const size_t pos = target.find(c);
+    if (pos == std::string::npos) throw PlanError{TNX_ERR_VALUE, std::string("free subscript '") + c +
+                                                                     "' missing from the output"};
+    perm.push_back(static_cast<int>(pos) * 2 + (cnt[c] >= 2 ? used[c] : 0));
+    used[c]++;
+  }
+  std::vector<std::pair<char, char>> pairs;
+  for (size_t i = 0; i < all.size(); ++i)
+    for (size_t j = i + 1; j < all.size(); ++j)
+      if (perm[i] > perm[j]) pairs.push_back({all[i], all[j]});
+  return pairs;
+}
+
+int parity_of(int64_t q) { return static_cast<int>(((q % 2) + 2) % 2); }
+
+// Fermionic exchange signs of a one- or two-operand plan (contractor.py:
+// 460-470), split so that every factor is exact and local: pairs of A's
+// characters (free or contracted) depend on the A block alone and negate its
+// packed copy, pairs of B's characters likewise, and pairs of one A-free and
+// one B-free character depend on the output block and negate its scatter.
+void assign_fermionic_signs(tnx_plan* p, const std::string& osubs) {
+  PairPlan& P = p->steps[0];
+  const TensorStruct& A = p->ins[0];
+  const TensorStruct& B = p->ins[1];
+  std::vector<std::string> in_subs{A.subs};
+  if (!p->has_scalar) in_subs.push_back(B.subs);
+  const auto pairs = inversion_pairs(in_subs, osubs);
+  auto in = [](const std::string& s, char c) { return s.find(c) != std::string::npos; };
+  std::vector<std::pair<char, char>> pa, pb, po;
+  for (auto& pr : pairs) {
+    if (in(A.subs, pr.first) && in(A.subs, pr.second))
+      pa.push_back(pr);
+    else if (in(B.subs, pr.first) && in(B.subs, pr.second))
+      pb.push_back(pr);
+    else
+      po.push_back(pr);
+  }
+  auto neg_of = [&](const std::vector<std::pair<char, char>>& prs, const std::string& subs, const Key& key) {
+    int odd = 0;
+    for (auto& pr : prs)
+      odd ^= parity_of(key[subs.find(pr.first)]) & parity_of(key[subs.find(pr.second)]);
+    return odd;
+  };
+  auto seg_neg = [&](std::vector<PackSeg>& segs, const TensorStruct& T, const std::vector<std::pair<char, char>>& prs) {
+    std::map<int64_t, size_t> by_off;
+    for (size_t b = 0; b < T.keys.size(); ++b) by_off[T.offs[b]] = b;
+    for (auto& sg : segs) {
+      auto it = by_off.find(sg.src_off);
+      if (it == by_off.end()) throw PlanError{TNX_ERR_RUNTIME, "internal: pack segment without its block"};
+      sg.neg = neg_of(prs, T.subs, T.keys[it->second]);
+    }
+  };
+  seg_neg(P.packA, A, pa);
+  seg_neg(P.packB, B, pb);
+  std::map<int64_t, size_t> out_by_off;
+  for (size_t b = 0; b < P.out.keys.size(); ++b) out_by_off[P.out.offs[b]] = b;
+  for (auto& sc : P.scatter) {
+    auto it = out_by_off.find(sc.dst_off);
+    if (it == out_by_off.end()) throw PlanError{TNX_ERR_RUNTIME, "internal: scatter segment without its block"};
+    sc.neg = neg_of(po, osubs, P.out.keys[it->second]);
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int tnx_plan_create_graded(const tnx_tensor_desc* ops, int32_t n_ops, const char* out_subs, int32_t mode,
+                           int32_t modulus, const int32_t* out_charges, const int64_t* out_leg_dims,
+                           const int32_t* out_flows, int32_t fermionic, tnx_plan** plan) {
   TNX_TRY({
     if (n_ops < 1) return set_err(TNX_ERR_VALUE, "contract() requires at least one tensor");
     if (!out_subs) return set_err(TNX_ERR_VALUE, "null output subscripts");
@@ -424,6 +516,11 @@ int tnx_plan_create(const tnx_tensor_desc* ops, int32_t n_ops, const char* out_s
       }
     }
     for (auto& s : p->steps) p->flops += s.flops;
+    if (fermionic) {
+      if (p->steps.size() != 1)
+        return set_err(TNX_ERR_UNSUPPORTED, "fermionic contraction of three or more operands: contract pairwise");
+      assign_fermionic_signs(p.get(), osubs);
+    }
     finalize_plan_out(p.get());
     *plan = p.release();
     return TNX_OK;
@@ -531,6 +628,7 @@ static void plan_build_device(tnx_plan* p, int precision) {
       x.ld = P.groups[sc.group].N;
       x.src_base = res_off[sc.group] + static_cast<int64_t>(sc.row0) * x.ld + sc.col0;
       x.nlegs = sc.nlegs;
+      x.neg = sc.neg;
       for (int l = 0; l < sc.nlegs; ++l) {
         x.dims[l] = sc.dims[l];
         x.rstr[l] = sc.rstr[l];
@@ -797,6 +895,7 @@ extern "C" int tnx_plan_execute_static(const tnx_plan* plan, const double* const
           x.ld = P.groups[sc.group].N;
           x.src_base = res_off[sc.group] + static_cast<int64_t>(sc.row0) * x.ld + sc.col0;
           x.nlegs = sc.nlegs;
+          x.neg = sc.neg;
           for (int l = 0; l < sc.nlegs; ++l) {
             x.dims[l] = sc.dims[l];
             x.rstr[l] = sc.rstr[l];
@@ -897,8 +996,9 @@ FusedLayout fused_layout(const HeffPlan& H, int mode, int32_t cc_req) {
   F.blocks.resize(H.pairs.size());
   for (size_t p = 0; p < H.pairs.size(); ++p) {
     const MpoPair& mp = H.pairs[p];
-    if (mp.n_in_slots > kFusedMaxSlots) {
-      F.why_not = "an MPO pair has more than " + std::to_string(kFusedMaxSlots) + " input slots";
+    if (mp.n_in_slots > kFusedMaxSlots || mp.n_out_slots > kFusedMaxOut) {
+      F.why_not = "an MPO pair has more than " + std::to_string(kFusedMaxSlots) + " input or " +
+                  std::to_string(kFusedMaxOut) + " output slots";
       return F;
     }
     for (size_t ii = 0; ii < mp.ins.size(); ++ii) {
@@ -1112,6 +1212,9 @@ int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const
     h->fl = FusedLayout{};
     if (mode != IMG_F64 && h->sched_fuse) {
       h->fl = fused_layout(H, mode, h->sched_cc);
+      for (auto& mp : H.pairs)
+        if (mp.terms.size() > static_cast<size_t>(kFusedMaxTerms))
+          h->fl.why_not = "an MPO pair has more than " + std::to_string(kFusedMaxTerms) + " W_l W_r terms";
       h->fused = h->fl.why_not.empty();
     }
     // the stage-1 A image (L) only serves the unfused path
@@ -1539,11 +1642,19 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
             FB.push_back(d);
             work += static_cast<int64_t>(fb.n_mma) * d.nKt;
           }
+          // an input slot's TMEM column (for c = 0) and its stride per c
+          std::vector<std::pair<int32_t, int32_t>> slot_col(mp.n_in_slots, {-1, 0});
+          for (const FusedBlk& fb : fl.blocks[pi])
+            for (int32_t bb = 0; bb < fb.mb; ++bb) slot_col[fb.slot0 + bb * fb.slot_stride] = {fb.col + bb, fb.mb};
           size_t u = 0;
           for (int32_t o = 0; o < mp.n_out_slots; ++o) {
             FTB.push_back(static_cast<int32_t>(FT.size()));
-            for (; u < mp.terms.size() && mp.terms[u].out_slot == o; ++u)
-              FT.push_back(DevFTerm{mp.terms[u].in_slot, static_cast<float>(mp.terms[u].w)});
+            for (; u < mp.terms.size() && mp.terms[u].out_slot == o; ++u) {
+              const auto sc = slot_col.at(mp.terms[u].in_slot);
+              if (sc.first < 0) return set_err(TNX_ERR_RUNTIME, "internal: MPO term reads an unmapped input slot");
+              FT.push_back(DevFTerm{static_cast<int16_t>(sc.first), static_cast<int16_t>(sc.second),
+                                    static_cast<float>(mp.terms[u].w)});
+            }
           }
           FTB.push_back(static_cast<int32_t>(FT.size()));
           if (u != mp.terms.size()) return set_err(TNX_ERR_RUNTIME, "internal: MPO terms not sorted by output slot");
@@ -1596,10 +1707,12 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
             fp.out0 + fp.n_out > static_cast<int64_t>(MO.size()) ||
             fp.tb0 + fp.n_out + 1 > static_cast<int64_t>(FTB.size()) || fp.cc < 1)
           return set_err(TNX_ERR_RUNTIME, "internal: fused pair table out of range");
+        if (fp.n_out > kFusedMaxOut || FTB[fp.tb0 + fp.n_out] - FTB[fp.tb0] > kFusedMaxTerms)
+          return set_err(TNX_ERR_RUNTIME, "internal: fused pair tables exceed the kernel's per-warp tables");
         for (int o = 0; o < fp.n_out; ++o)
           for (int u = FTB[fp.tb0 + o]; u < FTB[fp.tb0 + o + 1]; ++u)
-            if (FT[u].in_slot < 0 || FT[u].in_slot >= fp.n_in)
-              return set_err(TNX_ERR_RUNTIME, "internal: fused term reads outside its pair's input slots");
+            if (FT[u].col0 < 0 || FT[u].cstride < 1 || FT[u].col0 + (fp.cc - 1) * FT[u].cstride >= kFusedAccCols)
+              return set_err(TNX_ERR_RUNTIME, "internal: fused term reads outside its tile's accumulator");
         const int64_t n_dt = cdiv(fp.md, 128);
         for (int j = 0; j < fp.n_blk; ++j) {
           const DevFBlock& d = FB[fp.blk0 + j];
@@ -1830,6 +1943,268 @@ int tnx_heff_batch_error(tnx_heff_batch* b, int32_t* err) {
 // vectors
 // ---------------------------------------------------------------------------
 int64_t tnx_reduce_scratch_len(void) { return reduce_partials_count(); }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// device-side sector planning
+// ---------------------------------------------------------------------------
+namespace {
+// Distinct charges of every leg on the device, with their counts read back.
+struct DevLegs {
+  DevMem charges, leg_off, uniq, mult, n_uniq, status;
+  std::vector<int64_t> off;
+  std::vector<int32_t> nu;
+};
+
+// Gather legs' device charge arrays into one buffer and find their distinct
+// charges; throws on a range the kernel cannot histogram.
+void dev_legs(DevLegs& D, const std::vector<const int32_t*>& ch, const std::vector<int64_t>& dims, cudaStream_t st) {
+  const int n = static_cast<int>(ch.size());
+  D.off.assign(n + 1, 0);
+  for (int l = 0; l < n; ++l) D.off[l + 1] = D.off[l] + dims[l];
+  D.charges.alloc(std::max<int64_t>(1, D.off[n]) * 4);
+  for (int l = 0; l < n; ++l)
+    if (dims[l])
+      CUDA_OK(cudaMemcpyAsync(D.charges.as<int32_t>() + D.off[l], ch[l], dims[l] * 4, cudaMemcpyDeviceToDevice, st));
+  upload(D.leg_off, D.off, st);
+  D.uniq.alloc(std::max<int64_t>(1, D.off[n]) * 4);
+  D.mult.alloc(std::max<int64_t>(1, D.off[n]) * 4);
+  D.n_uniq.alloc(std::max(1, n) * 4);
+  D.status.alloc(std::max(1, n) * 4);
+  launch_unique_charges(n, D.charges.as<int32_t>(), D.leg_off.as<int64_t>(), D.uniq.as<int32_t>(),
+                        D.mult.as<int32_t>(), D.n_uniq.as<int32_t>(), D.status.as<int32_t>(), st);
+  CUDA_OK(cudaGetLastError());
+  D.nu.assign(n, 0);
+  std::vector<int32_t> stat(n, 0);
+  if (n) {
+    CUDA_OK(cudaMemcpyAsync(D.nu.data(), D.n_uniq.p, n * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(stat.data(), D.status.p, n * 4, cudaMemcpyDeviceToHost, st));
+  }
+  CUDA_OK(cudaStreamSynchronize(st));
+  for (int l = 0; l < n; ++l)
+    if (stat[l]) throw PlanError{TNX_ERR_UNSUPPORTED, "a leg's charge range exceeds 65536 (device planner)"};
+}
+
+// The reference-order valid keys of the legs in D into an owned device
+// buffer; returns the count.
+int64_t dev_valid_blocks(const DevLegs& D, const std::vector<int32_t>& flows, int32_t modulus, int64_t eff,
+                         DevMem& keys_out, cudaStream_t st) {
+  const int n = static_cast<int>(flows.size());
+  if (n == 0) {
+    keys_out.alloc(4);
+    return 1;  // the empty key
+  }
+  const int64_t kCap = int64_t(1) << 24;
+  int64_t entries = 1, max_nq = 1;
+  for (int l = 0; l < n; ++l) max_nq = std::max<int64_t>(max_nq, D.nu[l]);
+  for (int l = 0; l + 1 < n; ++l) {
+    entries *= std::max<int64_t>(1, D.nu[l]);
+    if (entries > kCap) throw PlanError{TNX_ERR_UNSUPPORTED, "too many partial keys for the device planner"};
+  }
+  entries = std::max(entries, max_nq);
+  const int64_t cap_grid = std::min<int64_t>(kCap, entries * max_nq);
+  const int64_t out_cap = std::min<int64_t>(kCap, entries * max_nq);
+  DevMem kb[2], ob[2], sb[2], cb[2], gnf, grank, goff, gfirst, cnt;
+  int32_t* kp[2];
+  int64_t* op[2];
+  int32_t* sp[2];
+  int32_t* cp[2];
+  for (int i = 0; i < 2; ++i) {
+    kb[i].alloc(entries * kMaxLegsDev * 4);
+    ob[i].alloc(entries * 8);
+    sb[i].alloc(entries * 4);
+    cb[i].alloc(entries * 4);
+    kp[i] = kb[i].as<int32_t>();
+    op[i] = ob[i].as<int64_t>();
+    sp[i] = sb[i].as<int32_t>();
+    cp[i] = cb[i].as<int32_t>();
+  }
+  gnf.alloc(cap_grid * 8);
+  grank.alloc(cap_grid * 4);
+  goff.alloc(cap_grid * 4);
+  gfirst.alloc(cap_grid * 4);
+  cnt.alloc(8);
+  keys_out.alloc(std::max<int64_t>(1, out_cap) * n * 4);
+  DevMem dfl;
+  upload(dfl, flows, st);
+  launch_valid_blocks(n, D.uniq.as<int32_t>(), D.leg_off.as<int64_t>(), D.n_uniq.as<int32_t>(), dfl.as<int32_t>(),
+                      modulus, eff, kp, op, sp, cp, gnf.as<int64_t>(), grank.as<int32_t>(), goff.as<int32_t>(),
+                      gfirst.as<int32_t>(), entries, entries, cap_grid, keys_out.as<int32_t>(), out_cap,
+                      cnt.as<int64_t>(), st);
+  CUDA_OK(cudaGetLastError());
+  int64_t count = 0;
+  CUDA_OK(cudaMemcpyAsync(&count, cnt.p, 8, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  if (count < 0) throw PlanError{TNX_ERR_UNSUPPORTED, "device planner capacity exceeded"};
+  return count;
+}
+}  // namespace
+
+extern "C" {
+
+int tnx_valid_blocks_dev(int32_t n_legs, const int32_t* charges_dev, const int64_t* leg_dims, const int32_t* flows,
+                         int32_t modulus, int32_t has_target, int64_t target, int64_t* n_keys, int32_t* keys_dev,
+                         int64_t keys_cap, void* stream) {
+  TNX_TRY({
+    if (n_legs < 0 || n_legs > kMaxLegs) return set_err(TNX_ERR_UNSUPPORTED, "at most 12 legs");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::vector<const int32_t*> ch(n_legs);
+    std::vector<int64_t> dims(leg_dims, leg_dims + n_legs);
+    int64_t off = 0;
+    for (int l = 0; l < n_legs; ++l) {
+      ch[l] = charges_dev + off;
+      off += dims[l];
+    }
+    DevLegs D;
+    dev_legs(D, ch, dims, st);
+    DevMem keys;
+    const int64_t n = dev_valid_blocks(D, std::vector<int32_t>(flows, flows + n_legs), modulus,
+                                       has_target ? target : 0, keys, st);
+    *n_keys = n;
+    if (keys_dev) {
+      if (keys_cap < n * n_legs) return set_err(TNX_ERR_VALUE, "keys_out capacity too small");
+      if (n * n_legs) CUDA_OK(cudaMemcpyAsync(keys_dev, keys.p, n * n_legs * 4, cudaMemcpyDeviceToDevice, st));
+    }
+    CUDA_OK(cudaStreamSynchronize(st));
+    return TNX_OK;
+  })
+}
+
+int tnx_contract_structure_dev(const tnx_tensor_desc* a, const tnx_tensor_desc* b, const char* out_subs,
+                               int32_t modulus, int64_t* n_out_blocks, int32_t* out_keys_dev, int64_t* out_offsets_dev,
+                               int64_t out_cap, int64_t* n_pairs, int32_t* pairs_dev, int64_t pairs_cap,
+                               void* stream) {
+  TNX_TRY({
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!a || !b || !out_subs || !a->subs || !b->subs) return set_err(TNX_ERR_VALUE, "null argument");
+    const std::string sa(a->subs), sb(b->subs), so(out_subs);
+    if (static_cast<int>(sa.size()) != a->n_legs || static_cast<int>(sb.size()) != b->n_legs)
+      return set_err(TNX_ERR_VALUE, "subscripts do not match leg counts");
+    if (static_cast<int>(so.size()) > kMaxLegs || a->n_legs > kMaxLegs || b->n_legs > kMaxLegs)
+      return set_err(TNX_ERR_UNSUPPORTED, "at most 12 legs");
+    MatchArgs m{};
+    m.la = a->n_legs;
+    m.lb = b->n_legs;
+    m.lo = static_cast<int32_t>(so.size());
+    std::string con;
+    for (char c : sa)
+      if (sb.find(c) != std::string::npos) con.push_back(c);
+    std::sort(con.begin(), con.end());
+    m.n_con = static_cast<int32_t>(con.size());
+    for (int i = 0; i < m.n_con; ++i) {
+      m.a_con[i] = static_cast<int32_t>(sa.find(con[i]));
+      m.b_con[i] = static_cast<int32_t>(sb.find(con[i]));
+    }
+    std::vector<int64_t> a_off(m.la + 1, 0), b_off(m.lb + 1, 0);
+    for (int l = 0; l < m.la; ++l) a_off[l + 1] = a_off[l] + a->leg_dims[l];
+    for (int l = 0; l < m.lb; ++l) b_off[l + 1] = b_off[l] + b->leg_dims[l];
+    std::vector<const int32_t*> och;
+    std::vector<int64_t> odims;
+    std::vector<int32_t> oflows;
+    for (int l = 0; l < m.lo; ++l) {
+      const char c = so[l];
+      const size_t pa = sa.find(c), pb = sb.find(c);
+      if (con.find(c) != std::string::npos) return set_err(TNX_ERR_VALUE, "an output subscript is contracted");
+      if (pa != std::string::npos) {
+        m.o_src[l] = static_cast<int32_t>(pa);
+        och.push_back(a->charges + a_off[pa]);
+        odims.push_back(a->leg_dims[pa]);
+        oflows.push_back(a->flows[pa]);
+      } else if (pb != std::string::npos) {
+        m.o_src[l] = m.la + static_cast<int32_t>(pb);
+        och.push_back(b->charges + b_off[pb]);
+        odims.push_back(b->leg_dims[pb]);
+        oflows.push_back(b->flows[pb]);
+      } else {
+        return set_err(TNX_ERR_VALUE, std::string("output subscript '") + c + "' is not a free index");
+      }
+    }
+    // the output target: operands whose blocks all carry one total charge
+    DevMem fa, fb, tg;
+    upload(fa, std::vector<int32_t>(a->flows, a->flows + m.la), st);
+    upload(fb, std::vector<int32_t>(b->flows, b->flows + m.lb), st);
+    tg.alloc(4 * 8);
+    launch_operand_target(a->keys, m.la, a->n_blocks, fa.as<int32_t>(), tg.as<int64_t>(), st);
+    launch_operand_target(b->keys, m.lb, b->n_blocks, fb.as<int32_t>(), tg.as<int64_t>() + 2, st);
+    CUDA_OK(cudaGetLastError());
+    int64_t t[4];
+    CUDA_OK(cudaMemcpyAsync(t, tg.p, sizeof(t), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    const int64_t total = (t[1] ? t[0] : 0) + (t[3] ? t[2] : 0);
+    // valid output keys (reference order), sorted for lookup
+    DevLegs D;
+    dev_legs(D, och, odims, st);
+    DevMem valid;
+    const int64_t nv = dev_valid_blocks(D, oflows, modulus, total, valid, st);
+    int64_t pow2 = 1;
+    while (pow2 < nv) pow2 <<= 1;
+    if (pow2 > (int64_t(1) << 16)) return set_err(TNX_ERR_UNSUPPORTED, "too many valid output keys (device planner)");
+    DevMem perm, vsorted;
+    perm.alloc(pow2 * 4);
+    vsorted.alloc(std::max<int64_t>(1, nv * m.lo) * 4);
+    if (m.lo > 0 && nv > 0) launch_sort_keys(valid.as<int32_t>(), m.lo, perm.as<int32_t>(), nv, pow2,
+                                             vsorted.as<int32_t>(), st);
+    // matching: counts per A block, their offsets, then the pairs
+    const int64_t na = a->n_blocks, nb = b->n_blocks;
+    DevMem rc, rb, pr, present;
+    rc.alloc(std::max<int64_t>(1, na) * 4);
+    launch_match(m, a->keys, na, b->keys, nb, vsorted.as<int32_t>(), nv, 0, rc.as<int32_t>(), nullptr, nullptr,
+                 nullptr, st);
+    CUDA_OK(cudaGetLastError());
+    std::vector<int32_t> counts(na);
+    if (na) CUDA_OK(cudaMemcpyAsync(counts.data(), rc.p, na * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    std::vector<int64_t> base(na + 1, 0);
+    for (int64_t i = 0; i < na; ++i) base[i + 1] = base[i] + counts[i];
+    const int64_t np = base[na];
+    upload(rb, base, st);
+    pr.alloc(std::max<int64_t>(1, np) * sizeof(int4));
+    present.alloc(std::max<int64_t>(1, nv) * 4);
+    CUDA_OK(cudaMemsetAsync(present.p, 0, present.n, st));
+    launch_match(m, a->keys, na, b->keys, nb, vsorted.as<int32_t>(), nv, 1, nullptr, rb.as<int64_t>(),
+                 pr.as<int4>(), present.as<int32_t>(), st);
+    DevMem vmap, okeys, ooffs, nout;
+    vmap.alloc(std::max<int64_t>(1, nv) * 4);
+    okeys.alloc(std::max<int64_t>(1, nv * std::max(1, static_cast<int>(m.lo))) * 4);
+    ooffs.alloc((nv + 1) * 8);
+    nout.alloc(8);
+    launch_compact_out(vsorted.as<int32_t>(), nv, m.lo, present.as<int32_t>(), D.uniq.as<int32_t>(),
+                       D.mult.as<int32_t>(), D.leg_off.as<int64_t>(), D.n_uniq.as<int32_t>(), vmap.as<int32_t>(),
+                       okeys.as<int32_t>(), ooffs.as<int64_t>(), nout.as<int64_t>(), pr.as<int4>(), np, st);
+    CUDA_OK(cudaGetLastError());
+    int64_t no = 0;
+    CUDA_OK(cudaMemcpyAsync(&no, nout.p, 8, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    *n_out_blocks = no;
+    *n_pairs = np;
+    if (out_keys_dev || out_offsets_dev) {
+      if (out_cap < no) return set_err(TNX_ERR_VALUE, "output capacity too small");
+      if (out_keys_dev && no * m.lo)
+        CUDA_OK(cudaMemcpyAsync(out_keys_dev, okeys.p, no * m.lo * 4, cudaMemcpyDeviceToDevice, st));
+      if (out_offsets_dev)
+        CUDA_OK(cudaMemcpyAsync(out_offsets_dev, ooffs.p, (no + 1) * 8, cudaMemcpyDeviceToDevice, st));
+    }
+    if (pairs_dev) {
+      if (pairs_cap < np) return set_err(TNX_ERR_VALUE, "pairs capacity too small");
+      // (A block, B block, output block) per pair
+      if (np)
+        CUDA_OK(cudaMemcpy2DAsync(pairs_dev, 3 * 4, pr.p, sizeof(int4), 3 * 4, np, cudaMemcpyDeviceToDevice, st));
+    }
+    CUDA_OK(cudaStreamSynchronize(st));
+    return TNX_OK;
+  })
+}
+
+int tnx_fused_charges_dev(const int32_t* qa_dev, int64_t da, int32_t fa, const int32_t* qb_dev, int64_t db,
+                          int32_t fb, int32_t fused_flow, int32_t modulus, int32_t* out_dev, void* stream) {
+  TNX_TRY({
+    launch_fused_charges(qa_dev, da, fa, qb_dev, db, fb, fused_flow, modulus, out_dev,
+                         static_cast<cudaStream_t>(stream));
+    CUDA_OK(cudaGetLastError());
+    return TNX_OK;
+  })
+}
 
 int tnx_dot(const double* x, const double* y, int64_t n, double* result, double* scratch, void* stream) {
   TNX_TRY({

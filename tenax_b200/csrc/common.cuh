@@ -57,7 +57,9 @@ __host__ __device__ inline int64_t img_byte_offset(int mode, int64_t tile0, int 
 constexpr int kMaxLegsDev = 12;  // equals kMaxLegs of the planner
 constexpr int kMpoKAlignDev = 8;  // equals kMpoKAlign of the planner (stage-4 d padding)
 constexpr int kFusedMaxN = 96;     // fused H_eff: largest L panel (MMA N) of one input block
-constexpr int kFusedMaxSlots = 48; // fused H_eff: input slots of one MPO pair (epilogue staging rows)
+constexpr int kFusedMaxSlots = 48; // fused H_eff: input slots of one MPO pair
+constexpr int kFusedMaxOut = 64;   // fused H_eff: output slots of one MPO pair (per-warp table rows)
+constexpr int kFusedMaxTerms = 160; // fused H_eff: W_l W_r terms of one MPO pair
 constexpr int kFusedAccCols = 256; // fused H_eff: TMEM columns of one tile's accumulator
 
 struct DevPackSeg {
@@ -90,7 +92,7 @@ struct DevScatSeg {
   int64_t dst_off;
   int64_t src_base;  // element offset of (row0, col0) in the result scratch
   int64_t ld;
-  int32_t nlegs, pad;
+  int32_t nlegs, neg;  // neg = 1: the block is written negated (a fermionic exchange sign)
   int32_t dims[kMaxLegsDev];
   int32_t rstr[kMaxLegsDev];
   int32_t cstr[kMaxLegsDev];
@@ -168,8 +170,8 @@ struct DevFBlock {
   int32_t mb, slot0, slot_stride;    // b extent; staging slot of (b = 0) and its stride per b
   int32_t pad;
 };
-struct DevFTerm {
-  int32_t in_slot;
+struct DevFTerm {  // y[o] += w * X1[d, col0 + c_local * cstride] (TMEM column of the input slot)
+  int16_t col0, cstride;
   float w;
 };
 struct DevFTile {

@@ -12,9 +12,10 @@
 // accumulating D[d, (c, b)] into its own TMEM column range.  TMEM lane = d for
 // every block, so after the MMAs one thread holds, for its d, every input
 // slot (b, p, q) of every c of the tile: the W_l W_r application is
-// thread-local.  Each epilogue warp stages one c's inputs in shared memory
-// (slot-major, lane-contiguous), sums each output slot's terms, and
-// transposes groups of 8 outputs across 8 lanes with XOR shuffles so that
+// thread-local.  Each epilogue warp keeps the current pair's output slots
+// and terms in its own shared-memory table, sums each output slot's terms
+// straight from TMEM (one column load per term), and transposes groups of 8
+// outputs across 8 lanes with XOR shuffles so that
 // every lane ends with 8 consecutive d of one output: one aligned 16-byte
 // chunk of a stage-4 image row (hi and lo images for BF16x3).
 //
@@ -42,7 +43,12 @@ constexpr int F_STAGE_BYTES_BF16 = 2 * F_A_BYTES + 2 * F_B_BYTES;
 constexpr int F_STAGE_BYTES_TF32 = F_A_BYTES + F_B_BYTES;
 constexpr int F_STAGES_BF16 = 3;
 constexpr int F_STAGES_TF32 = 6;
-constexpr int F_XS_BYTES = F_EPI_WARPS * kFusedMaxSlots * 32 * 4;  // per-warp input staging
+// per-warp copy of the current MPO pair's output slots, term offsets and terms
+constexpr int F_TAB_SO = kFusedMaxOut * static_cast<int>(sizeof(DevMpoOutSlot));
+constexpr int F_TAB_TB = (kFusedMaxOut + 1) * 4;
+constexpr int F_TAB_TM = kFusedMaxTerms * static_cast<int>(sizeof(DevFTerm));
+constexpr int F_TAB_BYTES = (F_TAB_SO + F_TAB_TB + F_TAB_TM + 15) / 16 * 16;
+constexpr int F_XS_BYTES = F_EPI_WARPS * F_TAB_BYTES;
 static_assert(F_A_BYTES % 1024 == 0 && F_B_BYTES % 1024 == 0, "SW128 operand tiles must start on 1024 bytes");
 
 // 8x8 transpose among the 8 lanes of each aligned lane group: on entry lane
@@ -92,7 +98,7 @@ __global__ void __launch_bounds__(F_THREADS, 1)
   uint64_t* drain = tempty + 2;
   uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
-  uint32_t* xs_all = reinterpret_cast<uint32_t*>(smem + STAGES * STAGE_BYTES + 256);
+  uint8_t* tab_all = smem + STAGES * STAGE_BYTES + 256;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -246,12 +252,30 @@ __global__ void __launch_bounds__(F_THREADS, 1)
     const int q = warp & 3;   // TMEM lane quarter this warp may access
     const int e = warp - 2;   // epilogue warp 0..7
     const int half = e >> 2;  // c values of this parity
-    uint32_t* xs = xs_all + e * kFusedMaxSlots * 32;
+    // this warp's copy of the current pair's tables (reloaded when the pair changes)
+    uint8_t* tab = tab_all + e * F_TAB_BYTES;
+    DevMpoOutSlot* wso = reinterpret_cast<DevMpoOutSlot*>(tab);
+    int32_t* wtb = reinterpret_cast<int32_t*>(tab + F_TAB_SO);
+    DevFTerm* wtm = reinterpret_cast<DevFTerm*>(tab + F_TAB_SO + F_TAB_TB);
+    int cached_pair = -1;
     int acc = 0;
     uint32_t aph = 0;
     for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
       const DevFTile tl = tiles[t];
       const DevFPair pr = pairs[tl.pair];
+      if (tl.pair != cached_pair) {
+        __syncwarp();
+        const uint32_t* so_src = reinterpret_cast<const uint32_t*>(oslots + pr.out0);
+        uint32_t* so_dst = reinterpret_cast<uint32_t*>(wso);
+        constexpr int kSoWords = static_cast<int>(sizeof(DevMpoOutSlot) / 4);
+        for (int i = lane; i < pr.n_out * kSoWords; i += 32) so_dst[i] = so_src[i];
+        const int t0 = term_begin[pr.tb0];
+        for (int i = lane; i <= pr.n_out; i += 32) wtb[i] = term_begin[pr.tb0 + i] - t0;
+        const int nterm = term_begin[pr.tb0 + pr.n_out] - t0;
+        for (int i = lane; i < nterm; i += 32) wtm[i] = terms[t0 + i];
+        __syncwarp();
+        cached_pair = tl.pair;
+      }
       // all lanes wait (the tcgen05.ld below is warp-collective)
       if (!wait_or_abort(&tfull[acc], aph, abort_flag, err_flag)) break;
       tc_fence_after();
@@ -261,46 +285,46 @@ __global__ void __launch_bounds__(F_THREADS, 1)
       for (int cl = half; cl < pr.cc; cl += 2) {
         const int64_t c = static_cast<int64_t>(tl.ct) * pr.cc + cl;
         if (c >= pr.mc) break;
-        // this c's input slots: TMEM column col + cl*mb + b of each block -> xs[slot][lane]
-        for (int j = 0; j < pr.n_blk; ++j) {
-          const DevFBlock bk = blocks[pr.blk0 + j];
-          const uint32_t col = tbase + static_cast<uint32_t>(bk.col + cl * bk.mb);
-          for (int r0 = 0; r0 < bk.mb; r0 += 8) {
-            uint32_t v[8];
-#pragma unroll
-            for (int r = 0; r < 8; ++r)
-              if (r0 + r < bk.mb) v[r] = tmem_ld1(col + r0 + r);
-            tmem_wait_ld();
-#pragma unroll
-            for (int r = 0; r < 8; ++r)
-              if (r0 + r < bk.mb) xs[(bk.slot0 + (r0 + r) * bk.slot_stride) * 32 + lane] = v[r];
-          }
-        }
-        __syncwarp();
-        // output slots in groups of 8: sum the terms, transpose, store 16-byte chunks
+        // output slots in groups of 8: every output's first two terms are
+        // loaded from TMEM together (one wait), further terms after
         for (int og = 0; og < pr.n_out; og += 8) {
           float y[8];
+          uint32_t v[8][2];
+          int tb[8], nt[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const int o = og + i;
+            tb[i] = o < pr.n_out ? wtb[o] : 0;
+            nt[i] = o < pr.n_out ? wtb[o + 1] - tb[i] : 0;
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+              if (k < nt[i]) {
+                const DevFTerm tm = wtm[tb[i] + k];
+                v[i][k] = tmem_ld1(tbase + static_cast<uint32_t>(tm.col0 + cl * tm.cstride));
+              }
+          }
+          tmem_wait_ld();
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
             y[i] = 0.0f;
-            const int o = og + i;
-            if (o < pr.n_out) {
-              const int tb = term_begin[pr.tb0 + o], te = term_begin[pr.tb0 + o + 1];
-              for (int u = tb; u < te; ++u) {
-                const DevFTerm tm = terms[u];
-                y[i] = fmaf(tm.w, __uint_as_float(xs[tm.in_slot * 32 + lane]), y[i]);
-              }
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+              if (k < nt[i]) y[i] = fmaf(wtm[tb[i] + k].w, __uint_as_float(v[i][k]), y[i]);
+            for (int k = 2; k < nt[i]; ++k) {
+              const DevFTerm tm = wtm[tb[i] + k];
+              const uint32_t x = tmem_ld1(tbase + static_cast<uint32_t>(tm.col0 + cl * tm.cstride));
+              tmem_wait_ld();
+              y[i] = fmaf(tm.w, __uint_as_float(x), y[i]);
             }
           }
           transpose8(y, lane);
           const int o = og + (lane & 7);
           if (o < pr.n_out && d_chunk < pr.md) {
-            const DevMpoOutSlot so = oslots[pr.out0 + o];
+            const DevMpoOutSlot so = wso[o];
             img_store_chunk<MODE>(reinterpret_cast<uint8_t*>(so.img_addr), so.lo_off, so.nKt,
                                   so.row0 + c * so.rows_per_c + so.row_add, so.k0 + so.k_add + d_chunk, y);
           }
         }
-        __syncwarp();
       }
       tc_fence_before();
       mbar_arrive(&tempty[acc]);

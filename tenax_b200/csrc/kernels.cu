@@ -82,7 +82,8 @@ __global__ void scatter_kernel(const TS* __restrict__ res, double* __restrict__ 
       row += idx * s.rstr[l];
       col += idx * s.cstr[l];
     }
-    out[s.dst_off + e] = static_cast<double>(res[s.src_base + row * s.ld + col]);
+    const double v = static_cast<double>(res[s.src_base + row * s.ld + col]);
+    out[s.dst_off + e] = s.neg ? -v : v;
   }
 }
 

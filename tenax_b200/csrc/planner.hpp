@@ -74,6 +74,7 @@ struct PackSeg {
   int32_t rstr[kMaxLegs];
   int32_t kstr[kMaxLegs];   // K strides of the contracted legs (unpadded: element order)
   int32_t kdstr[kMaxLegs];  // K strides in the operand image (the innermost may be padded)
+  int32_t neg = 0;          // fermionic exchange sign of this block: 1 packs the negated block
 };
 
 // Copy one output block out of a group's result matrix (M x N, row-major).
@@ -86,6 +87,7 @@ struct ScatSeg {
   int32_t dims[kMaxLegs];
   int32_t rstr[kMaxLegs];
   int32_t cstr[kMaxLegs];
+  int32_t neg = 0;  // fermionic exchange sign of this output block: 1 negates it
 };
 
 struct GroupShape {

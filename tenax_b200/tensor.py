@@ -247,10 +247,18 @@ class SymmetricTensor:
         return self._like(self._data, tuple(i.flip_flow() for i in self._indices))
 
     def dagger(self) -> "SymmetricTensor":
+        """Conjugate with dual legs (core/tensor.py:795-820); blocks of a
+        fermionic tensor take the twist phase, (-1) to the total parity of
+        their charges."""
         sym = self._indices[0].symmetry if self._indices else None
         new_idx = tuple(i.dual() for i in self._indices)
         new_keys = [tuple(int(sym.dual(np.int64(q))) for q in k) for k in self._keys]
-        blocks = {nk: self.blocks[k] for nk, k in zip(new_keys, self._keys)}
+        blocks = {}
+        for nk, k in zip(new_keys, self._keys):
+            b = self.blocks[k]
+            if sym is not None and sym.is_fermionic and int(np.sum(sym.parity(np.asarray(k)))) % 2:
+                b = -b
+            blocks[nk] = b
         return SymmetricTensor(blocks, new_idx, _validate=False)
 
     def transpose(self, axes) -> "SymmetricTensor":

@@ -3,7 +3,7 @@
 Run in the development container only (it needs the read-only reference
 checkout; nothing at test or bench time reads it):
 
-    python tests/golden/make_golden.py --ref /root/reference/src
+    python tests/golden/make_golden.py --ref <reference checkout>/src
 
 The reference modules are loaded by file path under the NumPy stand-in for
 jax (``_jax_standin.py``); their outputs -- plus the inputs that produced
@@ -623,9 +623,78 @@ def gen_ctm(M):
         json.dump(meta, fh, indent=1)
 
 
+def make_fermion_tensor(M, sym, legs, rng):
+    """A reference SymmetricTensor over a fermionic symmetry with N(0,1)
+    blocks on its valid-block set (sorted-key order)."""
+    core = M["tenax.core.tensor"]
+    idx = M["tenax.core.index"]
+    indices = tuple(
+        idx.TensorIndex(sym, np.asarray(c, np.int32), idx.FlowDirection(f), label=lab) for c, f, lab in legs
+    )
+    blocks = {}
+    for k in sorted(core._compute_valid_blocks(indices)):
+        _, shp = core._block_slices(indices, k)
+        if all(s > 0 for s in shp):
+            blocks[k] = rng.standard_normal(shp)
+    return core.SymmetricTensor(blocks, indices)
+
+
+def gen_fermion(M):
+    """Fermionic symmetries (FermionParity, FermionicU1): label contractions
+    whose leg reordering exchanges odd charges (contractor.py:206-285,
+    :460-470), transposes with the Koszul sign (core/tensor.py:32-50,
+    :836-862) and daggers with the twist phase (core/tensor.py:795-820)."""
+    contractor = M["tenax.contraction.contractor"]
+    symm = M["tenax.core.symmetry"]
+    rng = np.random.default_rng(29)
+    arrays, cases = {}, []
+    syms = {"fermion_parity": (symm.FermionParity(), 2), "fermionic_u1": (symm.FermionicU1(), None)}
+    for sname, (sym, mod) in syms.items():
+        if mod == 2:
+            a = [0, 1, 1, 0, 1]
+            b = [1, 0, 0, 1]
+            p = [0, 1]
+        else:
+            a = [-1, 0, 0, 1, 2, 1]
+            b = [0, 1, -1, 1]
+            p = [0, 1]
+        A = make_fermion_tensor(M, sym, [(a, 1, "i"), (p, 1, "s"), (b, -1, "k"), (p, -1, "t")], rng)
+        B = make_fermion_tensor(M, sym, [(b, 1, "k"), (p, 1, "u"), (a, -1, "j")], rng)
+        C = make_fermion_tensor(M, sym, [(p, 1, "t"), (b, -1, "m"), (a, 1, "j")], rng)
+        for name, ts, ol in (
+            ("pair", [A, B], None),
+            ("pair_perm", [A, B], ["j", "u", "t", "s", "i"]),
+            ("pair_rev", [B, A], None),
+            ("two_legs", [A, C], None),
+            ("two_legs_perm", [A, C], ["m", "s", "j", "k", "i"]),
+        ):
+            res = contractor.contract(*ts, output_labels=ol)
+            subs, _ = contractor._labels_to_subscripts(ts, ol)
+            cname = f"{sname}.{name}"
+            for i, t in enumerate(ts):
+                arrays.update(dump_tensor(f"{cname}.in{i}", t, mod))
+            arrays.update(dump_tensor(f"{cname}.out", res, mod))
+            cases.append({"name": cname, "kind": "contract", "symmetry": sname, "modulus": mod,
+                          "subscripts": subs, "output_labels": ol, "n_in": len(ts), "n_out_blocks": len(res.blocks)})
+        for axes in ((1, 0, 3, 2), (3, 2, 1, 0), (2, 0, 3, 1)):
+            res = A.transpose(axes)
+            cname = f"{sname}.transpose_{''.join(map(str, axes))}"
+            arrays.update(dump_tensor(f"{cname}.in0", A, mod))
+            arrays.update(dump_tensor(f"{cname}.out", res, mod))
+            cases.append({"name": cname, "kind": "transpose", "symmetry": sname, "modulus": mod, "axes": list(axes)})
+        res = A.dagger()
+        cname = f"{sname}.dagger"
+        arrays.update(dump_tensor(f"{cname}.in0", A, mod))
+        arrays.update(dump_tensor(f"{cname}.out", res, mod))
+        cases.append({"name": cname, "kind": "dagger", "symmetry": sname, "modulus": mod})
+    np.savez_compressed(os.path.join(HERE, "fermion.npz"), **arrays)
+    with open(os.path.join(HERE, "fermion.json"), "w") as f:
+        json.dump(cases, f, indent=1)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference/src")
+    ap.add_argument("--ref", required=True, help="the reference checkout's src directory")
     ap.add_argument("--only", default="")
     args = ap.parse_args()
     mods = _jax_standin.load_reference(args.ref, [
@@ -636,7 +705,7 @@ def main():
     ])
     mods["cfg"] = mods["tenax.algorithms.dmrg"].DMRGConfig
     todo = args.only.split(",") if args.only else ["valid", "contract", "pieces", "mpo", "c1", "ctm", "fuse", "split",
-                                                       "ctm_tensor", "netfile"]
+                                                       "ctm_tensor", "netfile", "fermion"]
     if "valid" in todo:
         gen_valid_blocks(mods)
     if "contract" in todo:
@@ -657,6 +726,8 @@ def main():
         gen_ctm_tensor(mods)
     if "netfile" in todo:
         gen_netfile(mods)
+    if "fermion" in todo:
+        gen_fermion(mods)
 
 
 if __name__ == "__main__":

@@ -91,3 +91,21 @@ def test_reference_arm_never_loads_the_library():
     )
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and "OK" in r.stdout, r.stderr[-2000:]
+
+
+def test_sector_histogram_key():
+    """The autotuner's cache key: power-of-two buckets of the bond sector
+    sizes of theta's outer legs, and the MPO bond dimension."""
+    import types
+
+    import numpy as np
+
+    from tenax_b200.autotune import sector_histogram
+
+    def leg(counts):
+        return types.SimpleNamespace(charges=np.repeat(np.arange(len(counts)), counts))
+
+    p = types.SimpleNamespace(theta=types.SimpleNamespace(indices=(leg([4, 200, 5]), None, None, leg([1, 64]))),
+                              Wl=types.SimpleNamespace(indices=(types.SimpleNamespace(charges=np.zeros(26)),)))
+    hist, dws = sector_histogram([p])
+    assert dict(hist) == {2: 1, 8: 1, 3: 1, 0: 1, 6: 1} and dws == (26,)

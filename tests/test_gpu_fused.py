@@ -124,3 +124,22 @@ def test_mixed_schedules_cannot_share_a_batch():
     a, b = _op(p, "bf16x3", FUSED), _op(p, "bf16x3", UNFUSED)
     with pytest.raises(ValueError):
         tb.HeffBatch([a, b])
+
+
+def test_autotune_picks_a_candidate_and_caches(tmp_path):
+    """The tuner times every candidate schedule on the problems, returns the
+    fastest, and a second call with the same sector profile reads it from
+    the cache without timing."""
+    from tenax_b200 import autotune
+
+    Wl, Wr = W.cylinder_bulk_w()
+    gen = np.random.default_rng(14)
+    probs = [W.make_heff_problem(c, c, Wl, Wr, gen, n_sectors=10, hi=48) for c in (120, 200)]
+    cands = autotune.candidates(probs, "bf16x3")
+    assert UNFUSED in cands and cands[0]["fuse_mpo"] == 1
+    path = str(tmp_path / "tune.json")
+    best, timings = autotune.tune(probs, "bf16x3", cache_path=path, reps=2)
+    assert best in cands and len(timings) == len(cands)
+    assert all(np.isfinite(v) and v > 0 for v in timings.values())
+    again, t2 = autotune.tune(probs, "bf16x3", cache_path=path)
+    assert again == best and t2 == {}
