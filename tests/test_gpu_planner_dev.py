@@ -75,13 +75,16 @@ def _bench_mod():
 @pytest.mark.parametrize("chi", [256, 512, 1024, 2048])
 def test_valid_blocks_benchmark_structures(chi):
     args, _ = _bench_mod().HostProblems(2).make(chi, fill=False)
-    for t in (args[0], args[1], args[4]):  # L, theta, R
+    for name, t in (("L", args[0]), ("theta", args[1]), ("R", args[4])):
         ch = [l.charges for l in t.legs]
         fl = [l.flow for l in t.legs]
         got = _valid_dev(ch, fl, None, None)
         host = [tuple(k) for k in _capi.valid_blocks(ch, fl, None, None)]
-        assert got == host
-        assert set(t.blocks) <= set(got)
+        assert got == host, name
+        # theta conserves charge; the environments carry the MPO's charge
+        # transfer, so only theta's blocks are a subset of the target-0 keys
+        if name == "theta":
+            assert set(t.blocks) <= set(got)
 
 
 def _structure_dev(a, b, subs_a, subs_b, out_subs, modulus):
