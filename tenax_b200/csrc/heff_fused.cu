@@ -282,34 +282,47 @@ __global__ void __launch_bounds__(F_THREADS, 1)
       const uint32_t tbase =
           tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * F_ACC_COLS);
       const int d_chunk = tl.dt * 128 + q * 32 + (lane >> 3) * 8;  // first d of this lane's output chunk
-      for (int cl = half; cl < pr.cc; cl += 2) {
-        const int64_t c = static_cast<int64_t>(tl.ct) * pr.cc + cl;
-        if (c >= pr.mc) break;
-        // output slots in groups of 8: every output's first two terms are
-        // loaded from TMEM together (one wait), further terms after
-        for (int og = 0; og < pr.n_out; og += 8) {
+      // a lane quarter whose d rows all lie past the sector has nothing to write
+      const bool live = tl.dt * 128 + q * 32 < pr.md;
+      for (int og = 0; live && og < pr.n_out; og += 8) {
+        // this group's table entries (every output's first two terms), read
+        // once and applied to each of this warp's c values
+        int nt[8], tb[8], col[8][2], cs[8][2];
+        float w[8][2];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int o = og + i;
+          tb[i] = o < pr.n_out ? wtb[o] : 0;
+          nt[i] = o < pr.n_out ? wtb[o + 1] - tb[i] : 0;
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            const DevFTerm tm = k < nt[i] ? wtm[tb[i] + k] : DevFTerm{0, 0, 0.0f};
+            col[i][k] = tm.col0;
+            cs[i][k] = tm.cstride;
+            w[i][k] = tm.w;
+          }
+        }
+        const int o_mine = og + (lane & 7);
+        const bool store = o_mine < pr.n_out && d_chunk < pr.md;
+        DevMpoOutSlot so{};
+        if (store) so = wso[o_mine];
+        for (int cl = half; cl < pr.cc; cl += 2) {
+          const int64_t c = static_cast<int64_t>(tl.ct) * pr.cc + cl;
+          if (c >= pr.mc) break;
           float y[8];
           uint32_t v[8][2];
-          int tb[8], nt[8];
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            const int o = og + i;
-            tb[i] = o < pr.n_out ? wtb[o] : 0;
-            nt[i] = o < pr.n_out ? wtb[o + 1] - tb[i] : 0;
+          for (int i = 0; i < 8; ++i)
 #pragma unroll
             for (int k = 0; k < 2; ++k)
-              if (k < nt[i]) {
-                const DevFTerm tm = wtm[tb[i] + k];
-                v[i][k] = tmem_ld1(tbase + static_cast<uint32_t>(tm.col0 + cl * tm.cstride));
-              }
-          }
+              if (k < nt[i]) v[i][k] = tmem_ld1(tbase + static_cast<uint32_t>(col[i][k] + cl * cs[i][k]));
           tmem_wait_ld();
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
             y[i] = 0.0f;
 #pragma unroll
             for (int k = 0; k < 2; ++k)
-              if (k < nt[i]) y[i] = fmaf(wtm[tb[i] + k].w, __uint_as_float(v[i][k]), y[i]);
+              if (k < nt[i]) y[i] = fmaf(w[i][k], __uint_as_float(v[i][k]), y[i]);
             for (int k = 2; k < nt[i]; ++k) {
               const DevFTerm tm = wtm[tb[i] + k];
               const uint32_t x = tmem_ld1(tbase + static_cast<uint32_t>(tm.col0 + cl * tm.cstride));
@@ -318,12 +331,9 @@ __global__ void __launch_bounds__(F_THREADS, 1)
             }
           }
           transpose8(y, lane);
-          const int o = og + (lane & 7);
-          if (o < pr.n_out && d_chunk < pr.md) {
-            const DevMpoOutSlot so = wso[o];
+          if (store)
             img_store_chunk<MODE>(reinterpret_cast<uint8_t*>(so.img_addr), so.lo_off, so.nKt,
                                   so.row0 + c * so.rows_per_c + so.row_add, so.k0 + so.k_add + d_chunk, y);
-          }
         }
       }
       tc_fence_before();
