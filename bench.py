@@ -259,8 +259,8 @@ def run_ours(args):
     # schedule of the mixed stages 1-3: tuned on these problems (autotune.py)
     # unless given on the command line
     tuning = None
-    if args.unfused or args.c_per_tile or args.no_tune:
-        schedule = {"fuse_mpo": 0 if args.unfused else 1, "c_per_tile": args.c_per_tile}
+    if args.unfused or args.routed or args.c_per_tile or args.no_tune:
+        schedule = {"fuse_mpo": 0 if args.unfused else (2 if args.routed else 1), "c_per_tile": args.c_per_tile}
     else:
         from tenax_b200 import autotune
 
@@ -279,14 +279,22 @@ def run_ours(args):
     peaks, peak_src = _peaks()
     # dominant GEMM stage of the mixed step
     st_ms = rmx["stage_ms"]
-    fused = bool(rmx["schedule"]["fuse_mpo"])
+    fused = rmx["schedule"]["fuse_mpo"] == 1
+    routed = rmx["schedule"]["fuse_mpo"] == 2
     # the fused kernel does stage 1 and the MPO; its tensor work is stage 1's
     gemm = {1: rmx["stage_flops"][0] + (rmx["stage_flops"][1] if fused else 0.0), 3: rmx["stage_flops"][2]}
     dom = max((1, 3), key=lambda s: st_ms[s])
-    stage_names = (["pack theta panels", "fused stages 1-3 (L.theta in TMEM, W_l W_r epilogue)",
-                    "none (MPO inside the fused kernel)", "stage-4 GEMM .R"] if fused else
-                   ["pack theta", "stage-1 GEMM L.theta", "fused MPO (W_l W_r)", "stage-4 GEMM .R"])
+    if fused:
+        stage_names = ["pack theta panels", "fused stages 1-3 (L.theta in TMEM, W_l W_r epilogue)",
+                       "none (MPO inside the fused kernel)", "stage-4 GEMM .R"]
+    elif routed:
+        stage_names = ["pack theta panels", "stage-1 GEMM L.theta, epilogue routes single-term W_l W_r outputs "
+                       "into the stage-4 operand", "MPO kernel: multi-term outputs from the kept X1 slots",
+                       "stage-4 GEMM .R"]
+    else:
+        stage_names = ["pack theta", "stage-1 GEMM L.theta", "fused MPO (W_l W_r)", "stage-4 GEMM .R"]
     dom_name = ("fused stages 1-3 (tcgen05 + W_l W_r epilogue)" if fused and dom == 1
+                else "stage-1 tcgen05 grouped GEMM, routed epilogue" if routed and dom == 1
                 else f"{STAGE_GEMM[dom]} tcgen05 grouped GEMM")
     split = 3.0 if args.precision == "bf16x3" else 1.0
     peak = peaks["bf16_tflops"] / split if args.precision == "bf16x3" else peaks["bf16_tflops"] / 2.0
@@ -294,7 +302,8 @@ def run_ours(args):
     traffic = None
     tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tp):
-        key = f"{args.precision}_fused1" if fused and dom == 1 else f"{args.precision}_stage{dom}"
+        key = (f"{args.precision}_fused1" if fused and dom == 1 else f"{args.precision}_routed1" if routed and dom == 1
+               else f"{args.precision}_stage{dom}")
         traffic = json.load(open(tp)).get(key)
     if rank == 0:
         out = {
@@ -1038,6 +1047,8 @@ def main():
     ap.add_argument("--no-graph", action="store_true", help="time eager applies instead of CUDA-graph replays")
     ap.add_argument("--unfused", action="store_true",
                     help="mixed stages 1-3 as stage-1 GEMM + X1 in HBM + MPO kernel instead of the fused kernel")
+    ap.add_argument("--routed", action="store_true",
+                    help="mixed stages 1-3 with the routed stage-1 epilogue, without tuning")
     ap.add_argument("--c-per-tile", type=int, default=0, help="fused kernel: c values per tile (0 = largest that fits)")
     ap.add_argument("--no-tune", action="store_true", help="fused schedule without tuning it")
     ap.add_argument("--mode", default="partition", choices=["partition", "replicas"],

@@ -3,10 +3,13 @@ histogram.
 
 The reference evaluates H_eff one block combination at a time and has no
 schedule to tune.  Here the mixed-precision stages 1-3 can run as one fused
-tcgen05 kernel (tile c extent ``c_per_tile``) or as three kernels with X1 in
-HBM, and which is faster depends on the sector sizes: the fused kernel's MMA
-rows are one d sector padded to 128, its columns ``c_per_tile`` c values per
-MPO input block.  The tuner times each candidate schedule on the actual
+tcgen05 kernel (tile c extent ``c_per_tile``), as a stage-1 GEMM whose
+epilogue routes the single-term W_l W_r outputs straight into the stage-4
+operand (routed), or as three kernels with X1 in HBM, and which is faster
+depends on the sector sizes and the MPO: the fused kernel's MMA rows are one
+d sector padded to 128, its columns ``c_per_tile`` c values per MPO input
+block; the routed epilogue writes each X1 row once per single-term output
+that reads it.  The tuner times each candidate schedule on the actual
 problems, keeps the fastest, and caches it under a key made of the device
 name, the precision and a histogram of the bond sector sizes (power-of-two
 buckets) with the MPO bond dimension, so later batches with the same sector
@@ -43,15 +46,24 @@ def sector_histogram(problems) -> tuple:
     return tuple(sorted(hist.items())), tuple(sorted(dws))
 
 
+# the schedules a tuned entry chose among: entries tuned over another set are re-tuned
+SCHEDULE_SET = ("fused", "routed", "unfused")
+
+
+def schedule_label(s: dict) -> str:
+    return {1: f"fused c={s['c_per_tile']}", 2: "routed"}.get(s["fuse_mpo"], "unfused")
+
+
 def cache_key(problems, precision: str) -> str:
     name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
     hist, dws = sector_histogram(problems)
-    return json.dumps({"device": name, "precision": precision, "dw": dws, "sectors": hist}, sort_keys=True)
+    return json.dumps({"device": name, "precision": precision, "dw": dws, "sectors": hist,
+                       "schedules": list(SCHEDULE_SET)}, sort_keys=True)
 
 
 def candidates(problems, precision: str) -> list:
     """The fused kernel at the largest c extent that fits, at half of it and
-    at 1, and the three-kernel path."""
+    at 1, the routed stage-1 epilogue, and the three-kernel path."""
     p = problems[0]
     probe = HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, precision,
                          schedule={"fuse_mpo": 1, "c_per_tile": 0})
@@ -60,6 +72,7 @@ def candidates(problems, precision: str) -> list:
     if cc:
         for c in sorted({cc, max(1, cc // 2), 1}, reverse=True):
             out.append({"fuse_mpo": 1, "c_per_tile": c})
+    out.append({"fuse_mpo": 2, "c_per_tile": 0})
     out.append({"fuse_mpo": 0, "c_per_tile": 0})
     return out
 
@@ -107,7 +120,7 @@ def tune(problems, precision: str, cache_path: str | None = DEFAULT_CACHE, reps:
     best, best_ms = None, float("inf")
     for s in candidates(problems, precision):
         ms = time_schedule(problems, precision, s, reps=reps)
-        label = f"fused c={s['c_per_tile']}" if s["fuse_mpo"] else "unfused"
+        label = schedule_label(s)
         timings[label] = round(ms, 4)
         if ms < best_ms:
             best, best_ms = s, ms

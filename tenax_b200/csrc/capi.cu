@@ -979,56 +979,56 @@ struct FusedLayout {
 
 int32_t round16(int64_t x) { return static_cast<int32_t>((x + 15) / 16 * 16); }
 
-FusedLayout fused_layout(const HeffPlan& H, int mode, int32_t cc_req) {
-  FusedLayout F;
-  const int tk = img_geom(mode).tk;
+// Every X1 block of every MPO pair as (L block, theta block, p, q): the
+// stage-1 product L[a, b, c] theta[a, p, q, d] over a that fills the input
+// slots (b, p, q) of the pair (q_c, q_d).  Returns why the structure has no
+// such decomposition (empty: it has).
+std::string pair_blocks(const HeffPlan& H, std::vector<std::vector<FusedBlk>>& blocks) {
   std::map<std::pair<int32_t, int32_t>, int> l_by_bc;  // (q_b, q_c) -> L block
   for (size_t i = 0; i < H.L.keys.size(); ++i) {
     auto key = std::make_pair(H.L.keys[i][1], H.L.keys[i][2]);
-    if (l_by_bc.count(key)) {
-      F.why_not = "an L block is not determined by its (q_b, q_c)";
-      return F;
-    }
+    if (l_by_bc.count(key)) return "an L block is not determined by its (q_b, q_c)";
     l_by_bc[key] = static_cast<int>(i);
   }
   std::map<Key, int> th_by_key;
   for (size_t i = 0; i < H.th.keys.size(); ++i) th_by_key[H.th.keys[i]] = static_cast<int>(i);
-  F.blocks.resize(H.pairs.size());
+  blocks.assign(H.pairs.size(), {});
   for (size_t p = 0; p < H.pairs.size(); ++p) {
     const MpoPair& mp = H.pairs[p];
+    for (size_t ii = 0; ii < mp.ins.size(); ++ii) {
+      const MpoIn& in = mp.ins[ii];
+      const Key& ik = H.mpo_in_keys[p][ii];  // (q_b, q_p, q_q)
+      auto lit = l_by_bc.find({ik[0], mp.qc});
+      if (lit == l_by_bc.end()) return "internal: no L block for an X1 block";
+      const int lb = lit->second;
+      const int32_t qa = H.L.keys[lb][0];
+      auto tit = th_by_key.find(Key{qa, ik[1], ik[2], mp.qd});
+      if (tit == th_by_key.end()) return "internal: no theta block for an X1 block";
+      const int tb = tit->second;
+      const auto& ld = H.L.dims[lb];
+      const auto& td = H.th.dims[tb];
+      if (ld[0] != td[0] || ld[1] != in.mb || ld[2] != mp.mc || td[1] != in.mp || td[2] != in.mq || td[3] != mp.md)
+        return "internal: inconsistent block dims";
+      for (int pp = 0; pp < in.mp; ++pp)
+        for (int qq = 0; qq < in.mq; ++qq)
+          blocks[p].push_back(FusedBlk{tb, pp, qq, lb, in.mb, static_cast<int32_t>(ld[0]), 0, 0,
+                                       mp.in_slot0[ii] + pp * in.mq + qq, in.mp * in.mq});
+    }
+  }
+  return "";
+}
+
+FusedLayout fused_layout(const HeffPlan& H, int mode, int32_t cc_req) {
+  FusedLayout F;
+  const int tk = img_geom(mode).tk;
+  for (const MpoPair& mp : H.pairs)
     if (mp.n_in_slots > kFusedMaxSlots || mp.n_out_slots > kFusedMaxOut) {
       F.why_not = "an MPO pair has more than " + std::to_string(kFusedMaxSlots) + " input or " +
                   std::to_string(kFusedMaxOut) + " output slots";
       return F;
     }
-    for (size_t ii = 0; ii < mp.ins.size(); ++ii) {
-      const MpoIn& in = mp.ins[ii];
-      const Key& ik = H.mpo_in_keys[p][ii];  // (q_b, q_p, q_q)
-      auto lit = l_by_bc.find({ik[0], mp.qc});
-      if (lit == l_by_bc.end()) {
-        F.why_not = "internal: no L block for an X1 block";
-        return F;
-      }
-      const int lb = lit->second;
-      const int32_t qa = H.L.keys[lb][0];
-      auto tit = th_by_key.find(Key{qa, ik[1], ik[2], mp.qd});
-      if (tit == th_by_key.end()) {
-        F.why_not = "internal: no theta block for an X1 block";
-        return F;
-      }
-      const int tb = tit->second;
-      const auto& ld = H.L.dims[lb];
-      const auto& td = H.th.dims[tb];
-      if (ld[0] != td[0] || ld[1] != in.mb || ld[2] != mp.mc || td[1] != in.mp || td[2] != in.mq || td[3] != mp.md) {
-        F.why_not = "internal: inconsistent block dims";
-        return F;
-      }
-      for (int pp = 0; pp < in.mp; ++pp)
-        for (int qq = 0; qq < in.mq; ++qq)
-          F.blocks[p].push_back(FusedBlk{tb, pp, qq, lb, in.mb, static_cast<int32_t>(ld[0]), 0, 0,
-                                         mp.in_slot0[ii] + pp * in.mq + qq, in.mp * in.mq});
-    }
-  }
+  F.why_not = pair_blocks(H, F.blocks);
+  if (!F.why_not.empty()) return F;
   // c values per tile: the largest that fits every pair's blocks side by side
   // in one accumulator, each block's panel within the kernel's operand stage
   int64_t max_mc = 1;
@@ -1084,6 +1084,62 @@ FusedLayout fused_layout(const HeffPlan& H, int mode, int32_t cc_req) {
   }
   return F;
 }
+
+// Routed stages 1-3 (mixed precisions): one stage-1 GEMM group per X1 block
+// (rows (b, c) of its L block, columns d of its theta slice), whose epilogue
+// writes every output slot with a single W_l W_r term straight into the
+// stage-4 image and keeps X1 (FP32) only for the input slots that multi-term
+// output slots read; the MPO kernel then forms just those outputs.
+struct RoutedLayout {
+  std::vector<std::vector<FusedBlk>> blocks;  // per MPO pair: its X1 blocks
+  std::vector<int64_t> lb_tile0;              // per L block: first 16 KB tile of its image (-1: unused)
+  std::vector<int32_t> lb_nKt;
+  int64_t lb_tiles = 0;
+  std::map<std::array<int32_t, 3>, int64_t> thp_tile0;  // (theta block, p, q) -> first tile
+  int64_t thp_tiles = 0;
+  std::vector<std::vector<int32_t>> out_terms;  // per pair and output slot: number of terms
+  std::vector<std::vector<char>> in_kept;       // per pair and input slot: read by a multi-term output
+  std::string why_not;
+};
+
+RoutedLayout routed_layout(const HeffPlan& H, int mode) {
+  RoutedLayout F;
+  const int tk = img_geom(mode).tk;
+  F.why_not = pair_blocks(H, F.blocks);
+  if (!F.why_not.empty()) return F;
+  F.lb_tile0.assign(H.L.keys.size(), -1);
+  F.lb_nKt.assign(H.L.keys.size(), 0);
+  for (auto& bl : F.blocks)
+    for (auto& b : bl) {
+      const auto& ld = H.L.dims[b.l_blk];
+      if (ld[1] * ld[2] > (int64_t{1} << 30)) {
+        F.why_not = "an L block has more than 2^30 rows (b, c)";
+        return F;
+      }
+      if (F.lb_tile0[b.l_blk] < 0) {
+        F.lb_nKt[b.l_blk] = static_cast<int32_t>(cdiv(ld[0], tk));
+        F.lb_tile0[b.l_blk] = F.lb_tiles;
+        F.lb_tiles += cdiv(ld[1] * ld[2], 128) * F.lb_nKt[b.l_blk];
+      }
+      const std::array<int32_t, 3> tkey{b.th_blk, b.pp, b.qq};
+      if (!F.thp_tile0.count(tkey)) {
+        const auto& td = H.th.dims[b.th_blk];
+        F.thp_tile0[tkey] = F.thp_tiles;
+        F.thp_tiles += cdiv(td[3], 128) * cdiv(td[0], tk);
+      }
+    }
+  F.out_terms.resize(H.pairs.size());
+  F.in_kept.resize(H.pairs.size());
+  for (size_t p = 0; p < H.pairs.size(); ++p) {
+    const MpoPair& mp = H.pairs[p];
+    F.out_terms[p].assign(mp.n_out_slots, 0);
+    F.in_kept[p].assign(mp.n_in_slots, 0);
+    for (const MpoTerm& t : mp.terms) ++F.out_terms[p][t.out_slot];
+    for (const MpoTerm& t : mp.terms)
+      if (F.out_terms[p][t.out_slot] > 1) F.in_kept[p][t.in_slot] = 1;
+  }
+  return F;
+}
 }  // namespace
 
 extern "C" {
@@ -1109,6 +1165,11 @@ struct tnx_heff {
   bool fused = false;
   FusedLayout fl;
   DevMem lp_img;
+  // routed stages 1-3 (mixed precisions): layout and the per-L-block image
+  bool routed = false;
+  RoutedLayout rl;
+  DevMem lb_img;
+  int64_t lb_lo = 0;
 };
 
 int tnx_heff_create(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, const tnx_tensor_desc* Wl,
@@ -1138,7 +1199,8 @@ int tnx_heff_create_for(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, 
 int tnx_heff_set_schedule(tnx_heff* h, const tnx_heff_schedule* sched) {
   if (!h || !sched) return set_err(TNX_ERR_VALUE, "null argument");
   if (sched->c_per_tile < 0 || sched->c_per_tile > 32) return set_err(TNX_ERR_VALUE, "c_per_tile must be in [0, 32]");
-  h->sched_fuse = sched->fuse_mpo ? 1 : 0;
+  if (sched->fuse_mpo < 0 || sched->fuse_mpo > 2) return set_err(TNX_ERR_VALUE, "fuse_mpo must be 0, 1 or 2");
+  h->sched_fuse = sched->fuse_mpo;
   h->sched_cc = sched->c_per_tile;
   return TNX_OK;
 }
@@ -1149,18 +1211,22 @@ int tnx_heff_get_schedule(const tnx_heff* h, tnx_heff_schedule* sched) {
     if (h->prec < 0) {
       // before tnx_heff_set_operators: the schedule the planned precision would get
       const int mode = img_mode_of(h->plan_prec);
-      bool fz = false;
+      bool fz = false, rt = false;
       int32_t cc = 0;
-      if (mode != IMG_F64 && h->sched_fuse && h->H.closed && h->H.s4_separable) {
+      if (mode != IMG_F64 && h->sched_fuse == 1 && h->H.closed && h->H.s4_separable) {
         const FusedLayout fl = fused_layout(h->H, mode, h->sched_cc);
         fz = fl.why_not.empty();
         cc = fl.cc;
       }
-      sched->fuse_mpo = fz ? 1 : 0;
+      if (mode != IMG_F64 && h->sched_fuse == 2 && h->H.closed && h->H.s4_separable) {
+        std::vector<std::vector<FusedBlk>> blocks;
+        rt = pair_blocks(h->H, blocks).empty();
+      }
+      sched->fuse_mpo = fz ? 1 : (rt ? 2 : 0);
       sched->c_per_tile = fz ? cc : 0;
       return TNX_OK;
     }
-    sched->fuse_mpo = h->fused ? 1 : 0;
+    sched->fuse_mpo = h->fused ? 1 : (h->routed ? 2 : 0);
     sched->c_per_tile = h->fused ? h->fl.cc : 0;
     return TNX_OK;
   })
@@ -1217,8 +1283,15 @@ int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const
           h->fl.why_not = "an MPO pair has more than " + std::to_string(kFusedMaxTerms) + " W_l W_r terms";
       h->fused = h->fl.why_not.empty();
     }
+    h->routed = false;
+    h->rl = RoutedLayout{};
+    if (mode != IMG_F64 && h->sched_fuse == 2) {
+      h->rl = routed_layout(H, mode);
+      h->routed = h->rl.why_not.empty();
+    }
     // the stage-1 A image (L) only serves the unfused path
-    h->l_img.alloc(h->fused ? 0 : std::max<int64_t>(1, h->g1.a_tiles) * ig.tile_bytes * split);
+    const bool plain = !h->fused && !h->routed;
+    h->l_img.alloc(plain ? std::max<int64_t>(1, h->g1.a_tiles) * ig.tile_bytes * split : 0);
     h->r_img.alloc(std::max<int64_t>(1, h->g4.b_tiles) * ig.tile_bytes * split);
     h->l_lo = h->g1.a_tiles * ig.tile_bytes;
     h->r_lo = h->g4.b_tiles * ig.tile_bytes;
@@ -1274,9 +1347,40 @@ int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const
     }
     std::vector<DevPackSeg> pl, pr;
     std::vector<DevChunk> cl, cr;
-    if (!h->fused)
+    if (plain)
       build_pack(H.s1.packA, h->g1, true, reinterpret_cast<uint64_t>(h->l_img.p), h->l_lo, ig.tile_bytes, 0, pl, cl,
                  1.0 / sL);
+    if (h->routed) {
+      // one image per L block: rows (b, c) with c fastest, K = a (the same
+      // values as the unfused image, split from FP64)
+      h->lb_img.alloc(std::max<int64_t>(1, h->rl.lb_tiles) * ig.tile_bytes * split);
+      h->lb_lo = h->rl.lb_tiles * ig.tile_bytes;
+      CUDA_OK(cudaMemsetAsync(h->lb_img.p, 0, h->lb_img.n, st));
+      for (size_t lb = 0; lb < H.L.keys.size(); ++lb) {
+        if (h->rl.lb_tile0[lb] < 0) continue;
+        const auto& ld = H.L.dims[lb];
+        DevPackSeg d{};
+        d.src_off = H.L.offs[lb];
+        d.img_addr = reinterpret_cast<uint64_t>(h->lb_img.p) + static_cast<uint64_t>(h->rl.lb_tile0[lb]) * ig.tile_bytes;
+        d.lo_off = h->lb_lo;
+        d.nKt = h->rl.lb_nKt[lb];
+        d.nlegs = 3;
+        d.src_slot = 0;
+        d.kcount = static_cast<int32_t>(ld[0]);
+        d.scale = 1.0 / sL;
+        for (int l = 0; l < 3; ++l) d.dims[l] = static_cast<int32_t>(ld[l]);
+        d.rstr[1] = static_cast<int32_t>(ld[2]);
+        d.rstr[2] = 1;
+        d.kstr[0] = 1;
+        d.kdstr[0] = 1;
+        const int seg_id = static_cast<int>(pl.size());
+        pl.push_back(d);
+        const int64_t count = ld[0] * ld[1] * ld[2];
+        for (int64_t e0 = 0; e0 < count; e0 += 2048) cl.push_back({seg_id, 0, e0, std::min<int64_t>(2048, count - e0)});
+      }
+    } else {
+      h->lb_img.alloc(0);
+    }
     build_pack(H.s4.packB, h->g4, false, reinterpret_cast<uint64_t>(h->r_img.p), h->r_lo, ig.tile_bytes, 1, pr, cr,
                1.0 / sR);
     DevMem dpl, dcl, dpr, dcr, tab;
@@ -1328,6 +1432,10 @@ struct tnx_heff_batch {
   int n_thp_row_chunks = 0;
   DevMem f_pairs, f_blocks, f_tb, f_terms, f_tiles;
   int n_f_tiles = 0;
+  // routed stages 1-3: the stage-1 epilogue's destinations (per row class b:
+  // a range of routes) and X1 of the input slots multi-term outputs read
+  bool routed = false;
+  DevMem routes, route_rng;
   const int32_t* skip = nullptr;
   int n_launches = 0;
   std::vector<uint64_t> last_src, last_out;
@@ -1368,16 +1476,18 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     const bool f32 = mode != IMG_F64;
     for (int i = 0; i < n; ++i) {
       if (hs[i]->prec != precision) return set_err(TNX_ERR_VALUE, "operators were packed for another precision");
-      if (hs[i]->fused != hs[0]->fused)
-        return set_err(TNX_ERR_VALUE, "operators of one batch must all run fused stages 1-3 or all unfused");
+      if (hs[i]->fused != hs[0]->fused || hs[i]->routed != hs[0]->routed)
+        return set_err(TNX_ERR_VALUE, "operators of one batch must all run the same schedule of stages 1-3");
       b->hs.push_back(hs[i]);
     }
     b->fused = hs[0]->fused;
+    b->routed = hs[0]->routed;
     for (int i = 0; i < n; ++i) {
       b->th_off.push_back(b->th_total);
       b->th_total += hs[i]->H.th.total;
     }
     // sizes: theta images (stage-1 B), X1 results, X3 images (stage-4 A)
+    const bool fz = b->fused, rt = b->routed;
     int64_t th_tiles = 0, x3_tiles = 0, x1_elems = 0;
     std::vector<int64_t> th_t0(n), x3_t0(n), x1_0(n);
     for (int i = 0; i < n; ++i) {
@@ -1387,11 +1497,20 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
       x1_0[i] = x1_elems;
       th_tiles += hs[i]->g1.b_tiles;
       x3_tiles += hs[i]->g4.a_tiles;
-      for (auto& g : H.s1.groups) x1_elems += g.M * x1_ld(g.N);
+      if (rt) {
+        // X1 of the kept input slots only: (c, d) with d padded to kMpoKAlign
+        for (size_t pi = 0; pi < H.pairs.size(); ++pi) {
+          const int64_t md_pad = (H.pairs[pi].md + kMpoKAlign - 1) / kMpoKAlign * kMpoKAlign;
+          for (char k : hs[i]->rl.in_kept[pi])
+            if (k) x1_elems += H.pairs[pi].mc * md_pad;
+        }
+      } else {
+        for (auto& g : H.s1.groups) x1_elems += g.M * x1_ld(g.N);
+      }
     }
-    // the unfused path's stage-1 B image and X1 result; the fused path's theta panels
-    const bool fz = b->fused;
-    b->th_img.alloc(fz ? 16 : std::max<int64_t>(1, th_tiles) * ig.tile_bytes * split);
+    // the unfused path's stage-1 B image and X1 result; the fused and routed
+    // paths' theta panels (and the routed path's kept X1 slots)
+    b->th_img.alloc(fz || rt ? 16 : std::max<int64_t>(1, th_tiles) * ig.tile_bytes * split);
     b->x3_img.alloc(std::max<int64_t>(1, x3_tiles) * ig.tile_bytes * split);
     b->th_lo = th_tiles * ig.tile_bytes;
     b->x3_lo = x3_tiles * ig.tile_bytes;
@@ -1400,10 +1519,10 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     CUDA_OK(cudaMemset(b->x3_img.p, 0, b->x3_img.n));
     std::vector<int64_t> thp_t0(n, 0);
     int64_t thp_tiles = 0;
-    if (fz) {
+    if (fz || rt) {
       for (int i = 0; i < n; ++i) {
         thp_t0[i] = thp_tiles;
-        thp_tiles += hs[i]->fl.thp_tiles;
+        thp_tiles += fz ? hs[i]->fl.thp_tiles : hs[i]->rl.thp_tiles;
       }
       b->thp_img.alloc(std::max<int64_t>(1, thp_tiles) * ig.tile_bytes * split);
       CUDA_OK(cudaMemset(b->thp_img.p, 0, b->thp_img.n));
@@ -1435,6 +1554,8 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     std::vector<DevMpoTerm> MT;
     std::vector<int2> MC;
     std::vector<DevChunk> ZC;
+    std::vector<DevRoute> RT;
+    std::vector<int2> RB;
     for (int i = 0; i < n; ++i) {
       tnx_heff* h = hs[i];
       const HeffPlan& H = h->H;
@@ -1473,10 +1594,10 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         for (int r0 = 0; r0 < rs.rows; r0 += 256)
           for (int kc = 0; kc < nkc; kc += cpt) trc.push_back(make_int4(id, r0, kc, 0));
       }
-      if (fz) {
+      if (fz || rt) {
         // theta panels: each referenced (theta block, p, q) slice as rows d, K = a
         const int tk = ig.tk;
-        for (const auto& kv : h->fl.thp_tile0) {
+        for (const auto& kv : fz ? h->fl.thp_tile0 : h->rl.thp_tile0) {
           const int tb = kv.first[0], pp = kv.first[1], qq = kv.first[2];
           const auto& td = H.th.dims[tb];
           DevRowPackSeg rs{};
@@ -1498,10 +1619,10 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
             for (int kc = 0; kc < nkc; kc += cpt) fthc.push_back(make_int4(id, r0, kc, 0));
         }
       }
-      // stage-1 groups
+      // stage-1 groups (the routed path builds its own with the MPO tables)
       std::vector<int64_t> x1_goff;
       int64_t xo = x1_0[i];
-      for (size_t g = 0; g < H.s1.groups.size(); ++g) {
+      for (size_t g = 0; g < H.s1.groups.size() && !rt; ++g) {
         x1_goff.push_back(xo);
         DevGroup x{};
         x.a_addr = reinterpret_cast<uint64_t>(h->l_img.p) + static_cast<uint64_t>(h->g1.a_tile0[g]) * ig.tile_bytes;
@@ -1522,8 +1643,10 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         G1.push_back(x);
       }
       std::vector<std::pair<int64_t, DevTile>> tl;
-      build_tiles(H.s1, h->g1, static_cast<int>(G1.size() - H.s1.groups.size()), tl);
-      T1.insert(T1.end(), tl.begin(), tl.end());
+      if (!rt) {
+        build_tiles(H.s1, h->g1, static_cast<int>(G1.size() - H.s1.groups.size()), tl);
+        T1.insert(T1.end(), tl.begin(), tl.end());
+      }
       // stage-4 groups
       PairGeom gx3 = h->g4;
       for (auto& t : gx3.a_tile0) t += x3_t0[i];
@@ -1550,9 +1673,14 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
       for (auto& zr : H.zero_ranges)
         for (int64_t st = 0; st < zr.second; st += 4096)
           ZC.push_back({1 + i, 0, zr.first + st, std::min<int64_t>(4096, zr.second - st)});
-      // MPO tables
+      // MPO tables (routed: the multi-term output slots only, reading the kept X1 slots)
+      int64_t x1k = x1_0[i];
       for (size_t pi = 0; pi < H.pairs.size(); ++pi) {
         const MpoPair& mp = H.pairs[pi];
+        const int32_t md_pad = (mp.md + kMpoKAlign - 1) / kMpoKAlign * kMpoKAlign;
+        std::vector<MpoTerm> terms;
+        for (const MpoTerm& t : mp.terms)
+          if (!rt || h->rl.out_terms[pi][t.out_slot] > 1) terms.push_back(t);
         DevMpoPair dp{};
         dp.mc = mp.mc;
         dp.md = mp.md;
@@ -1561,15 +1689,28 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         dp.out0 = static_cast<int32_t>(MO.size());
         dp.n_out = mp.n_out_slots;
         dp.term0 = static_cast<int32_t>(MT.size());
-        dp.n_terms = static_cast<int32_t>(mp.terms.size());
+        dp.n_terms = static_cast<int32_t>(terms.size());
         dp.n_in_slots = mp.n_in_slots;
         dp.n_out_slots = mp.n_out_slots;
-        b->mpo_smem = std::max<size_t>(b->mpo_smem, mp.terms.size() * sizeof(DevMpoTerm) +
+        b->mpo_smem = std::max<size_t>(b->mpo_smem, terms.size() * sizeof(DevMpoTerm) +
                                                        mp.n_in_slots * sizeof(DevMpoSlot) +
                                                        mp.n_out_slots * sizeof(DevMpoOutSlot));
         // X1 columns of one (p,q) slot: its d range padded to H.x1_align
         const int64_t md_x1 = (mp.md + H.x1_align - 1) / H.x1_align * H.x1_align;
-        for (size_t k = 0; k < mp.ins.size(); ++k) {
+        for (int32_t sl = 0; sl < mp.n_in_slots && rt; ++sl) {
+          // kept slots: X1 rows (c, d), d padded to kMpoKAlign; the others are never read
+          DevMpoSlot r{};
+          r.base = x1_base;
+          r.ld = md_pad;
+          if (h->rl.in_kept[pi][sl]) {
+            r.base = x1_base + static_cast<uint64_t>(x1k) * 4;
+            x1k += static_cast<int64_t>(mp.mc) * md_pad;
+            if (x1k * 4 > static_cast<int64_t>(b->x1.n))
+              return set_err(TNX_ERR_RUNTIME, "internal: kept X1 slots outside their buffer");
+          }
+          MI.push_back(r);
+        }
+        for (size_t k = 0; k < mp.ins.size() && !rt; ++k) {
           // one record per input slot (b,p,q): address of its point (c=0, d=0)
           const MpoIn& in = mp.ins[k];
           const int64_t ld = x1_ld(H.s1.groups[in.g1].N);
@@ -1589,9 +1730,9 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
               }
         }
         // stage-4 K places each f block's d range at a multiple of kMpoKAlign
-        const int32_t md_pad = (mp.md + kMpoKAlign - 1) / kMpoKAlign * kMpoKAlign;
         for (size_t k = 0; k < mp.outs.size(); ++k) {
           const MpoOut& o = mp.outs[k];
+          const int64_t img_rows = cdiv(H.s4.groups[o.g4].M, 128) * 128;
           for (int s = 0; s < o.ms; ++s)
             for (int t = 0; t < o.mt; ++t)
               for (int f = 0; f < o.mf; ++f) {
@@ -1604,12 +1745,72 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
                 os.rows_per_c = o.ms * o.mt;
                 os.row_add = s * o.mt + t;
                 os.k_add = f * md_pad;
+                // every (c, d) of the slot lands inside its group's image
+                if (os.row0 + os.row_add + static_cast<int64_t>(mp.mc - 1) * os.rows_per_c >= img_rows ||
+                    os.k0 + os.k_add + md_pad > static_cast<int64_t>(os.nKt) * ig.tk)
+                  return set_err(TNX_ERR_RUNTIME, "internal: an X3 slot lies outside its stage-4 image");
                 MO.push_back(os);
               }
         }
-        for (auto& t : mp.terms) MT.push_back({t.out_slot, t.in_slot, t.w});
+        for (auto& t : terms) MT.push_back({t.out_slot, t.in_slot, t.w});
         const int pair_id = static_cast<int>(MP.size());
         MP.push_back(dp);
+        if (rt) {
+          // one stage-1 group per X1 block; a row class b routes to the
+          // single-term output slots of its input slot and, when a
+          // multi-term output reads that slot, to its kept X1 rows
+          std::vector<std::vector<std::pair<int32_t, double>>> singles(mp.n_in_slots);
+          for (const MpoTerm& t : mp.terms)
+            if (h->rl.out_terms[pi][t.out_slot] == 1) singles[t.in_slot].push_back({t.out_slot, t.w});
+          for (const FusedBlk& fb : h->rl.blocks[pi]) {
+            DevGroup x{};
+            x.a_addr = reinterpret_cast<uint64_t>(h->lb_img.p) +
+                       static_cast<uint64_t>(h->rl.lb_tile0[fb.l_blk]) * ig.tile_bytes;
+            x.b_addr = thp_base + static_cast<uint64_t>(thp_t0[i] + h->rl.thp_tile0.at({fb.th_blk, fb.pp, fb.qq})) *
+                                      ig.tile_bytes;
+            x.a_lo = h->lb_lo;
+            x.b_lo = thp_lo;
+            x.M = fb.mb * mp.mc;
+            x.N = mp.md;
+            x.nKt = h->rl.lb_nKt[fb.l_blk];
+            x.kk_last = kk_last_of(fb.ma, b->mode);
+            x.scale = 1.0;
+            x.routed = 1;
+            x.route0 = static_cast<int32_t>(RB.size());
+            x.mc = mp.mc;
+            x.md = mp.md;
+            for (int32_t bb = 0; bb < fb.mb; ++bb) {
+              const int32_t sl = fb.slot0 + bb * fb.slot_stride;
+              const int32_t r0 = static_cast<int32_t>(RT.size());
+              for (const auto& ow : singles.at(sl)) {
+                const DevMpoOutSlot& os = MO[dp.out0 + ow.first];
+                DevRoute r{};
+                r.addr = os.img_addr;
+                r.lo_off = os.lo_off;
+                r.nKt = os.nKt;
+                r.row0 = os.row0 + os.row_add;
+                r.rstride = os.rows_per_c;
+                r.k0 = os.k0 + os.k_add;
+                r.w = static_cast<float>(ow.second);
+                r.kind = 0;
+                RT.push_back(r);
+              }
+              if (h->rl.in_kept[pi][sl]) {
+                DevRoute r{};
+                r.addr = MI[dp.in0 + sl].base;
+                r.rstride = md_pad;
+                r.w = 1.0f;
+                r.kind = 1;
+                RT.push_back(r);
+              }
+              RB.push_back(make_int2(r0, static_cast<int32_t>(RT.size()) - r0));
+            }
+            const int gid = static_cast<int>(G1.size());
+            G1.push_back(x);
+            for (int mt = 0; mt < cdiv(x.M, 128); ++mt)
+              for (int nt = 0; nt < cdiv(x.N, 128); ++nt) T1.push_back({x.nKt, DevTile{gid, mt, nt, 0}});
+          }
+        }
         if (fz) {
           // fused tables of this pair: its MMA blocks, its terms by output slot, its tiles
           const FusedLayout& fl = h->fl;
@@ -1667,7 +1868,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         const int ppc = mpo_points_per_cta();
         const int dpt = mpo_d_per_thread(b->mode);
         const int npts = mp.mc * ((mp.md + dpt - 1) / dpt);
-        for (int p0 = 0; p0 < npts; p0 += ppc) MC.push_back(make_int2(pair_id, p0));
+        for (int p0 = 0; p0 < npts && dp.n_terms > 0; p0 += ppc) MC.push_back(make_int2(pair_id, p0));
       }
     }
     if (b->mpo_smem > 200 * 1024)
@@ -1735,9 +1936,6 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
             return set_err(TNX_ERR_RUNTIME, "internal: L panels outside their image");
         }
       }
-      upload(b->thp_rows, fth);
-      upload(b->thp_row_chunks, fthc);
-      b->n_thp_row_chunks = static_cast<int>(fthc.size());
       upload(b->f_pairs, FP);
       upload(b->f_blocks, FB);
       upload(b->f_tb, FTB);
@@ -1748,6 +1946,41 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
       for (auto& x : FTL) ftl.push_back(x.second);
       upload(b->f_tiles, ftl);
       b->n_f_tiles = static_cast<int>(ftl.size());
+    }
+    if (fz || rt) {
+      upload(b->thp_rows, fth);
+      upload(b->thp_row_chunks, fthc);
+      b->n_thp_row_chunks = static_cast<int>(fthc.size());
+    }
+    if (rt) {
+      // every route stays inside the X3 image or the kept X1 slots
+      const uint64_t x3_end = x3_base + static_cast<uint64_t>(x3_tiles) * ig.tile_bytes;
+      const uint64_t x1_end = x1_base + static_cast<uint64_t>(b->x1.n);
+      for (const DevGroup& g : G1) {
+        if (!g.routed || g.mc < 1 || g.M % g.mc || g.route0 < 0 || g.route0 + g.M / g.mc > static_cast<int64_t>(RB.size()))
+          return set_err(TNX_ERR_RUNTIME, "internal: routed group tables out of range");
+        const int32_t md_pad = (g.md + kMpoKAlign - 1) / kMpoKAlign * kMpoKAlign;
+        for (int bb = 0; bb < g.M / g.mc; ++bb) {
+          const int2 rr = RB[g.route0 + bb];
+          if (rr.x < 0 || rr.y < 0 || rr.x + rr.y > static_cast<int64_t>(RT.size()))
+            return set_err(TNX_ERR_RUNTIME, "internal: route range out of range");
+          for (int r = rr.x; r < rr.x + rr.y; ++r) {
+            const DevRoute& R = RT[r];
+            const int64_t last = static_cast<int64_t>(g.mc - 1) * R.rstride;
+            if (R.kind == 0) {
+              const uint64_t end = R.addr + static_cast<uint64_t>(cdiv(R.row0 + last + 1, 128) * R.nKt) * ig.tile_bytes;
+              if (R.addr < x3_base || end > x3_end || R.lo_off != b->x3_lo || R.k0 + md_pad > R.nKt * ig.tk)
+                return set_err(TNX_ERR_RUNTIME, "internal: a route writes outside the X3 image");
+            } else {
+              const uint64_t end = R.addr + static_cast<uint64_t>(last + md_pad) * 4;
+              if (R.addr < x1_base || end > x1_end || R.addr % 32 || R.rstride % kMpoKAlign)
+                return set_err(TNX_ERR_RUNTIME, "internal: a route writes outside the kept X1 slots");
+            }
+          }
+        }
+      }
+      upload(b->routes, RT);
+      upload(b->route_rng, RB);
     }
     b->n_mpo_chunks = static_cast<int>(MC.size());
     b->err.alloc(sizeof(int32_t));
@@ -1792,6 +2025,11 @@ static void heff_batch_stage(tnx_heff_batch* b, int stage, cudaStream_t st, cons
                         b->n_f_tiles, b->err.as<int32_t>(), b->skip, st);
     return;
   }
+  if (b->routed && stage == 0) {
+    launch_pack_rows(src_tab, b->thp_rows.as<DevRowPackSeg>(), b->thp_row_chunks.as<int4>(), b->n_thp_row_chunks,
+                     b->mode, b->skip, st);
+    return;
+  }
   switch (stage) {
     case 0:
       if (b->th_by_rows)
@@ -1807,7 +2045,8 @@ static void heff_batch_stage(tnx_heff_batch* b, int stage, cudaStream_t st, cons
                         b->out_tab1.as<uint64_t>(), b->skip, st);
       else
         launch_gemm_tc(b->mode, b->g1.as<DevGroup>(), b->t1.as<DevTile>(), b->n_t1, b->ro1.as<int64_t>(),
-                       b->out_tab1.as<uint64_t>(), false, b->err.as<int32_t>(), b->skip, st);
+                       b->out_tab1.as<uint64_t>(), false, b->err.as<int32_t>(), b->skip, st,
+                       b->routed ? b->routes.as<DevRoute>() : nullptr, b->routed ? b->route_rng.as<int2>() : nullptr);
       break;
     case 2:
       launch_mpo_apply(f32, b->mode, b->mpo_pairs.as<DevMpoPair>(), b->mpo_slots.as<DevMpoSlot>(),

@@ -124,6 +124,22 @@ struct DevGroup {
   int32_t vec_ld;           // > 0: every row offset is a multiple of 4 elements and the first
                             // vec_ld (a multiple of 4, >= N) columns may be written: 16-byte stores
   int32_t kk_last;          // tcgen05: MMA K steps (of the 4 per slab) the last K slab needs; 0 = all 4
+  // routed epilogue (tcgen05 H_eff stage 1): rows are (b, c) with c fastest,
+  // columns are d; row (b, c) goes through routes[route_rng[route0 + b]]
+  // instead of the row-offset table.  routed = 0: plain rows.
+  int32_t routed, route0, mc, md;
+};
+
+// One destination of a routed stage-1 row (b, c): kind 0 writes w * row into
+// the stage-4 operand image at image row row0 + c * rstride, K k0 + d (8 d per
+// aligned chunk, the image's own precision split); kind 1 writes w * row in
+// FP32 at addr + (c * rstride + d) * 4.
+struct DevRoute {
+  uint64_t addr;     // kind 0: image tile 0; kind 1: element (c = 0, d = 0)
+  int64_t lo_off;    // kind 0: byte offset of the low-part image
+  int32_t nKt, row0, rstride, k0;
+  float w;
+  int32_t kind;
 };
 
 struct DevTile {

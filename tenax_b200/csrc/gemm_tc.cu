@@ -78,7 +78,8 @@ template <bool TF32, typename OutT>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_tc_kernel(const DevGroup* __restrict__ groups, const DevTile* __restrict__ tiles, int n_tiles,
                    const int64_t* __restrict__ rowoff, const uint64_t* __restrict__ out_tab, int32_t* err_flag,
-                   const int32_t* __restrict__ skip) {
+                   const int32_t* __restrict__ skip, const DevRoute* __restrict__ routes,
+                   const int2* __restrict__ route_rng) {
   constexpr int NT = TF32 ? 2 : 4;          // operand tiles per stage
   constexpr int STAGES = TF32 ? 6 : 3;      // 192 KB of operand ring either way
   constexpr int KSUB = 4;                   // MMAs per 128-byte K slab (32 B each)
@@ -261,6 +262,60 @@ __global__ void __launch_bounds__(THREADS, 1)
       it.prefetch();
       const DevTile tl = it.tl;
       const DevGroup g = it.g;
+      if constexpr (sizeof(OutT) == 4) {
+        if (g.routed) {
+          // routed rows (b, c): each row's d values go to the destinations
+          // of its b, scaled by their weights, 8 d per aligned chunk; the
+          // route range does not depend on the accumulator
+          const int row = tl.mt * TBM + r_in_tile;
+          int cc = 0;
+          int2 rr = make_int2(0, 0);
+          if (row < g.M) {
+            const int bb = row / g.mc;
+            cc = row - bb * g.mc;
+            rr = route_rng[g.route0 + bb];
+          }
+          if (!wait_or_abort(&tfull[acc], aph, abort_flag, err_flag)) break;
+          tc_fence_after();
+          const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * TBN);
+          const int d_tile = tl.nt * TBN;
+#pragma unroll 1
+          for (int c0 = c_begin; c0 < c_begin + kColsPerWarp; c0 += 32) {
+            if (d_tile + c0 >= g.md) break;  // warp-uniform: no valid d left
+            uint32_t v[32];
+            tmem_ld32(tbase + c0, v);
+#pragma unroll 1
+            for (int r = rr.x; r < rr.x + rr.y; ++r) {
+              const DevRoute R = routes[r];
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const int d0 = d_tile + c0 + 8 * u;
+                if (d0 >= g.md) break;
+                float x[kMpoVec];
+#pragma unroll
+                for (int e = 0; e < kMpoVec; ++e) x[e] = __uint_as_float(v[8 * u + e]) * R.w;
+                if (R.kind == 0) {
+                  img_store_chunk<TF32 ? IMG_TF32 : IMG_BF16, float>(
+                      reinterpret_cast<uint8_t*>(R.addr), R.lo_off, R.nKt,
+                      static_cast<int64_t>(R.row0) + static_cast<int64_t>(cc) * R.rstride, R.k0 + d0, x);
+                } else {
+                  float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(R.addr) +
+                                                          static_cast<int64_t>(cc) * R.rstride + d0);
+                  dst[0] = make_float4(x[0], x[1], x[2], x[3]);
+                  dst[1] = make_float4(x[4], x[5], x[6], x[7]);
+                }
+              }
+            }
+          }
+          tc_fence_before();
+          mbar_arrive(&tempty[acc]);
+          if (++acc == NACC) {
+            acc = 0;
+            aph ^= 1u;
+          }
+          continue;
+        }
+      }
       // the row offset does not depend on the accumulator: request it before waiting
       const int row = tl.mt * TBM + r_in_tile;
       const int64_t ro = row < g.M ? rowoff[g.rowoff0 + row] : -1;
@@ -350,7 +405,8 @@ __global__ void __launch_bounds__(THREADS, 1)
 
 template <bool TF32, typename OutT>
 void launch_tc_impl(const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
-                    const uint64_t* out_tab, int32_t* err_flag, const int32_t* skip, cudaStream_t st) {
+                    const uint64_t* out_tab, int32_t* err_flag, const int32_t* skip, cudaStream_t st,
+                    const DevRoute* routes, const int2* route_rng) {
   constexpr int NT = TF32 ? 2 : 4;
   constexpr int STAGES = TF32 ? 6 : 3;
   const int smem = STAGES * NT * TILE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + kEpiStageBytes;
@@ -360,23 +416,24 @@ void launch_tc_impl(const DevGroup* groups, const DevTile* tiles, int n_tiles, c
   int grid = device_sm_count();
   if (grid > n_tiles) grid = n_tiles;
   gemm_tc_kernel<TF32, OutT>
-      <<<grid, THREADS, smem, st>>>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip);
+      <<<grid, THREADS, smem, st>>>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, routes, route_rng);
 }
 }  // namespace
 
 void launch_gemm_tc(int mode, const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
-                    const uint64_t* out_tab, bool out_f64, int32_t* err_flag, const int32_t* skip, cudaStream_t st) {
+                    const uint64_t* out_tab, bool out_f64, int32_t* err_flag, const int32_t* skip, cudaStream_t st,
+                    const DevRoute* routes, const int2* route_rng) {
   if (n_tiles <= 0) return;
   if (mode == IMG_TF32) {
     if (out_f64)
-      launch_tc_impl<true, double>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st);
+      launch_tc_impl<true, double>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, routes, route_rng);
     else
-      launch_tc_impl<true, float>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st);
+      launch_tc_impl<true, float>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, routes, route_rng);
   } else {
     if (out_f64)
-      launch_tc_impl<false, double>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st);
+      launch_tc_impl<false, double>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, routes, route_rng);
     else
-      launch_tc_impl<false, float>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st);
+      launch_tc_impl<false, float>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, routes, route_rng);
   }
 }
 

@@ -96,8 +96,11 @@ class HeffOperator:
     structures of U(1) MPS/MPO problems satisfy.  With a mixed precision,
     ``schedule={"fuse_mpo": 1}`` runs stages 1-3 as one kernel that applies
     W_l W_r straight from tensor memory (``c_per_tile`` sets the fused
-    tile's c extent), ``{"fuse_mpo": 0}`` the stage-1 GEMM, X1 in HBM and
-    the MPO kernel; ``self.schedule`` reports the schedule in effect.  Other structures (``fused`` False) apply
+    tile's c extent), ``{"fuse_mpo": 2}`` (routed) a stage-1 GEMM whose
+    epilogue writes every single-term W_l W_r output straight into the
+    stage-4 operand and keeps X1 only for the multi-term outputs, which the
+    MPO kernel forms, ``{"fuse_mpo": 0}`` the stage-1 GEMM, all of X1 in HBM
+    and the MPO kernel; ``self.schedule`` reports the schedule in effect.  Other structures (``fused`` False) apply
     H_eff through the general unfiltered contraction engine, the
     reference's ``_blockwise_contract`` semantics, one pairwise chain per
     apply: the same result, without the fused kernels."""

@@ -59,10 +59,16 @@ def test_benchmark_structures_plan_fused(chi):
         _capi.check(_capi.LIB.tnx_heff_get_schedule(h, C.byref(s)))
         assert s.fuse_mpo == want, (chi, prec)
         assert (s.c_per_tile >= 1) == bool(want)
+        routed = _capi.HeffSchedule(2, 0)
+        _capi.check(_capi.LIB.tnx_heff_set_schedule(h, C.byref(routed)))
+        _capi.check(_capi.LIB.tnx_heff_get_schedule(h, C.byref(s)))
+        assert s.fuse_mpo == 2 * want and s.c_per_tile == 0
         off = _capi.HeffSchedule(0, 0)
         _capi.check(_capi.LIB.tnx_heff_set_schedule(h, C.byref(off)))
         _capi.check(_capi.LIB.tnx_heff_get_schedule(h, C.byref(s)))
         assert s.fuse_mpo == 0
         bad = _capi.HeffSchedule(1, 99)
+        assert _capi.LIB.tnx_heff_set_schedule(h, C.byref(bad)) == _capi.TNX_ERR_VALUE
+        bad = _capi.HeffSchedule(3, 0)
         assert _capi.LIB.tnx_heff_set_schedule(h, C.byref(bad)) == _capi.TNX_ERR_VALUE
         _capi.LIB.tnx_heff_destroy(h)

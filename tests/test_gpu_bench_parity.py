@@ -61,7 +61,7 @@ def _check(p):
     # FP64, and both mixed precisions on both schedules of stages 1-3
     ops = {"fp64": tb.HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, "fp64")}
     for prec in ("bf16x3", "tf32"):
-        for fz in (0, 1):
+        for fz in (0, 1, 2):
             ops[(prec, fz)] = tb.HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, prec,
                                               schedule={"fuse_mpo": fz, "c_per_tile": 0})
             assert ops[(prec, fz)].schedule["fuse_mpo"] == fz

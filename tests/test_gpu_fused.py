@@ -1,10 +1,14 @@
 """The fused H_eff stages 1-3 kernel (L.theta accumulated in tensor memory,
-W_l W_r applied in its epilogue) against the oracle and against the unfused
-three-kernel path (stage-1 GEMM, X1 in HBM, MPO kernel) on the same inputs.
+W_l W_r applied in its epilogue) and the routed schedule (stage-1 GEMM whose
+epilogue writes the single-term W_l W_r outputs into the stage-4 operand)
+against the oracle and against the unfused three-kernel path (stage-1 GEMM,
+X1 in HBM, MPO kernel) on the same inputs.
 
 Tolerances (relative Frobenius error against the oracle): split-BF16x3 2e-5,
 TF32 5e-3; fused against unfused: 1e-6 (BF16x3) and 1e-4 (TF32), since the
-two paths sum the same FP32 products in different orders.
+two paths sum the same FP32 products in different orders.  Routed against
+unfused: bit for bit (the same operand images, the same MMA K order per
+point, the same FP32 arithmetic for every output slot).
 """
 
 import numpy as np
@@ -26,6 +30,7 @@ TOL = {"bf16x3": 2e-5, "tf32": 5e-3}
 PATH_TOL = {"bf16x3": 1e-6, "tf32": 1e-4}
 FUSED = {"fuse_mpo": 1, "c_per_tile": 0}
 UNFUSED = {"fuse_mpo": 0, "c_per_tile": 0}
+ROUTED = {"fuse_mpo": 2, "c_per_tile": 0}
 
 
 def _host(t):
@@ -86,6 +91,49 @@ def test_fused_matches_oracle_and_unfused(case, precision):
     assert _rel(yf, yu) < PATH_TOL[precision]
 
 
+@pytest.mark.parametrize("precision", ["bf16x3", "tf32"])
+@pytest.mark.parametrize("case", ["cylinder_multi_tile", "tiny_sectors", "wide_chain", "cylinder_gaussian"])
+def test_routed_matches_unfused_bitwise(case, precision):
+    p = _problem(case)
+    rt = _op(p, precision, ROUTED)
+    assert rt.schedule == ROUTED
+    unf = _op(p, precision, UNFUSED)
+    assert rt.keys == unf.keys
+    x = embed_in_keys(p.theta, rt.keys)
+    yr, yu = _apply(rt, x), _apply(unf, x)
+    assert torch.equal(yr, yu)
+    ref = o_blockwise([_host(t) for t in (p.L, x, p.Wl, p.Wr, p.R)], "abc,apqd,bpse,eqtf,dfg->cstg").blocks
+    got = SymmetricTensor.from_flat(p.theta.indices, rt.keys, yr).numpy_blocks()
+    assert _rel({k: v for k, v in got.items() if k in ref}, ref) < TOL[precision]
+
+
+def test_routed_batch_equals_individual():
+    """Three problems of different chi in one routed batch: bit for bit the
+    single-problem applies."""
+    Wl, Wr = W.cylinder_bulk_w()
+    gen = np.random.default_rng(18)
+    probs = [W.make_heff_problem(c, c, Wl, Wr, gen, n_sectors=10, hi=48) for c in (120, 200, 160)]
+    ops = [_op(p, "bf16x3", ROUTED) for p in probs]
+    assert all(o.schedule == ROUTED for o in ops)
+    xs = [embed_in_keys(p.theta, o.keys).data for p, o in zip(probs, ops)]
+    singles = [o.apply(x) for o, x in zip(ops, xs)]
+    batch = tb.HeffBatch(ops)
+    outs = [o.out_like() for o in ops]
+    batch.apply(xs, outs)
+    torch.cuda.synchronize()
+    assert batch.device_error() == 0
+    for a, b in zip(singles, outs):
+        torch.testing.assert_close(a, b, rtol=0, atol=0)
+
+
+def test_routed_fp64_keeps_three_kernels():
+    """FP64 has no routed epilogue: the request falls back to the unfused
+    schedule, which is reported."""
+    p = _problem("tiny_sectors")
+    op = _op(p, "fp64", ROUTED)
+    assert op.schedule == UNFUSED
+
+
 @pytest.mark.parametrize("cc", [1, 2, 5])
 def test_fused_tile_c_extent(cc):
     """Any c extent per tile gives the automatic choice's result (the MMA
@@ -119,9 +167,10 @@ def test_fused_batch_equals_individual():
         torch.testing.assert_close(a, b, rtol=0, atol=0)
 
 
-def test_mixed_schedules_cannot_share_a_batch():
+@pytest.mark.parametrize("pair", [(FUSED, UNFUSED), (ROUTED, UNFUSED), (ROUTED, FUSED)])
+def test_mixed_schedules_cannot_share_a_batch(pair):
     p = _problem("tiny_sectors")
-    a, b = _op(p, "bf16x3", FUSED), _op(p, "bf16x3", UNFUSED)
+    a, b = _op(p, "bf16x3", pair[0]), _op(p, "bf16x3", pair[1])
     with pytest.raises(ValueError):
         tb.HeffBatch([a, b])
 
@@ -136,7 +185,7 @@ def test_autotune_picks_a_candidate_and_caches(tmp_path):
     gen = np.random.default_rng(14)
     probs = [W.make_heff_problem(c, c, Wl, Wr, gen, n_sectors=10, hi=48) for c in (120, 200)]
     cands = autotune.candidates(probs, "bf16x3")
-    assert UNFUSED in cands and cands[0]["fuse_mpo"] == 1
+    assert UNFUSED in cands and ROUTED in cands and cands[0]["fuse_mpo"] == 1
     path = str(tmp_path / "tune.json")
     best, timings = autotune.tune(probs, "bf16x3", cache_path=path, reps=2)
     assert best in cands and len(timings) == len(cands)
