@@ -1085,49 +1085,26 @@ FusedLayout fused_layout(const HeffPlan& H, int mode, int32_t cc_req) {
   return F;
 }
 
-// Routed stages 1-3 (mixed precisions): one stage-1 GEMM group per X1 block
-// (rows (b, c) of its L block, columns d of its theta slice), whose epilogue
-// writes every output slot with a single W_l W_r term straight into the
-// stage-4 image and keeps X1 (FP32) only for the input slots that multi-term
-// output slots read; the MPO kernel then forms just those outputs.
+// Routed stages 1-3 (mixed precisions): the stage-1 GEMM groups and operand
+// images of the unfused path, with an epilogue that writes every output slot
+// with a single W_l W_r term straight into the stage-4 image and keeps X1
+// (FP32) only for the input slots that multi-term output slots read; the MPO
+// kernel then forms just those outputs.
 struct RoutedLayout {
-  std::vector<std::vector<FusedBlk>> blocks;  // per MPO pair: its X1 blocks
-  std::vector<int64_t> lb_tile0;              // per L block: first 16 KB tile of its image (-1: unused)
-  std::vector<int32_t> lb_nKt;
-  int64_t lb_tiles = 0;
-  std::map<std::array<int32_t, 3>, int64_t> thp_tile0;  // (theta block, p, q) -> first tile
-  int64_t thp_tiles = 0;
   std::vector<std::vector<int32_t>> out_terms;  // per pair and output slot: number of terms
   std::vector<std::vector<char>> in_kept;       // per pair and input slot: read by a multi-term output
-  std::string why_not;
 };
 
-RoutedLayout routed_layout(const HeffPlan& H, int mode) {
+// The destinations of one X1 row class (an L block's b: rows rkey .. rkey +
+// mc - 1 of a stage-1 group) in one column class (a theta block's (p, q): the
+// d range starting at column ckey).
+struct RoutedEntry {
+  int32_t g = 0, rkey = 0, ckey = 0, mc = 0, md_pad = 0;
+  std::vector<DevRoute> routes;
+};
+
+RoutedLayout routed_layout(const HeffPlan& H) {
   RoutedLayout F;
-  const int tk = img_geom(mode).tk;
-  F.why_not = pair_blocks(H, F.blocks);
-  if (!F.why_not.empty()) return F;
-  F.lb_tile0.assign(H.L.keys.size(), -1);
-  F.lb_nKt.assign(H.L.keys.size(), 0);
-  for (auto& bl : F.blocks)
-    for (auto& b : bl) {
-      const auto& ld = H.L.dims[b.l_blk];
-      if (ld[1] * ld[2] > (int64_t{1} << 30)) {
-        F.why_not = "an L block has more than 2^30 rows (b, c)";
-        return F;
-      }
-      if (F.lb_tile0[b.l_blk] < 0) {
-        F.lb_nKt[b.l_blk] = static_cast<int32_t>(cdiv(ld[0], tk));
-        F.lb_tile0[b.l_blk] = F.lb_tiles;
-        F.lb_tiles += cdiv(ld[1] * ld[2], 128) * F.lb_nKt[b.l_blk];
-      }
-      const std::array<int32_t, 3> tkey{b.th_blk, b.pp, b.qq};
-      if (!F.thp_tile0.count(tkey)) {
-        const auto& td = H.th.dims[b.th_blk];
-        F.thp_tile0[tkey] = F.thp_tiles;
-        F.thp_tiles += cdiv(td[3], 128) * cdiv(td[0], tk);
-      }
-    }
   F.out_terms.resize(H.pairs.size());
   F.in_kept.resize(H.pairs.size());
   for (size_t p = 0; p < H.pairs.size(); ++p) {
@@ -1165,11 +1142,9 @@ struct tnx_heff {
   bool fused = false;
   FusedLayout fl;
   DevMem lp_img;
-  // routed stages 1-3 (mixed precisions): layout and the per-L-block image
+  // routed stages 1-3 (mixed precisions): which output slots the epilogue writes
   bool routed = false;
   RoutedLayout rl;
-  DevMem lb_img;
-  int64_t lb_lo = 0;
 };
 
 int tnx_heff_create(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, const tnx_tensor_desc* Wl,
@@ -1218,10 +1193,7 @@ int tnx_heff_get_schedule(const tnx_heff* h, tnx_heff_schedule* sched) {
         fz = fl.why_not.empty();
         cc = fl.cc;
       }
-      if (mode != IMG_F64 && h->sched_fuse == 2 && h->H.closed && h->H.s4_separable) {
-        std::vector<std::vector<FusedBlk>> blocks;
-        rt = pair_blocks(h->H, blocks).empty();
-      }
+      if (mode != IMG_F64 && h->sched_fuse == 2 && h->H.closed && h->H.s4_separable) rt = true;
       sched->fuse_mpo = fz ? 1 : (rt ? 2 : 0);
       sched->c_per_tile = fz ? cc : 0;
       return TNX_OK;
@@ -1276,7 +1248,7 @@ int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const
     // fused stages 1-3 where the schedule asks for it and the structure fits
     h->fused = false;
     h->fl = FusedLayout{};
-    if (mode != IMG_F64 && h->sched_fuse) {
+    if (mode != IMG_F64 && h->sched_fuse == 1) {
       h->fl = fused_layout(H, mode, h->sched_cc);
       for (auto& mp : H.pairs)
         if (mp.terms.size() > static_cast<size_t>(kFusedMaxTerms))
@@ -1286,11 +1258,11 @@ int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const
     h->routed = false;
     h->rl = RoutedLayout{};
     if (mode != IMG_F64 && h->sched_fuse == 2) {
-      h->rl = routed_layout(H, mode);
-      h->routed = h->rl.why_not.empty();
+      h->rl = routed_layout(H);
+      h->routed = true;
     }
-    // the stage-1 A image (L) only serves the unfused path
-    const bool plain = !h->fused && !h->routed;
+    // the stage-1 A image (L) serves the unfused and routed paths
+    const bool plain = !h->fused;
     h->l_img.alloc(plain ? std::max<int64_t>(1, h->g1.a_tiles) * ig.tile_bytes * split : 0);
     h->r_img.alloc(std::max<int64_t>(1, h->g4.b_tiles) * ig.tile_bytes * split);
     h->l_lo = h->g1.a_tiles * ig.tile_bytes;
@@ -1350,37 +1322,6 @@ int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const
     if (plain)
       build_pack(H.s1.packA, h->g1, true, reinterpret_cast<uint64_t>(h->l_img.p), h->l_lo, ig.tile_bytes, 0, pl, cl,
                  1.0 / sL);
-    if (h->routed) {
-      // one image per L block: rows (b, c) with c fastest, K = a (the same
-      // values as the unfused image, split from FP64)
-      h->lb_img.alloc(std::max<int64_t>(1, h->rl.lb_tiles) * ig.tile_bytes * split);
-      h->lb_lo = h->rl.lb_tiles * ig.tile_bytes;
-      CUDA_OK(cudaMemsetAsync(h->lb_img.p, 0, h->lb_img.n, st));
-      for (size_t lb = 0; lb < H.L.keys.size(); ++lb) {
-        if (h->rl.lb_tile0[lb] < 0) continue;
-        const auto& ld = H.L.dims[lb];
-        DevPackSeg d{};
-        d.src_off = H.L.offs[lb];
-        d.img_addr = reinterpret_cast<uint64_t>(h->lb_img.p) + static_cast<uint64_t>(h->rl.lb_tile0[lb]) * ig.tile_bytes;
-        d.lo_off = h->lb_lo;
-        d.nKt = h->rl.lb_nKt[lb];
-        d.nlegs = 3;
-        d.src_slot = 0;
-        d.kcount = static_cast<int32_t>(ld[0]);
-        d.scale = 1.0 / sL;
-        for (int l = 0; l < 3; ++l) d.dims[l] = static_cast<int32_t>(ld[l]);
-        d.rstr[1] = static_cast<int32_t>(ld[2]);
-        d.rstr[2] = 1;
-        d.kstr[0] = 1;
-        d.kdstr[0] = 1;
-        const int seg_id = static_cast<int>(pl.size());
-        pl.push_back(d);
-        const int64_t count = ld[0] * ld[1] * ld[2];
-        for (int64_t e0 = 0; e0 < count; e0 += 2048) cl.push_back({seg_id, 0, e0, std::min<int64_t>(2048, count - e0)});
-      }
-    } else {
-      h->lb_img.alloc(0);
-    }
     build_pack(H.s4.packB, h->g4, false, reinterpret_cast<uint64_t>(h->r_img.p), h->r_lo, ig.tile_bytes, 1, pr, cr,
                1.0 / sR);
     DevMem dpl, dcl, dpr, dcr, tab;
@@ -1435,7 +1376,7 @@ struct tnx_heff_batch {
   // routed stages 1-3: the stage-1 epilogue's destinations (per row class b:
   // a range of routes) and X1 of the input slots multi-term outputs read
   bool routed = false;
-  DevMem routes, route_rng;
+  DevMem routes, route_win, route_rows, route_cols;
   const int32_t* skip = nullptr;
   int n_launches = 0;
   std::vector<uint64_t> last_src, last_out;
@@ -1508,9 +1449,9 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         for (auto& g : H.s1.groups) x1_elems += g.M * x1_ld(g.N);
       }
     }
-    // the unfused path's stage-1 B image and X1 result; the fused and routed
-    // paths' theta panels (and the routed path's kept X1 slots)
-    b->th_img.alloc(fz || rt ? 16 : std::max<int64_t>(1, th_tiles) * ig.tile_bytes * split);
+    // the unfused and routed paths' stage-1 B image and X1 result (routed:
+    // the kept X1 slots only); the fused path's theta panels
+    b->th_img.alloc(fz ? 16 : std::max<int64_t>(1, th_tiles) * ig.tile_bytes * split);
     b->x3_img.alloc(std::max<int64_t>(1, x3_tiles) * ig.tile_bytes * split);
     b->th_lo = th_tiles * ig.tile_bytes;
     b->x3_lo = x3_tiles * ig.tile_bytes;
@@ -1519,10 +1460,10 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     CUDA_OK(cudaMemset(b->x3_img.p, 0, b->x3_img.n));
     std::vector<int64_t> thp_t0(n, 0);
     int64_t thp_tiles = 0;
-    if (fz || rt) {
+    if (fz) {
       for (int i = 0; i < n; ++i) {
         thp_t0[i] = thp_tiles;
-        thp_tiles += fz ? hs[i]->fl.thp_tiles : hs[i]->rl.thp_tiles;
+        thp_tiles += hs[i]->fl.thp_tiles;
       }
       b->thp_img.alloc(std::max<int64_t>(1, thp_tiles) * ig.tile_bytes * split);
       CUDA_OK(cudaMemset(b->thp_img.p, 0, b->thp_img.n));
@@ -1555,9 +1496,11 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     std::vector<int2> MC;
     std::vector<DevChunk> ZC;
     std::vector<DevRoute> RT;
-    std::vector<int2> RB;
+    std::vector<int2> RB, RI, CI;
+    std::vector<int2> RG;  // routed groups: (first RB entry, column classes)
     for (int i = 0; i < n; ++i) {
       tnx_heff* h = hs[i];
+      std::vector<RoutedEntry> rents;
       const HeffPlan& H = h->H;
       // theta pack: source slot i, images into the batch theta buffer
       PairGeom gth = h->g1;  // b_tile0 relative to this problem
@@ -1594,10 +1537,10 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         for (int r0 = 0; r0 < rs.rows; r0 += 256)
           for (int kc = 0; kc < nkc; kc += cpt) trc.push_back(make_int4(id, r0, kc, 0));
       }
-      if (fz || rt) {
+      if (fz) {
         // theta panels: each referenced (theta block, p, q) slice as rows d, K = a
         const int tk = ig.tk;
-        for (const auto& kv : fz ? h->fl.thp_tile0 : h->rl.thp_tile0) {
+        for (const auto& kv : h->fl.thp_tile0) {
           const int tb = kv.first[0], pp = kv.first[1], qq = kv.first[2];
           const auto& td = H.th.dims[tb];
           DevRowPackSeg rs{};
@@ -1619,10 +1562,12 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
             for (int kc = 0; kc < nkc; kc += cpt) fthc.push_back(make_int4(id, r0, kc, 0));
         }
       }
-      // stage-1 groups (the routed path builds its own with the MPO tables)
+      // stage-1 groups (routed: their rows and 8-column units get classes and
+      // destinations with the MPO tables below)
       std::vector<int64_t> x1_goff;
       int64_t xo = x1_0[i];
-      for (size_t g = 0; g < H.s1.groups.size() && !rt; ++g) {
+      const int g1base = static_cast<int>(G1.size());
+      for (size_t g = 0; g < H.s1.groups.size(); ++g) {
         x1_goff.push_back(xo);
         DevGroup x{};
         x.a_addr = reinterpret_cast<uint64_t>(h->l_img.p) + static_cast<uint64_t>(h->g1.a_tile0[g]) * ig.tile_bytes;
@@ -1636,6 +1581,17 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         x.kk_last = kk_last_of(H.s1.groups[g].K, b->mode);
         x.out_slot = 0;
         x.scale = 1.0;
+        if (rt) {
+          // row and 8-column-unit classes, filled with the MPO tables below
+          x.routed = 1;
+          x.rowoff0 = static_cast<int64_t>(RI.size());
+          x.cinfo0 = static_cast<int32_t>(CI.size());
+          RI.resize(RI.size() + H.s1.groups[g].M, make_int2(-1, 0));
+          CI.resize(CI.size() + cdiv(H.s1.groups[g].N, 8), make_int2(-1, 0));
+          G1.push_back(x);
+          RG.resize(G1.size(), make_int2(0, 1));
+          continue;
+        }
         const int64_t ld = x1_ld(H.s1.groups[g].N);
         x.vec_ld = static_cast<int32_t>(ld);
         for (int64_t r = 0; r < H.s1.groups[g].M; ++r) R1.push_back(xo + r * ld);
@@ -1643,10 +1599,8 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         G1.push_back(x);
       }
       std::vector<std::pair<int64_t, DevTile>> tl;
-      if (!rt) {
-        build_tiles(H.s1, h->g1, static_cast<int>(G1.size() - H.s1.groups.size()), tl);
-        T1.insert(T1.end(), tl.begin(), tl.end());
-      }
+      build_tiles(H.s1, h->g1, g1base, tl);
+      T1.insert(T1.end(), tl.begin(), tl.end());
       // stage-4 groups
       PairGeom gx3 = h->g4;
       for (auto& t : gx3.a_tile0) t += x3_t0[i];
@@ -1756,59 +1710,50 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         const int pair_id = static_cast<int>(MP.size());
         MP.push_back(dp);
         if (rt) {
-          // one stage-1 group per X1 block; a row class b routes to the
-          // single-term output slots of its input slot and, when a
-          // multi-term output reads that slot, to its kept X1 rows
+          // the destinations of every X1 row (b, c) and (p, q) column range of
+          // this pair: the single-term output slots its input slot feeds and,
+          // when a multi-term output reads that slot, its kept X1 rows
           std::vector<std::vector<std::pair<int32_t, double>>> singles(mp.n_in_slots);
           for (const MpoTerm& t : mp.terms)
             if (h->rl.out_terms[pi][t.out_slot] == 1) singles[t.in_slot].push_back({t.out_slot, t.w});
-          for (const FusedBlk& fb : h->rl.blocks[pi]) {
-            DevGroup x{};
-            x.a_addr = reinterpret_cast<uint64_t>(h->lb_img.p) +
-                       static_cast<uint64_t>(h->rl.lb_tile0[fb.l_blk]) * ig.tile_bytes;
-            x.b_addr = thp_base + static_cast<uint64_t>(thp_t0[i] + h->rl.thp_tile0.at({fb.th_blk, fb.pp, fb.qq})) *
-                                      ig.tile_bytes;
-            x.a_lo = h->lb_lo;
-            x.b_lo = thp_lo;
-            x.M = fb.mb * mp.mc;
-            x.N = mp.md;
-            x.nKt = h->rl.lb_nKt[fb.l_blk];
-            x.kk_last = kk_last_of(fb.ma, b->mode);
-            x.scale = 1.0;
-            x.routed = 1;
-            x.route0 = static_cast<int32_t>(RB.size());
-            x.mc = mp.mc;
-            x.md = mp.md;
-            for (int32_t bb = 0; bb < fb.mb; ++bb) {
-              const int32_t sl = fb.slot0 + bb * fb.slot_stride;
-              const int32_t r0 = static_cast<int32_t>(RT.size());
-              for (const auto& ow : singles.at(sl)) {
-                const DevMpoOutSlot& os = MO[dp.out0 + ow.first];
-                DevRoute r{};
-                r.addr = os.img_addr;
-                r.lo_off = os.lo_off;
-                r.nKt = os.nKt;
-                r.row0 = os.row0 + os.row_add;
-                r.rstride = os.rows_per_c;
-                r.k0 = os.k0 + os.k_add;
-                r.w = static_cast<float>(ow.second);
-                r.kind = 0;
-                RT.push_back(r);
-              }
-              if (h->rl.in_kept[pi][sl]) {
-                DevRoute r{};
-                r.addr = MI[dp.in0 + sl].base;
-                r.rstride = md_pad;
-                r.w = 1.0f;
-                r.kind = 1;
-                RT.push_back(r);
-              }
-              RB.push_back(make_int2(r0, static_cast<int32_t>(RT.size()) - r0));
-            }
-            const int gid = static_cast<int>(G1.size());
-            G1.push_back(x);
-            for (int mt = 0; mt < cdiv(x.M, 128); ++mt)
-              for (int nt = 0; nt < cdiv(x.N, 128); ++nt) T1.push_back({x.nKt, DevTile{gid, mt, nt, 0}});
+          for (size_t k = 0; k < mp.ins.size(); ++k) {
+            const MpoIn& in = mp.ins[k];
+            for (int32_t bb = 0; bb < in.mb; ++bb)
+              for (int32_t pp = 0; pp < in.mp; ++pp)
+                for (int32_t qq = 0; qq < in.mq; ++qq) {
+                  const int32_t sl = mp.in_slot0[k] + (bb * in.mp + pp) * in.mq + qq;
+                  RoutedEntry e;
+                  e.g = in.g1;
+                  e.rkey = in.row0 + bb * mp.mc;
+                  e.ckey = static_cast<int32_t>(in.col0 + (pp * in.mq + qq) * md_x1);
+                  e.mc = mp.mc;
+                  for (const auto& ow : singles.at(sl)) {
+                    const DevMpoOutSlot& os = MO[dp.out0 + ow.first];
+                    DevRoute r{};
+                    r.addr = os.img_addr;
+                    if (os.nKt > 65535) return set_err(TNX_ERR_UNSUPPORTED, "a stage-4 group has more than 65535 K tiles");
+                    r.nKt = static_cast<uint16_t>(os.nKt);
+                    r.row0 = os.row0 + os.row_add;
+                    r.rstride = os.rows_per_c;
+                    r.k0 = os.k0 + os.k_add;
+                    r.w = static_cast<float>(ow.second);
+                    // a power-of-two weight rescales the row's image form exactly
+                    int ex = 0;
+                    const double mant = std::frexp(std::fabs(ow.second), &ex);
+                    r.kind = static_cast<uint8_t>((mant == 0.5 && ex >= -20 && ex <= 21) ? 2 : 0);
+                    e.routes.push_back(r);
+                  }
+                  if (h->rl.in_kept[pi][sl]) {
+                    DevRoute r{};
+                    r.addr = MI[dp.in0 + sl].base;
+                    r.rstride = md_pad;
+                    r.w = 1.0f;
+                    r.kind = 1;
+                    e.routes.push_back(r);
+                  }
+                  e.md_pad = md_pad;
+                  rents.push_back(std::move(e));
+                }
           }
         }
         if (fz) {
@@ -1870,6 +1815,71 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         const int npts = mp.mc * ((mp.md + dpt - 1) / dpt);
         for (int p0 = 0; p0 < npts && dp.n_terms > 0; p0 += ppc) MC.push_back(make_int2(pair_id, p0));
       }
+      if (rt) {
+        // classes of each group in row and column order, the rows' and
+        // units' classes, and the routes in (row class, column class) order,
+        // so that the rows of one warp read one contiguous range of routes
+        const size_t ng = H.s1.groups.size();
+        std::vector<std::map<int32_t, int32_t>> rcl(ng), ccl(ng);
+        std::vector<int64_t> rb0;
+        std::vector<int32_t> ncc;
+        for (const RoutedEntry& e : rents) {
+          if (e.ckey % 8 || e.g < 0 || static_cast<size_t>(e.g) >= ng)
+            return set_err(TNX_ERR_RUNTIME, "internal: a routed column range is not 8-aligned");
+          rcl[e.g][e.rkey] = 0;
+          ccl[e.g][e.ckey] = 0;
+        }
+        for (size_t g = 0; g < ng; ++g) {
+          int32_t id = 0;
+          for (auto& kv : rcl[g]) kv.second = id++;
+          id = 0;
+          for (auto& kv : ccl[g]) kv.second = id++;
+          if (ccl[g].size() > 255) return set_err(TNX_ERR_UNSUPPORTED, "a stage-1 group has more than 255 column classes");
+          rb0.push_back(static_cast<int64_t>(RB.size()));
+          ncc.push_back(std::max<int32_t>(1, static_cast<int32_t>(ccl[g].size())));
+          RB.resize(RB.size() + rcl[g].size() * static_cast<size_t>(ncc.back()), make_int2(0, 0));
+        }
+        std::vector<std::array<int64_t, 4>> order;  // (group, RB index, entry, classes)
+        for (size_t k = 0; k < rents.size(); ++k) {
+          const RoutedEntry& e = rents[k];
+          const DevGroup& x = G1[g1base + e.g];
+          const int32_t rc = rcl[e.g][e.rkey], cc = ccl[e.g][e.ckey];
+          const GroupShape& gs = H.s1.groups[e.g];
+          if (e.rkey < 0 || e.rkey + e.mc > gs.M || e.ckey + e.md_pad > cdiv(gs.N, 8) * 8)
+            return set_err(TNX_ERR_RUNTIME, "internal: a routed X1 block lies outside its group");
+          for (int32_t c = 0; c < e.mc; ++c) RI[x.rowoff0 + e.rkey + c] = make_int2(rc, c);
+          for (int32_t j = 0; j < e.md_pad / 8; ++j) CI[x.cinfo0 + e.ckey / 8 + j] = make_int2(cc, 8 * j);
+          order.push_back({e.g, rb0[e.g] + static_cast<int64_t>(rc) * ncc[e.g] + cc, static_cast<int64_t>(k),
+                           (static_cast<int64_t>(rc) << 8) | cc});
+        }
+        std::sort(order.begin(), order.end());
+        for (size_t g = 0; g < ng; ++g) {
+          RG[g1base + g] = make_int2(static_cast<int32_t>(rb0[g]), ncc[g]);
+        }
+        const uint64_t x1_end = x1_base + static_cast<uint64_t>(b->x1.n);
+        for (const auto& o : order) {
+          const RoutedEntry& e = rents[o[2]];
+          if (RB[o[1]].y != 0) return set_err(TNX_ERR_RUNTIME, "internal: two X1 blocks share a routed class pair");
+          RB[o[1]] = make_int2(static_cast<int32_t>(RT.size()), static_cast<int32_t>(e.routes.size()));
+          for (DevRoute r : e.routes) {
+            r.rc = static_cast<int32_t>(o[3] >> 8);
+            r.cc = static_cast<uint8_t>(o[3] & 255);
+            // every (c, d) of the entry lands inside the X3 image or the kept X1 slots
+            const int64_t last = static_cast<int64_t>(e.mc - 1) * r.rstride;
+            if (r.kind != 1) {
+              const uint64_t end = r.addr + static_cast<uint64_t>(cdiv(r.row0 + last + 1, 128) * r.nKt) * ig.tile_bytes;
+              if (r.addr < x3_base || end > x3_base + static_cast<uint64_t>(x3_tiles) * ig.tile_bytes ||
+                  r.k0 + e.md_pad > static_cast<int64_t>(r.nKt) * ig.tk)
+                return set_err(TNX_ERR_RUNTIME, "internal: a route writes outside the X3 image");
+            } else {
+              const uint64_t end = r.addr + static_cast<uint64_t>(last + e.md_pad) * 4;
+              if (r.addr < x1_base || end > x1_end || r.addr % 32 || r.rstride % kMpoKAlign)
+                return set_err(TNX_ERR_RUNTIME, "internal: a route writes outside the kept X1 slots");
+            }
+            RT.push_back(r);
+          }
+        }
+      }
     }
     if (b->mpo_smem > 200 * 1024)
       return set_err(TNX_ERR_UNSUPPORTED, "MPO term tables too large for the fused MPO kernel");
@@ -1886,6 +1896,35 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     upload(b->ro1, R1);
     auto t1 = sorted_tiles(T1);
     upload(b->t1, t1);
+    if (rt) {
+      // per (tile, lane quarter, 32-column chunk): the one range of routes
+      // holding every (row class, column class) pair of its 32 rows and 4 units
+      std::vector<int2> TW(t1.size() * 16, make_int2(0, 0));
+      for (size_t t = 0; t < t1.size(); ++t) {
+        const DevGroup& g = G1[t1[t].g];
+        const int2 rg = RG[t1[t].g];
+        for (int q = 0; q < 4; ++q)
+          for (int ch = 0; ch < 4; ++ch) {
+            const int col0 = t1[t].nt * 128 + 32 * ch;
+            int lo = 0x7fffffff, hi = 0;
+            for (int lane = 0; lane < 32; ++lane) {
+              const int row = t1[t].mt * 128 + 32 * q + lane;
+              if (row >= g.M || RI[g.rowoff0 + row].x < 0) continue;
+              for (int u = 0; u < 4; ++u) {
+                const int col = col0 + 8 * u;
+                if (col >= g.N || CI[g.cinfo0 + col / 8].x < 0) continue;
+                const int2 r = RB[rg.x + static_cast<int64_t>(RI[g.rowoff0 + row].x) * rg.y + CI[g.cinfo0 + col / 8].x];
+                if (r.y > 0) {
+                  lo = std::min(lo, r.x);
+                  hi = std::max(hi, r.x + r.y);
+                }
+              }
+            }
+            if (hi > lo) TW[t * 16 + q * 4 + ch] = make_int2(lo, hi - lo);
+          }
+      }
+      upload(b->route_win, TW);
+    }
     b->n_t1 = static_cast<int>(t1.size());
     upload(b->g4, G4);
     upload(b->ro4, R4);
@@ -1947,40 +1986,15 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
       upload(b->f_tiles, ftl);
       b->n_f_tiles = static_cast<int>(ftl.size());
     }
-    if (fz || rt) {
+    if (fz) {
       upload(b->thp_rows, fth);
       upload(b->thp_row_chunks, fthc);
       b->n_thp_row_chunks = static_cast<int>(fthc.size());
     }
     if (rt) {
-      // every route stays inside the X3 image or the kept X1 slots
-      const uint64_t x3_end = x3_base + static_cast<uint64_t>(x3_tiles) * ig.tile_bytes;
-      const uint64_t x1_end = x1_base + static_cast<uint64_t>(b->x1.n);
-      for (const DevGroup& g : G1) {
-        if (!g.routed || g.mc < 1 || g.M % g.mc || g.route0 < 0 || g.route0 + g.M / g.mc > static_cast<int64_t>(RB.size()))
-          return set_err(TNX_ERR_RUNTIME, "internal: routed group tables out of range");
-        const int32_t md_pad = (g.md + kMpoKAlign - 1) / kMpoKAlign * kMpoKAlign;
-        for (int bb = 0; bb < g.M / g.mc; ++bb) {
-          const int2 rr = RB[g.route0 + bb];
-          if (rr.x < 0 || rr.y < 0 || rr.x + rr.y > static_cast<int64_t>(RT.size()))
-            return set_err(TNX_ERR_RUNTIME, "internal: route range out of range");
-          for (int r = rr.x; r < rr.x + rr.y; ++r) {
-            const DevRoute& R = RT[r];
-            const int64_t last = static_cast<int64_t>(g.mc - 1) * R.rstride;
-            if (R.kind == 0) {
-              const uint64_t end = R.addr + static_cast<uint64_t>(cdiv(R.row0 + last + 1, 128) * R.nKt) * ig.tile_bytes;
-              if (R.addr < x3_base || end > x3_end || R.lo_off != b->x3_lo || R.k0 + md_pad > R.nKt * ig.tk)
-                return set_err(TNX_ERR_RUNTIME, "internal: a route writes outside the X3 image");
-            } else {
-              const uint64_t end = R.addr + static_cast<uint64_t>(last + md_pad) * 4;
-              if (R.addr < x1_base || end > x1_end || R.addr % 32 || R.rstride % kMpoKAlign)
-                return set_err(TNX_ERR_RUNTIME, "internal: a route writes outside the kept X1 slots");
-            }
-          }
-        }
-      }
       upload(b->routes, RT);
-      upload(b->route_rng, RB);
+      upload(b->route_rows, RI);
+      upload(b->route_cols, CI);
     }
     b->n_mpo_chunks = static_cast<int>(MC.size());
     b->err.alloc(sizeof(int32_t));
@@ -2025,11 +2039,6 @@ static void heff_batch_stage(tnx_heff_batch* b, int stage, cudaStream_t st, cons
                         b->n_f_tiles, b->err.as<int32_t>(), b->skip, st);
     return;
   }
-  if (b->routed && stage == 0) {
-    launch_pack_rows(src_tab, b->thp_rows.as<DevRowPackSeg>(), b->thp_row_chunks.as<int4>(), b->n_thp_row_chunks,
-                     b->mode, b->skip, st);
-    return;
-  }
   switch (stage) {
     case 0:
       if (b->th_by_rows)
@@ -2046,7 +2055,9 @@ static void heff_batch_stage(tnx_heff_batch* b, int stage, cudaStream_t st, cons
       else
         launch_gemm_tc(b->mode, b->g1.as<DevGroup>(), b->t1.as<DevTile>(), b->n_t1, b->ro1.as<int64_t>(),
                        b->out_tab1.as<uint64_t>(), false, b->err.as<int32_t>(), b->skip, st,
-                       b->routed ? b->routes.as<DevRoute>() : nullptr, b->routed ? b->route_rng.as<int2>() : nullptr);
+                       b->routed ? DevRouteTabs{b->x3_lo, b->routes.as<DevRoute>(), b->route_win.as<int2>(),
+                                                b->route_rows.as<int2>(), b->route_cols.as<int2>()}
+                                 : DevRouteTabs{});
       break;
     case 2:
       launch_mpo_apply(f32, b->mode, b->mpo_pairs.as<DevMpoPair>(), b->mpo_slots.as<DevMpoSlot>(),

@@ -124,22 +124,37 @@ struct DevGroup {
   int32_t vec_ld;           // > 0: every row offset is a multiple of 4 elements and the first
                             // vec_ld (a multiple of 4, >= N) columns may be written: 16-byte stores
   int32_t kk_last;          // tcgen05: MMA K steps (of the 4 per slab) the last K slab needs; 0 = all 4
-  // routed epilogue (tcgen05 H_eff stage 1): rows are (b, c) with c fastest,
-  // columns are d; row (b, c) goes through routes[route_rng[route0 + b]]
-  // instead of the row-offset table.  routed = 0: plain rows.
-  int32_t routed, route0, mc, md;
+  // routed epilogue (tcgen05 H_eff stage 1), instead of the row-offset table:
+  // row r has (row class, c) = rows[rowoff0 + r], the 8-column unit u has
+  // (column class, d of its first column) = cols[cinfo0 + u]; the routes a
+  // warp's rows and chunk may need are one window of the route list, named
+  // per tile.  routed = 0: plain rows.
+  int32_t routed, cinfo0, pad0, pad1;
 };
 
-// One destination of a routed stage-1 row (b, c): kind 0 writes w * row into
-// the stage-4 operand image at image row row0 + c * rstride, K k0 + d (8 d per
-// aligned chunk, the image's own precision split); kind 1 writes w * row in
-// FP32 at addr + (c * rstride + d) * 4.
+// One destination of the routed stage-1 rows of one (row class, column class)
+// pair: kinds 0 and 2 write w * row into the stage-4 operand image at image
+// row row0 + c * rstride, K k0 + d (8 d per aligned unit, the image's own
+// precision split; kind 2: w is a power of two, applied to the split form,
+// which gives the same bits); kind 1 writes w * row in FP32 at
+// addr + (c * rstride + d) * 4.  32 bytes: two 16-byte asynchronous copies.
 struct DevRoute {
-  uint64_t addr;     // kind 0: image tile 0; kind 1: element (c = 0, d = 0)
-  int64_t lo_off;    // kind 0: byte offset of the low-part image
-  int32_t nKt, row0, rstride, k0;
+  uint64_t addr;     // kinds 0, 2: image tile 0; kind 1: element (c = 0, d = 0)
+  int32_t row0, rstride, k0;
   float w;
-  int32_t kind;
+  uint16_t nKt;
+  uint8_t kind, cc;  // cc: the column class the route serves
+  int32_t rc;        // the row class the route serves
+};
+static_assert(sizeof(DevRoute) == 32, "route records are two 16-byte units");
+
+// The routed epilogue's tables (see DevGroup and DevRoute).
+struct DevRouteTabs {
+  int64_t lo_off;    // byte offset of the low-part stage-4 image (kinds 0, 2)
+  const DevRoute* routes;
+  const int2* win;   // per (tile, lane quarter, 32-column chunk): (first route, count)
+  const int2* rows;  // (row class, c) per group row; class -1: no destinations
+  const int2* cols;  // (column class, d) per 8-column unit; class -1: padding
 };
 
 struct DevTile {

@@ -74,12 +74,119 @@ struct TileIter {
 constexpr int kStagePitch = 33;  // fp32 words per staged row (+1 breaks bank conflicts)
 constexpr int kEpiStageBytes = EPI_WARPS * 32 * kStagePitch * 4;
 
+// 8 values in their image form: BF16 -> four hi and four lo bf16x2 words
+// (split as the packing kernels split); TF32 -> two units of four TF32 words
+// (hi[0..3] then lo[0..3] hold the eight values).
+template <bool TF32>
+static __device__ __forceinline__ void img_units(const float (&v)[kMpoVec], uint32_t (&hi)[4], uint32_t (&lo)[4]) {
+  if constexpr (TF32) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi[u]) : "f"(v[u]));
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo[u]) : "f"(v[4 + u]));
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * u], v[2 * u + 1]);
+      const __nv_bfloat162 l = __floats2bfloat162_rn(v[2 * u] - __low2float(h), v[2 * u + 1] - __high2float(h));
+      hi[u] = *reinterpret_cast<const uint32_t*>(&h);
+      lo[u] = *reinterpret_cast<const uint32_t*>(&l);
+    }
+  }
+}
+
+// Image units from img_units scaled by a power of two w (exact: the image
+// form of w * v), stored at K k (a multiple of 8) of the row at `img`.
+template <bool TF32>
+static __device__ __forceinline__ void img_store_units(uint8_t* img, int64_t lo_off, int key, int k,
+                                                       const uint32_t (&hi)[4], const uint32_t (&lo)[4], float w) {
+  if constexpr (TF32) {
+    const int j = (k >> 2) & 7;
+    uint8_t* t = img + static_cast<int64_t>(k >> 5) * TILE_BYTES;
+    uint32_t a[4], b[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a[u] = __float_as_uint(__uint_as_float(hi[u]) * w);
+      b[u] = __float_as_uint(__uint_as_float(lo[u]) * w);
+    }
+    *reinterpret_cast<uint4*>(t + ((j ^ key) << 4)) = make_uint4(a[0], a[1], a[2], a[3]);
+    *reinterpret_cast<uint4*>(t + (((j + 1) ^ key) << 4)) = make_uint4(b[0], b[1], b[2], b[3]);
+  } else {
+    const __nv_bfloat162 w2 = __float2bfloat162_rn(w);
+    uint32_t a[4], b[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const __nv_bfloat162 h = __hmul2(*reinterpret_cast<const __nv_bfloat162*>(&hi[u]), w2);
+      const __nv_bfloat162 l = __hmul2(*reinterpret_cast<const __nv_bfloat162*>(&lo[u]), w2);
+      a[u] = *reinterpret_cast<const uint32_t*>(&h);
+      b[u] = *reinterpret_cast<const uint32_t*>(&l);
+    }
+    uint8_t* t = img + static_cast<int64_t>(k >> 6) * TILE_BYTES + ((((k >> 3) & 7) ^ key) << 4);
+    *reinterpret_cast<uint4*>(t) = make_uint4(a[0], a[1], a[2], a[3]);
+    *reinterpret_cast<uint4*>(t + lo_off) = make_uint4(b[0], b[1], b[2], b[3]);
+  }
+}
+
+// route records of one 32-column chunk's window a warp's staging buffer holds
+// (two buffers of NCH windows); larger windows are read from global memory
+constexpr int kWin = 32;
+static_assert(2 * (TBN / 32 / (EPI_WARPS / 4)) * kWin * 32 <= 32 * kStagePitch * 4,
+              "route windows fit the warp's staging buffer");
+
+// 16-byte asynchronous copy global -> shared (L2 only), its group commit and
+// the wait for every group but the most recent one
+static __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
+}
+static __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+static __device__ __forceinline__ void cp_async_wait_prior() {
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+
+// Byte offset of the start of row `row` in an operand image of nKt K tiles
+// (16 KB tiles of 128 rows x 128 bytes, SWIZZLE_128B: the 16-byte unit j of
+// a row sits at unit j ^ (row & 7)).
+static __device__ __forceinline__ int64_t img_row_base(int nKt, int64_t row) {
+  return (row >> 7) * static_cast<int64_t>(nKt) * TILE_BYTES + (row & 127) * 128;
+}
+
+// 8 consecutive K (k a multiple of 8) of one image row whose start is `img`
+// and swizzle key `key`: a 16-byte unit of the hi and of the lo BF16 images
+// (split as the packing kernels split), or two units of TF32.
+template <bool TF32>
+static __device__ __forceinline__ void img_row_chunk(uint8_t* img, int64_t lo_off, int key, int k,
+                                                     const float (&v)[kMpoVec]) {
+  if constexpr (TF32) {
+    const int j = (k >> 2) & 7;
+    uint8_t* t = img + static_cast<int64_t>(k >> 5) * TILE_BYTES;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      uint32_t w[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(w[u]) : "f"(v[4 * h + u]));
+      *reinterpret_cast<uint4*>(t + (((j + h) ^ key) << 4)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  } else {
+    uint32_t hi[4], lo[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * u], v[2 * u + 1]);
+      const __nv_bfloat162 l = __floats2bfloat162_rn(v[2 * u] - __low2float(h), v[2 * u + 1] - __high2float(h));
+      hi[u] = *reinterpret_cast<const uint32_t*>(&h);
+      lo[u] = *reinterpret_cast<const uint32_t*>(&l);
+    }
+    uint8_t* t = img + static_cast<int64_t>(k >> 6) * TILE_BYTES + ((((k >> 3) & 7) ^ key) << 4);
+    *reinterpret_cast<uint4*>(t) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<uint4*>(t + lo_off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  }
+}
+
 template <bool TF32, typename OutT>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_tc_kernel(const DevGroup* __restrict__ groups, const DevTile* __restrict__ tiles, int n_tiles,
                    const int64_t* __restrict__ rowoff, const uint64_t* __restrict__ out_tab, int32_t* err_flag,
-                   const int32_t* __restrict__ skip, const DevRoute* __restrict__ routes,
-                   const int2* __restrict__ route_rng) {
+                   const int32_t* __restrict__ skip, const DevRouteTabs rt) {
   constexpr int NT = TF32 ? 2 : 4;          // operand tiles per stage
   constexpr int STAGES = TF32 ? 6 : 3;      // 192 KB of operand ring either way
   constexpr int KSUB = 4;                   // MMAs per 128-byte K slab (32 B each)
@@ -258,55 +365,139 @@ __global__ void __launch_bounds__(THREADS, 1)
     float* stg = epi_stage + e * 32 * kStagePitch;
     int acc = 0;
     uint32_t aph = 0;
+    // Routed launches: each warp's route windows of a tile (one per 32-column
+    // chunk it writes) are copied into its staging buffer asynchronously one
+    // tile ahead (two buffers), the window bounds two tiles ahead, and the
+    // next tile's row and column classes one tile ahead, so no table load
+    // sits between a tile's accumulator and its stores.
+    constexpr int NCH = TBN / 32 / (EPI_WARPS / 4);  // 32-column chunks per warp
+    const bool routed_launch = sizeof(OutT) == 4 && rt.win != nullptr;
+    DevRoute* wbuf = reinterpret_cast<DevRoute*>(stg);  // [2 buffers][NCH chunks][kWin records]
+    const int step = static_cast<int>(gridDim.x);
+    int par = 0;
+    int2 tw0[NCH], tw1[NCH], tw2[NCH];
+    int2 ri_n = make_int2(-1, 0), cu_n[NCH];
+    auto win_of = [&](int t, int j) -> int2 {
+      return t < n_tiles ? rt.win[static_cast<int64_t>(t) * 16 + q * 4 + (e / 4) + (EPI_WARPS / 4) * j] : make_int2(0, 0);
+    };
+    auto copy_windows = [&](const int2 (&w)[NCH], int buf) {
+#pragma unroll
+      for (int j = 0; j < NCH; ++j)
+        if (lane < w[j].y && w[j].y <= kWin) {
+          const DevRoute* src = rt.routes + w[j].x + lane;
+          DevRoute* dst = wbuf + (buf * NCH + j) * kWin + lane;
+          cp_async16(dst, src);
+          cp_async16(reinterpret_cast<uint8_t*>(dst) + 16, reinterpret_cast<const uint8_t*>(src) + 16);
+        }
+      cp_async_commit();
+    };
+    auto classes_of = [&](int t, const DevGroup& gg, const DevTile& tt) {
+      // this lane's row class and the chunk units' column classes (lane u < 4: unit u)
+      const int row = tt.mt * TBM + r_in_tile;
+      ri_n = (t < n_tiles && gg.routed && row < gg.M) ? rt.rows[gg.rowoff0 + row] : make_int2(-1, 0);
+#pragma unroll
+      for (int j = 0; j < NCH; ++j) {
+        const int col = tt.nt * TBN + 32 * (e / 4) + 32 * (EPI_WARPS / 4) * j + 8 * (lane & 3);
+        cu_n[j] = (t < n_tiles && gg.routed && col < gg.N) ? rt.cols[gg.cinfo0 + col / 8] : make_int2(-1, 0);
+      }
+    };
+    if (routed_launch && static_cast<int>(blockIdx.x) < n_tiles) {
+#pragma unroll
+      for (int j = 0; j < NCH; ++j) {
+        tw0[j] = win_of(blockIdx.x, j);
+        tw1[j] = win_of(blockIdx.x + step, j);
+        tw2[j] = win_of(blockIdx.x + 2 * step, j);
+      }
+      copy_windows(tw0, 0);
+      const DevTile t0 = tiles[blockIdx.x];
+      classes_of(blockIdx.x, groups[t0.g], t0);
+    }
     for (TileIter it(tiles, groups, n_tiles, blockIdx.x); it.t < n_tiles; it.advance()) {
       it.prefetch();
       const DevTile tl = it.tl;
       const DevGroup g = it.g;
       if constexpr (sizeof(OutT) == 4) {
-        if (g.routed) {
-          // routed rows (b, c): each row's d values go to the destinations
-          // of its b, scaled by their weights, 8 d per aligned chunk; the
-          // route range does not depend on the accumulator
-          const int row = tl.mt * TBM + r_in_tile;
-          int cc = 0;
-          int2 rr = make_int2(0, 0);
-          if (row < g.M) {
-            const int bb = row / g.mc;
-            cc = row - bb * g.mc;
-            rr = route_rng[g.route0 + bb];
+        if (g.routed && routed_launch) {
+          // Routed rows: lane = row (b, c) of this lane quarter; its row class
+          // and the chunk units' column classes select the routes of the
+          // tile's window that apply, each written per 8-column unit.
+          const int2 ri = ri_n;
+          int2 cu[NCH];
+#pragma unroll
+          for (int j = 0; j < NCH; ++j) cu[j] = cu_n[j];
+          int2 tw[NCH];
+#pragma unroll
+          for (int j = 0; j < NCH; ++j) tw[j] = tw0[j];
+          // the next tile: its windows into the other buffer, its classes,
+          // and the window bounds one tile further
+          copy_windows(tw1, par ^ 1);
+          if (it.t + step < n_tiles) classes_of(it.t + step, it.g1, it.tl1);
+#pragma unroll
+          for (int j = 0; j < NCH; ++j) {
+            tw0[j] = tw1[j];
+            tw1[j] = tw2[j];
+            tw2[j] = win_of(it.t + 3 * step, j);
           }
+          cp_async_wait_prior();  // this tile's windows have landed
+          __syncwarp();
           if (!wait_or_abort(&tfull[acc], aph, abort_flag, err_flag)) break;
           tc_fence_after();
           const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * TBN);
-          const int d_tile = tl.nt * TBN;
-#pragma unroll 1
-          for (int c0 = c_begin; c0 < c_begin + kColsPerWarp; c0 += 32) {
-            if (d_tile + c0 >= g.md) break;  // warp-uniform: no valid d left
+#pragma unroll
+          for (int j = 0; j < NCH; ++j) {
+            const int c0 = 32 * (e / 4) + 32 * (EPI_WARPS / 4) * j;
+            if (tl.nt * TBN + c0 >= g.N || tw[j].y == 0) continue;  // warp-uniform: nothing to write
+            int ucc[4], ud[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              ucc[u] = __shfl_sync(0xffffffffu, cu[j].x, u);
+              ud[u] = __shfl_sync(0xffffffffu, cu[j].y, u);
+            }
             uint32_t v[32];
             tmem_ld32(tbase + c0, v);
+            // each unit's image form once: a power-of-two weight scales it exactly
+            uint32_t hv[4][4], lw[4][4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              float xu[kMpoVec];
+#pragma unroll
+              for (int t = 0; t < kMpoVec; ++t) xu[t] = __uint_as_float(v[8 * u + t]);
+              img_units<TF32>(xu, hv[u], lw[u]);
+            }
+            const DevRoute* wr = wbuf + (par * NCH + j) * kWin;
+            const bool in_smem = tw[j].y <= kWin;  // warp-uniform
 #pragma unroll 1
-            for (int r = rr.x; r < rr.x + rr.y; ++r) {
-              const DevRoute R = routes[r];
+            for (int r = 0; r < tw[j].y; ++r) {
+              const DevRoute R = in_smem ? wr[r] : rt.routes[tw[j].x + r];
+              if (R.rc != ri.x) continue;
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
-                const int d0 = d_tile + c0 + 8 * u;
-                if (d0 >= g.md) break;
-                float x[kMpoVec];
-#pragma unroll
-                for (int e = 0; e < kMpoVec; ++e) x[e] = __uint_as_float(v[8 * u + e]) * R.w;
-                if (R.kind == 0) {
-                  img_store_chunk<TF32 ? IMG_TF32 : IMG_BF16, float>(
-                      reinterpret_cast<uint8_t*>(R.addr), R.lo_off, R.nKt,
-                      static_cast<int64_t>(R.row0) + static_cast<int64_t>(cc) * R.rstride, R.k0 + d0, x);
-                } else {
+                if (ucc[u] != R.cc) continue;
+                if (R.kind == 1) {
                   float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(R.addr) +
-                                                          static_cast<int64_t>(cc) * R.rstride + d0);
-                  dst[0] = make_float4(x[0], x[1], x[2], x[3]);
-                  dst[1] = make_float4(x[4], x[5], x[6], x[7]);
+                                                          static_cast<int64_t>(ri.y) * R.rstride + ud[u]);
+                  dst[0] = make_float4(__uint_as_float(v[8 * u]) * R.w, __uint_as_float(v[8 * u + 1]) * R.w,
+                                       __uint_as_float(v[8 * u + 2]) * R.w, __uint_as_float(v[8 * u + 3]) * R.w);
+                  dst[1] = make_float4(__uint_as_float(v[8 * u + 4]) * R.w, __uint_as_float(v[8 * u + 5]) * R.w,
+                                       __uint_as_float(v[8 * u + 6]) * R.w, __uint_as_float(v[8 * u + 7]) * R.w);
+                  continue;
+                }
+                const int64_t irow = static_cast<int64_t>(R.row0) + static_cast<int64_t>(ri.y) * R.rstride;
+                uint8_t* img = reinterpret_cast<uint8_t*>(R.addr) + img_row_base(R.nKt, irow);
+                const int key = static_cast<int>(irow & 7);
+                if (R.kind == 2) {
+                  img_store_units<TF32>(img, rt.lo_off, key, R.k0 + ud[u], hv[u], lw[u], R.w);
+                } else {
+                  float x[kMpoVec];
+#pragma unroll
+                  for (int t = 0; t < kMpoVec; ++t) x[t] = __uint_as_float(v[8 * u + t]) * R.w;
+                  img_row_chunk<TF32>(img, rt.lo_off, key, R.k0 + ud[u], x);
                 }
               }
             }
           }
+          __syncwarp();  // this buffer is rewritten two tiles later
+          par ^= 1;
           tc_fence_before();
           mbar_arrive(&tempty[acc]);
           if (++acc == NACC) {
@@ -394,6 +585,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       }
     }
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");  // no route copy outlives the CTA
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
@@ -406,7 +598,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 template <bool TF32, typename OutT>
 void launch_tc_impl(const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
                     const uint64_t* out_tab, int32_t* err_flag, const int32_t* skip, cudaStream_t st,
-                    const DevRoute* routes, const int2* route_rng) {
+                    const DevRouteTabs& rt) {
   constexpr int NT = TF32 ? 2 : 4;
   constexpr int STAGES = TF32 ? 6 : 3;
   const int smem = STAGES * NT * TILE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + kEpiStageBytes;
@@ -416,24 +608,24 @@ void launch_tc_impl(const DevGroup* groups, const DevTile* tiles, int n_tiles, c
   int grid = device_sm_count();
   if (grid > n_tiles) grid = n_tiles;
   gemm_tc_kernel<TF32, OutT>
-      <<<grid, THREADS, smem, st>>>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, routes, route_rng);
+      <<<grid, THREADS, smem, st>>>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, rt);
 }
 }  // namespace
 
 void launch_gemm_tc(int mode, const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
                     const uint64_t* out_tab, bool out_f64, int32_t* err_flag, const int32_t* skip, cudaStream_t st,
-                    const DevRoute* routes, const int2* route_rng) {
+                    const DevRouteTabs& rt) {
   if (n_tiles <= 0) return;
   if (mode == IMG_TF32) {
     if (out_f64)
-      launch_tc_impl<true, double>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, routes, route_rng);
+      launch_tc_impl<true, double>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
     else
-      launch_tc_impl<true, float>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, routes, route_rng);
+      launch_tc_impl<true, float>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
   } else {
     if (out_f64)
-      launch_tc_impl<false, double>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, routes, route_rng);
+      launch_tc_impl<false, double>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
     else
-      launch_tc_impl<false, float>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, routes, route_rng);
+      launch_tc_impl<false, float>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
   }
 }
 

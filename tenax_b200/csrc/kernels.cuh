@@ -62,11 +62,10 @@ void launch_renorm_adjoint(const RenormArgs& a, int nt, double eps, const double
 void launch_gemm_f64(const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
                      const uint64_t* out_tab, const int32_t* skip, cudaStream_t st);
 // tcgen05 grouped GEMM; mode IMG_BF16 (3 products over hi/lo images) or IMG_TF32.
-// routes / route_rng: the routed groups' destinations (FP32 results only; null
-// when no group is routed)
+// rt: the routed groups' tables (FP32 results only; empty when no group is routed)
 void launch_gemm_tc(int mode, const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
                     const uint64_t* out_tab, bool out_f64, int32_t* err_flag, const int32_t* skip, cudaStream_t st,
-                    const DevRoute* routes = nullptr, const int2* route_rng = nullptr);
+                    const DevRouteTabs& rt = DevRouteTabs{});
 int device_sm_count();
 // fused H_eff stages 1-3 (tcgen05, mode IMG_BF16 or IMG_TF32): X3 image from theta and L panels
 void launch_heff_fused(int mode, const DevFPair* pairs, const DevFBlock* blocks, const int32_t* term_begin,
