@@ -171,11 +171,15 @@ int tnx_heff_create_for(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, 
  * stage-4 operand directly (no X1 in HBM), wherever the structure fits (at
  * most 48 input slots per sector pair, every pair's blocks side by side in
  * 256 accumulator columns); c_per_tile c values per tile, 0 = the largest
- * that fits.  fuse_mpo = 0: stage-1 GEMM, X1 in HBM, MPO kernel.  Takes
- * effect at the next tnx_heff_set_operators; FP64 operators always run
- * unfused.  tnx_heff_get_schedule reports the schedule in effect (fuse_mpo =
- * 1 only if the operator runs fused); before tnx_heff_set_operators, the one
- * the precision given to tnx_heff_create_for would get (host planning only). */
+ * that fits.  fuse_mpo = 2 (routed): the stage-1 GEMM's epilogue writes
+ * every W_l W_r output with a single term straight into the stage-4 operand
+ * and keeps X1 only for the input slots that multi-term outputs read, which
+ * the MPO kernel then forms; results equal the unfused schedule's bit for
+ * bit.  fuse_mpo = 0: stage-1 GEMM, X1 in HBM, MPO kernel.  Other values:
+ * TNX_ERR_VALUE.  Takes effect at the next tnx_heff_set_operators; FP64
+ * operators always run unfused.  tnx_heff_get_schedule reports the schedule
+ * in effect; before tnx_heff_set_operators, the one the precision given to
+ * tnx_heff_create_for would get (host planning only). */
 typedef struct tnx_heff_schedule {
   int32_t fuse_mpo;
   int32_t c_per_tile;
@@ -195,7 +199,7 @@ void tnx_heff_destroy(tnx_heff* h);
 
 /* Many independent H_eff problems applied in one launch per stage
  * (persistent grouped GEMMs over all sectors of all problems).  The
- * operators of one batch must all run fused stages 1-3 or all unfused
+ * operators of one batch must all run the same schedule of stages 1-3
  * (tnx_heff_get_schedule); otherwise TNX_ERR_VALUE. */
 int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx_heff_batch** b);
 int tnx_heff_batch_apply(tnx_heff_batch* b, const double* const* thetas, double* const* outs, void* stream);
