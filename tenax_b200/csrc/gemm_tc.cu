@@ -130,9 +130,21 @@ static __device__ __forceinline__ void img_store_units(uint8_t* img, int64_t lo_
 
 // route records of one 32-column chunk's window a warp's staging buffer holds
 // (two buffers of NCH windows); larger windows are read from global memory
-constexpr int kWin = 32;
-static_assert(2 * (TBN / 32 / (EPI_WARPS / 4)) * kWin * 32 <= 32 * kStagePitch * 4,
-              "route windows fit the warp's staging buffer");
+constexpr int kWin = 64;
+
+template <bool TF32, bool ROUTED>
+__host__ __device__ constexpr int gemm_tc_stages() {
+  return ROUTED ? (TF32 ? 4 : 2) : (TF32 ? 6 : 3);
+}
+// dynamic shared memory: operand ring, alignment slack, barriers, per
+// epilogue warp a 32 x 33 FP32 staging buffer and (routed) two route windows
+template <bool TF32, bool ROUTED>
+constexpr int gemm_tc_smem() {
+  return gemm_tc_stages<TF32, ROUTED>() * (TF32 ? 2 : 4) * TILE_BYTES + 1024 + 256 + kEpiStageBytes +
+         (ROUTED ? EPI_WARPS * 2 * (TBN / 32 / (EPI_WARPS / 4)) * kWin * static_cast<int>(sizeof(DevRoute)) : 0);
+}
+static_assert(gemm_tc_smem<false, false>() <= 232448 && gemm_tc_smem<false, true>() <= 232448 &&
+                  gemm_tc_smem<true, true>() <= 232448, "fits 227 KB of shared memory");
 
 // 16-byte asynchronous copy global -> shared (L2 only), its group commit and
 // the wait for every group but the most recent one
@@ -182,13 +194,17 @@ static __device__ __forceinline__ void img_row_chunk(uint8_t* img, int64_t lo_of
   }
 }
 
-template <bool TF32, typename OutT>
+// ROUTED: the H_eff stage-1 instance whose groups all carry destinations per
+// row class (DevRouteTabs); it runs a 2-stage operand ring (stage 1 is
+// short-K) so that each epilogue warp also holds a transpose buffer and two
+// route windows in shared memory.
+template <bool TF32, typename OutT, bool ROUTED>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_tc_kernel(const DevGroup* __restrict__ groups, const DevTile* __restrict__ tiles, int n_tiles,
                    const int64_t* __restrict__ rowoff, const uint64_t* __restrict__ out_tab, int32_t* err_flag,
                    const int32_t* __restrict__ skip, const DevRouteTabs rt) {
   constexpr int NT = TF32 ? 2 : 4;          // operand tiles per stage
-  constexpr int STAGES = TF32 ? 6 : 3;      // 192 KB of operand ring either way
+  constexpr int STAGES = gemm_tc_stages<TF32, ROUTED>();  // 192 KB of operand ring (128 KB routed)
   constexpr int KSUB = 4;                   // MMAs per 128-byte K slab (32 B each)
   if (skip && *skip) return;
 
@@ -371,8 +387,9 @@ __global__ void __launch_bounds__(THREADS, 1)
     // next tile's row and column classes one tile ahead, so no table load
     // sits between a tile's accumulator and its stores.
     constexpr int NCH = TBN / 32 / (EPI_WARPS / 4);  // 32-column chunks per warp
-    const bool routed_launch = sizeof(OutT) == 4 && rt.win != nullptr;
-    DevRoute* wbuf = reinterpret_cast<DevRoute*>(stg);  // [2 buffers][NCH chunks][kWin records]
+    constexpr bool routed_launch = ROUTED;
+    // [2 buffers][NCH chunks][kWin records], after every warp's transpose buffer
+    DevRoute* wbuf = reinterpret_cast<DevRoute*>(epi_stage + EPI_WARPS * 32 * kStagePitch) + e * 2 * NCH * kWin;
     const int step = static_cast<int>(gridDim.x);
     int par = 0;
     int2 tw0[NCH], tw1[NCH], tw2[NCH];
@@ -383,12 +400,13 @@ __global__ void __launch_bounds__(THREADS, 1)
     auto copy_windows = [&](const int2 (&w)[NCH], int buf) {
 #pragma unroll
       for (int j = 0; j < NCH; ++j)
-        if (lane < w[j].y && w[j].y <= kWin) {
-          const DevRoute* src = rt.routes + w[j].x + lane;
-          DevRoute* dst = wbuf + (buf * NCH + j) * kWin + lane;
-          cp_async16(dst, src);
-          cp_async16(reinterpret_cast<uint8_t*>(dst) + 16, reinterpret_cast<const uint8_t*>(src) + 16);
-        }
+        if (w[j].y <= kWin)
+          for (int k = lane; k < w[j].y; k += 32) {
+            const DevRoute* src = rt.routes + w[j].x + k;
+            DevRoute* dst = wbuf + (buf * NCH + j) * kWin + k;
+            cp_async16(dst, src);
+            cp_async16(reinterpret_cast<uint8_t*>(dst) + 16, reinterpret_cast<const uint8_t*>(src) + 16);
+          }
       cp_async_commit();
     };
     auto classes_of = [&](int t, const DevGroup& gg, const DevTile& tt) {
@@ -418,16 +436,26 @@ __global__ void __launch_bounds__(THREADS, 1)
       const DevGroup g = it.g;
       if constexpr (sizeof(OutT) == 4) {
         if (g.routed && routed_launch) {
-          // Routed rows: lane = row (b, c) of this lane quarter; its row class
-          // and the chunk units' column classes select the routes of the
-          // tile's window that apply, each written per 8-column unit.
+          // Routed rows (b, c): the lane quarter's 32 rows, 32-column chunks.
+          // A chunk is staged through shared memory so that each lane then
+          // holds its 8-column unit (lane % 4) of four rows (lane / 4 + 8 i)
+          // and the four lanes of a quad write one row's 32 columns: every
+          // store instruction fills whole 32-byte sectors of 8 rows.  A row's
+          // row class and a unit's column class select the routes of the
+          // tile's window that apply.
           const int2 ri = ri_n;
-          int2 cu[NCH];
+          int2 cu[NCH], tw[NCH];
 #pragma unroll
-          for (int j = 0; j < NCH; ++j) cu[j] = cu_n[j];
-          int2 tw[NCH];
+          for (int j = 0; j < NCH; ++j) {
+            cu[j] = cu_n[j];
+            tw[j] = tw0[j];
+          }
+          int rcl[4], crow[4];
 #pragma unroll
-          for (int j = 0; j < NCH; ++j) tw[j] = tw0[j];
+          for (int i = 0; i < 4; ++i) {
+            rcl[i] = __shfl_sync(0xffffffffu, ri.x, (lane >> 2) + 8 * i);
+            crow[i] = __shfl_sync(0xffffffffu, ri.y, (lane >> 2) + 8 * i);
+          }
           // the next tile: its windows into the other buffer, its classes,
           // and the window bounds one tile further
           copy_windows(tw1, par ^ 1);
@@ -447,56 +475,51 @@ __global__ void __launch_bounds__(THREADS, 1)
           for (int j = 0; j < NCH; ++j) {
             const int c0 = 32 * (e / 4) + 32 * (EPI_WARPS / 4) * j;
             if (tl.nt * TBN + c0 >= g.N || tw[j].y == 0) continue;  // warp-uniform: nothing to write
-            int ucc[4], ud[4];
+            {
+              uint32_t v[32];
+              tmem_ld32(tbase + c0, v);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              ucc[u] = __shfl_sync(0xffffffffu, cu[j].x, u);
-              ud[u] = __shfl_sync(0xffffffffu, cu[j].y, u);
+              for (int t = 0; t < 32; ++t) stg[lane * kStagePitch + t] = __uint_as_float(v[t]);
             }
-            uint32_t v[32];
-            tmem_ld32(tbase + c0, v);
-            // each unit's image form once: a power-of-two weight scales it exactly
-            uint32_t hv[4][4], lw[4][4];
+            __syncwarp();
+            float xv[4][kMpoVec];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              float xu[kMpoVec];
+            for (int i = 0; i < 4; ++i)
 #pragma unroll
-              for (int t = 0; t < kMpoVec; ++t) xu[t] = __uint_as_float(v[8 * u + t]);
-              img_units<TF32>(xu, hv[u], lw[u]);
-            }
-            const DevRoute* wr = wbuf + (par * NCH + j) * kWin;
+              for (int t = 0; t < kMpoVec; ++t) xv[i][t] = stg[((lane >> 2) + 8 * i) * kStagePitch + 8 * (lane & 3) + t];
+            __syncwarp();  // the staging buffer is free for the next chunk
+            const int ccl = cu[j].x, dl = cu[j].y;  // this lane's unit: column class, d
+            DevRoute* wr = wbuf + (par * NCH + j) * kWin;
             const bool in_smem = tw[j].y <= kWin;  // warp-uniform
 #pragma unroll 1
             for (int r = 0; r < tw[j].y; ++r) {
-              const DevRoute R = in_smem ? wr[r] : rt.routes[tw[j].x + r];
-              if (R.rc != ri.x) continue;
+              if (!in_smem && r % kWin == 0) {
+                // a window larger than the buffer: the next kWin records, copied in by the warp
+                __syncwarp();
+                for (int k = lane; k < kWin && r + k < tw[j].y; k += 32) wr[k] = rt.routes[tw[j].x + r + k];
+                __syncwarp();
+              }
+              const DevRoute R = wr[r % kWin];
+              if (R.cc != ccl) continue;
 #pragma unroll
-              for (int u = 0; u < 4; ++u) {
-                if (ucc[u] != R.cc) continue;
+              for (int i = 0; i < 4; ++i) {
+                if (R.rc != rcl[i]) continue;
+                float x[kMpoVec];
+#pragma unroll
+                for (int t = 0; t < kMpoVec; ++t) x[t] = xv[i][t] * R.w;
+                const int64_t irow = static_cast<int64_t>(R.row0) + static_cast<int64_t>(crow[i]) * R.rstride;
                 if (R.kind == 1) {
-                  float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(R.addr) +
-                                                          static_cast<int64_t>(ri.y) * R.rstride + ud[u]);
-                  dst[0] = make_float4(__uint_as_float(v[8 * u]) * R.w, __uint_as_float(v[8 * u + 1]) * R.w,
-                                       __uint_as_float(v[8 * u + 2]) * R.w, __uint_as_float(v[8 * u + 3]) * R.w);
-                  dst[1] = make_float4(__uint_as_float(v[8 * u + 4]) * R.w, __uint_as_float(v[8 * u + 5]) * R.w,
-                                       __uint_as_float(v[8 * u + 6]) * R.w, __uint_as_float(v[8 * u + 7]) * R.w);
-                  continue;
-                }
-                const int64_t irow = static_cast<int64_t>(R.row0) + static_cast<int64_t>(ri.y) * R.rstride;
-                uint8_t* img = reinterpret_cast<uint8_t*>(R.addr) + img_row_base(R.nKt, irow);
-                const int key = static_cast<int>(irow & 7);
-                if (R.kind == 2) {
-                  img_store_units<TF32>(img, rt.lo_off, key, R.k0 + ud[u], hv[u], lw[u], R.w);
+                  float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(R.addr) + irow - R.row0 + dl);
+                  dst[0] = make_float4(x[0], x[1], x[2], x[3]);
+                  dst[1] = make_float4(x[4], x[5], x[6], x[7]);
                 } else {
-                  float x[kMpoVec];
-#pragma unroll
-                  for (int t = 0; t < kMpoVec; ++t) x[t] = __uint_as_float(v[8 * u + t]) * R.w;
-                  img_row_chunk<TF32>(img, rt.lo_off, key, R.k0 + ud[u], x);
+                  img_row_chunk<TF32>(reinterpret_cast<uint8_t*>(R.addr) + img_row_base(R.nKt, irow), rt.lo_off,
+                                      static_cast<int>(irow & 7), R.k0 + dl, x);
                 }
               }
             }
           }
-          __syncwarp();  // this buffer is rewritten two tiles later
+          __syncwarp();  // this window buffer is rewritten two tiles later
           par ^= 1;
           tc_fence_before();
           mbar_arrive(&tempty[acc]);
@@ -595,19 +618,17 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
 }
 
-template <bool TF32, typename OutT>
+template <bool TF32, typename OutT, bool ROUTED>
 void launch_tc_impl(const DevGroup* groups, const DevTile* tiles, int n_tiles, const int64_t* rowoff,
                     const uint64_t* out_tab, int32_t* err_flag, const int32_t* skip, cudaStream_t st,
                     const DevRouteTabs& rt) {
-  constexpr int NT = TF32 ? 2 : 4;
-  constexpr int STAGES = TF32 ? 6 : 3;
-  const int smem = STAGES * NT * TILE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + kEpiStageBytes;
-  if (cudaFuncSetAttribute(gemm_tc_kernel<TF32, OutT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+  constexpr int smem = gemm_tc_smem<TF32, ROUTED>();
+  if (cudaFuncSetAttribute(gemm_tc_kernel<TF32, OutT, ROUTED>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
       cudaSuccess)
     return;  // the thread's last CUDA error, checked by every caller
   int grid = device_sm_count();
   if (grid > n_tiles) grid = n_tiles;
-  gemm_tc_kernel<TF32, OutT>
+  gemm_tc_kernel<TF32, OutT, ROUTED>
       <<<grid, THREADS, smem, st>>>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, rt);
 }
 }  // namespace
@@ -616,16 +637,21 @@ void launch_gemm_tc(int mode, const DevGroup* groups, const DevTile* tiles, int 
                     const uint64_t* out_tab, bool out_f64, int32_t* err_flag, const int32_t* skip, cudaStream_t st,
                     const DevRouteTabs& rt) {
   if (n_tiles <= 0) return;
+  const bool routed = rt.win != nullptr;  // every group routed, FP32 results
   if (mode == IMG_TF32) {
     if (out_f64)
-      launch_tc_impl<true, double>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
+      launch_tc_impl<true, double, false>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
+    else if (routed)
+      launch_tc_impl<true, float, true>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
     else
-      launch_tc_impl<true, float>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
+      launch_tc_impl<true, float, false>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
   } else {
     if (out_f64)
-      launch_tc_impl<false, double>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
+      launch_tc_impl<false, double, false>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
+    else if (routed)
+      launch_tc_impl<false, float, true>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
     else
-      launch_tc_impl<false, float>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
+      launch_tc_impl<false, float, false>(groups, tiles, n_tiles, rowoff, out_tab, err_flag, skip, st, rt);
   }
 }
 
