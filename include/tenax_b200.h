@@ -176,8 +176,9 @@ int tnx_heff_create_for(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, 
  * and keeps X1 only for the input slots that multi-term outputs read, which
  * the MPO kernel then forms; results equal the unfused schedule's bit for
  * bit.  fuse_mpo = 0: stage-1 GEMM, X1 in HBM, MPO kernel.  Other values:
- * TNX_ERR_VALUE.  Takes effect at the next tnx_heff_set_operators; FP64
- * operators always run unfused.  tnx_heff_get_schedule reports the schedule
+ * TNX_ERR_VALUE.  An operator given no schedule runs routed when its
+ * stage FLOPs (tnx_heff_flops) reach 5e9, unfused below.  Takes effect at the
+ * next tnx_heff_set_operators; FP64 operators always run unfused.  tnx_heff_get_schedule reports the schedule
  * in effect; before tnx_heff_set_operators, the one the precision given to
  * tnx_heff_create_for would get (host planning only). */
 typedef struct tnx_heff_schedule {
@@ -199,8 +200,9 @@ void tnx_heff_destroy(tnx_heff* h);
 
 /* Many independent H_eff problems applied in one launch per stage
  * (persistent grouped GEMMs over all sectors of all problems).  The
- * operators of one batch must all run the same schedule of stages 1-3
- * (tnx_heff_get_schedule); otherwise TNX_ERR_VALUE. */
+ * operators of one batch must all run fused stages 1-3 or none of them
+ * (tnx_heff_get_schedule); otherwise TNX_ERR_VALUE.  Routed and unfused
+ * operators mix freely. */
 int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx_heff_batch** b);
 int tnx_heff_batch_apply(tnx_heff_batch* b, const double* const* thetas, double* const* outs, void* stream);
 /* Host-resident streaming (no counterpart in the reference, which applies one

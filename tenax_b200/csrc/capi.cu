@@ -1124,8 +1124,15 @@ extern "C" {
 // ---------------------------------------------------------------------------
 // H_eff
 // ---------------------------------------------------------------------------
-// default of tnx_heff_schedule.fuse_mpo for mixed-precision operators
-constexpr int32_t kDefaultFuse = 0;
+// Schedule of an operator that was given none: routed stages 1-3 for the
+// mixed precisions at or above kRoutedMinFlops (on the cylinder MPO the routed
+// epilogue gains from chi ~ 1024 on, where sectors are wide enough that a
+// warp's rows share one destination list), the three kernels below it.
+constexpr int32_t kAutoFuse = -1;
+constexpr double kRoutedMinFlops = 5e9;
+static int32_t resolved_fuse(int32_t fuse, double flops) {
+  return fuse != kAutoFuse ? fuse : (flops >= kRoutedMinFlops ? 2 : 0);
+}
 
 struct tnx_heff {
   HeffPlan H;
@@ -1136,7 +1143,7 @@ struct tnx_heff {
   bool terms_ready = false;
   double out_scale = 1.0;  // 2^(eL + eR): undoes the operator range scaling
   // schedule requested by tnx_heff_set_schedule, applied by tnx_heff_set_operators
-  int32_t sched_fuse = kDefaultFuse, sched_cc = 0;
+  int32_t sched_fuse = kAutoFuse, sched_cc = 0;
   int32_t plan_prec = TNX_PREC_FP64;  // precision given to tnx_heff_create_for
   // fused stages 1-3 (mixed precisions): layout and L panels (hi plane, then lo)
   bool fused = false;
@@ -1188,12 +1195,13 @@ int tnx_heff_get_schedule(const tnx_heff* h, tnx_heff_schedule* sched) {
       const int mode = img_mode_of(h->plan_prec);
       bool fz = false, rt = false;
       int32_t cc = 0;
-      if (mode != IMG_F64 && h->sched_fuse == 1 && h->H.closed && h->H.s4_separable) {
+      const int32_t fz_req = resolved_fuse(h->sched_fuse, h->H.flops);
+      if (mode != IMG_F64 && fz_req == 1 && h->H.closed && h->H.s4_separable) {
         const FusedLayout fl = fused_layout(h->H, mode, h->sched_cc);
         fz = fl.why_not.empty();
         cc = fl.cc;
       }
-      if (mode != IMG_F64 && h->sched_fuse == 2 && h->H.closed && h->H.s4_separable) rt = true;
+      if (mode != IMG_F64 && fz_req == 2 && h->H.closed && h->H.s4_separable) rt = true;
       sched->fuse_mpo = fz ? 1 : (rt ? 2 : 0);
       sched->c_per_tile = fz ? cc : 0;
       return TNX_OK;
@@ -1248,7 +1256,8 @@ int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const
     // fused stages 1-3 where the schedule asks for it and the structure fits
     h->fused = false;
     h->fl = FusedLayout{};
-    if (mode != IMG_F64 && h->sched_fuse == 1) {
+    const int32_t fz_req = resolved_fuse(h->sched_fuse, H.flops);
+    if (mode != IMG_F64 && fz_req == 1) {
       h->fl = fused_layout(H, mode, h->sched_cc);
       for (auto& mp : H.pairs)
         if (mp.terms.size() > static_cast<size_t>(kFusedMaxTerms))
@@ -1257,7 +1266,7 @@ int tnx_heff_set_operators(tnx_heff* h, const double* L, const double* Wl, const
     }
     h->routed = false;
     h->rl = RoutedLayout{};
-    if (mode != IMG_F64 && h->sched_fuse == 2) {
+    if (mode != IMG_F64 && fz_req == 2) {
       h->rl = routed_layout(H);
       h->routed = true;
     }
@@ -1417,12 +1426,15 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     const bool f32 = mode != IMG_F64;
     for (int i = 0; i < n; ++i) {
       if (hs[i]->prec != precision) return set_err(TNX_ERR_VALUE, "operators were packed for another precision");
-      if (hs[i]->fused != hs[0]->fused || hs[i]->routed != hs[0]->routed)
-        return set_err(TNX_ERR_VALUE, "operators of one batch must all run the same schedule of stages 1-3");
+      if (hs[i]->fused != hs[0]->fused)
+        return set_err(TNX_ERR_VALUE, "operators of one batch must all run fused stages 1-3 or none");
       b->hs.push_back(hs[i]);
     }
+    // routed and unfused operators share a batch: one stage-1 launch holds
+    // both kinds of groups, the MPO tables are per problem
     b->fused = hs[0]->fused;
-    b->routed = hs[0]->routed;
+    b->routed = false;
+    for (int i = 0; i < n; ++i) b->routed = b->routed || hs[i]->routed;
     for (int i = 0; i < n; ++i) {
       b->th_off.push_back(b->th_total);
       b->th_total += hs[i]->H.th.total;
@@ -1438,7 +1450,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
       x1_0[i] = x1_elems;
       th_tiles += hs[i]->g1.b_tiles;
       x3_tiles += hs[i]->g4.a_tiles;
-      if (rt) {
+      if (hs[i]->routed) {
         // X1 of the kept input slots only: (c, d) with d padded to kMpoKAlign
         for (size_t pi = 0; pi < H.pairs.size(); ++pi) {
           const int64_t md_pad = (H.pairs[pi].md + kMpoKAlign - 1) / kMpoKAlign * kMpoKAlign;
@@ -1500,6 +1512,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
     std::vector<int2> RG;  // routed groups: (first RB entry, column classes)
     for (int i = 0; i < n; ++i) {
       tnx_heff* h = hs[i];
+      const bool rti = h->routed;
       std::vector<RoutedEntry> rents;
       const HeffPlan& H = h->H;
       // theta pack: source slot i, images into the batch theta buffer
@@ -1581,7 +1594,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         x.kk_last = kk_last_of(H.s1.groups[g].K, b->mode);
         x.out_slot = 0;
         x.scale = 1.0;
-        if (rt) {
+        if (rti) {
           // row and 8-column-unit classes, filled with the MPO tables below
           x.routed = 1;
           x.rowoff0 = static_cast<int64_t>(RI.size());
@@ -1598,6 +1611,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         xo += H.s1.groups[g].M * ld;
         G1.push_back(x);
       }
+      RG.resize(G1.size(), make_int2(0, 1));
       std::vector<std::pair<int64_t, DevTile>> tl;
       build_tiles(H.s1, h->g1, g1base, tl);
       T1.insert(T1.end(), tl.begin(), tl.end());
@@ -1634,7 +1648,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         const int32_t md_pad = (mp.md + kMpoKAlign - 1) / kMpoKAlign * kMpoKAlign;
         std::vector<MpoTerm> terms;
         for (const MpoTerm& t : mp.terms)
-          if (!rt || h->rl.out_terms[pi][t.out_slot] > 1) terms.push_back(t);
+          if (!rti || h->rl.out_terms[pi][t.out_slot] > 1) terms.push_back(t);
         DevMpoPair dp{};
         dp.mc = mp.mc;
         dp.md = mp.md;
@@ -1651,7 +1665,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
                                                        mp.n_out_slots * sizeof(DevMpoOutSlot));
         // X1 columns of one (p,q) slot: its d range padded to H.x1_align
         const int64_t md_x1 = (mp.md + H.x1_align - 1) / H.x1_align * H.x1_align;
-        for (int32_t sl = 0; sl < mp.n_in_slots && rt; ++sl) {
+        for (int32_t sl = 0; sl < mp.n_in_slots && rti; ++sl) {
           // kept slots: X1 rows (c, d), d padded to kMpoKAlign; the others are never read
           DevMpoSlot r{};
           r.base = x1_base;
@@ -1664,7 +1678,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
           }
           MI.push_back(r);
         }
-        for (size_t k = 0; k < mp.ins.size() && !rt; ++k) {
+        for (size_t k = 0; k < mp.ins.size() && !rti; ++k) {
           // one record per input slot (b,p,q): address of its point (c=0, d=0)
           const MpoIn& in = mp.ins[k];
           const int64_t ld = x1_ld(H.s1.groups[in.g1].N);
@@ -1709,7 +1723,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         for (auto& t : terms) MT.push_back({t.out_slot, t.in_slot, t.w});
         const int pair_id = static_cast<int>(MP.size());
         MP.push_back(dp);
-        if (rt) {
+        if (rti) {
           // the destinations of every X1 row (b, c) and (p, q) column range of
           // this pair: the single-term output slots its input slot feeds and,
           // when a multi-term output reads that slot, its kept X1 rows
@@ -1815,7 +1829,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         const int npts = mp.mc * ((mp.md + dpt - 1) / dpt);
         for (int p0 = 0; p0 < npts && dp.n_terms > 0; p0 += ppc) MC.push_back(make_int2(pair_id, p0));
       }
-      if (rt) {
+      if (rti) {
         // classes of each group in row and column order, the rows' and
         // units' classes, and the routes in (row class, column class) order,
         // so that the rows of one warp read one contiguous range of routes
@@ -1902,6 +1916,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
       std::vector<int2> TW(t1.size() * 16, make_int2(0, 0));
       for (size_t t = 0; t < t1.size(); ++t) {
         const DevGroup& g = G1[t1[t].g];
+        if (!g.routed) continue;
         const int2 rg = RG[t1[t].g];
         for (int q = 0; q < 4; ++q)
           for (int ch = 0; ch < 4; ++ch) {

@@ -100,7 +100,9 @@ class HeffOperator:
     epilogue writes every single-term W_l W_r output straight into the
     stage-4 operand and keeps X1 only for the multi-term outputs, which the
     MPO kernel forms, ``{"fuse_mpo": 0}`` the stage-1 GEMM, all of X1 in HBM
-    and the MPO kernel; ``self.schedule`` reports the schedule in effect.  Other structures (``fused`` False) apply
+    and the MPO kernel; with no schedule given, routed from 5e9 stage FLOPs
+    (``self.flops``) on and unfused below.  ``self.schedule`` reports the
+    schedule in effect.  Other structures (``fused`` False) apply
     H_eff through the general unfiltered contraction engine, the
     reference's ``_blockwise_contract`` semantics, one pairwise chain per
     apply: the same result, without the fused kernels."""

@@ -53,9 +53,14 @@ def test_benchmark_structures_plan_fused(chi):
         h = C.c_void_p()
         _capi.check(_capi.LIB.tnx_heff_create_for(*[C.byref(x.desc) for x in hold], _capi.PRECISIONS[prec],
                                                   C.byref(h)))
+        # no schedule given: routed for the mixed precisions from 5e9 stage FLOPs on
+        s = _capi.HeffSchedule()
+        _capi.check(_capi.LIB.tnx_heff_get_schedule(h, C.byref(s)))
+        big = _capi.LIB.tnx_heff_flops(h) >= 5e9
+        assert s.fuse_mpo == (2 if want and big else 0), (chi, prec)
+        assert big == (chi >= 1024), chi
         on = _capi.HeffSchedule(1, 0)
         _capi.check(_capi.LIB.tnx_heff_set_schedule(h, C.byref(on)))
-        s = _capi.HeffSchedule()
         _capi.check(_capi.LIB.tnx_heff_get_schedule(h, C.byref(s)))
         assert s.fuse_mpo == want, (chi, prec)
         assert (s.c_per_tile >= 1) == bool(want)

@@ -167,7 +167,26 @@ def test_fused_batch_equals_individual():
         torch.testing.assert_close(a, b, rtol=0, atol=0)
 
 
-@pytest.mark.parametrize("pair", [(FUSED, UNFUSED), (ROUTED, UNFUSED), (ROUTED, FUSED)])
+def test_routed_and_unfused_share_a_batch():
+    """Routed and unfused operators in one batch (one stage-1 launch with both
+    kinds of groups, MPO tables per problem): bit for bit the single applies."""
+    Wl, Wr = W.cylinder_bulk_w()
+    gen = np.random.default_rng(21)
+    probs = [W.make_heff_problem(c, c, Wl, Wr, gen, n_sectors=10, hi=48) for c in (120, 200, 160)]
+    ops = [_op(p, "bf16x3", s) for p, s in zip(probs, (ROUTED, UNFUSED, ROUTED))]
+    assert [o.schedule["fuse_mpo"] for o in ops] == [2, 0, 2]
+    xs = [embed_in_keys(p.theta, o.keys).data for p, o in zip(probs, ops)]
+    singles = [o.apply(x) for o, x in zip(ops, xs)]
+    batch = tb.HeffBatch(ops)
+    outs = [o.out_like() for o in ops]
+    batch.apply(xs, outs)
+    torch.cuda.synchronize()
+    assert batch.device_error() == 0
+    for a, b in zip(singles, outs):
+        torch.testing.assert_close(a, b, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("pair", [(FUSED, UNFUSED), (ROUTED, FUSED)])
 def test_mixed_schedules_cannot_share_a_batch(pair):
     p = _problem("tiny_sectors")
     a, b = _op(p, "bf16x3", pair[0]), _op(p, "bf16x3", pair[1])
