@@ -227,7 +227,7 @@ def run_ours(args):
             tot_sf += sf
         res = {"ms": ms, "flops": flops, "stage_ms": stage_ms, "stage_flops": tot_sf.tolist(), "err": err,
                "per_problem_flops": [o.flops for o in ops], "launches": batch.launches_per_apply,
-               "schedule": ops[0].schedule}
+               "schedule": _batch_schedule(ops)}
         if with_e2e:
             # end to end through HeffBatch.apply_host: every step copies its
             # inputs in from pinned host memory and its outputs back; step
@@ -280,15 +280,19 @@ def run_ours(args):
     # dominant GEMM stage of the mixed step
     st_ms = rmx["stage_ms"]
     fused = rmx["schedule"]["fuse_mpo"] == 1
-    routed = rmx["schedule"]["fuse_mpo"] == 2
+    routed = rmx["schedule"]["fuse_mpo"] in (2, -1)
     # the fused kernel does stage 1 and the MPO; its tensor work is stage 1's
     gemm = {1: rmx["stage_flops"][0] + (rmx["stage_flops"][1] if fused else 0.0), 3: rmx["stage_flops"][2]}
     dom = max((1, 3), key=lambda s: st_ms[s])
     if fused:
         stage_names = ["pack theta panels", "fused stages 1-3 (L.theta in TMEM, W_l W_r epilogue)",
                        "none (MPO inside the fused kernel)", "stage-4 GEMM .R"]
+    elif routed and rmx["schedule"]["fuse_mpo"] == -1:
+        stage_names = ["pack theta", "stage-1 GEMM L.theta: routed epilogue for the routed problems, X1 for the "
+                       "others", "MPO kernel: multi-term outputs (routed problems), all outputs (the others)",
+                       "stage-4 GEMM .R"]
     elif routed:
-        stage_names = ["pack theta panels", "stage-1 GEMM L.theta, epilogue routes single-term W_l W_r outputs "
+        stage_names = ["pack theta", "stage-1 GEMM L.theta, epilogue routes single-term W_l W_r outputs "
                        "into the stage-4 operand", "MPO kernel: multi-term outputs from the kept X1 slots",
                        "stage-4 GEMM .R"]
     else:
@@ -356,6 +360,15 @@ def bench_config(n_problems, chi_counts, flops_per_step, parallelism):
             "flops_per_step": flops_per_step,
             "flop_count": "block-sparse 4-stage sector GEMM flops from stored block dims",
             "l2": "inputs larger than L2 (operators+theta >> 126 MB); no flush", "parallelism": parallelism}
+
+
+def _batch_schedule(ops) -> dict:
+    """The schedule of a batch's operators; with the automatic schedule
+    (routed from 5e9 FLOPs per operator, unfused below) the count of each."""
+    kinds = [o.schedule["fuse_mpo"] for o in ops]
+    if len(set(kinds)) == 1:
+        return ops[0].schedule
+    return {"fuse_mpo": -1, "c_per_tile": 0, "routed_problems": kinds.count(2), "unfused_problems": kinds.count(0)}
 
 
 def bench_parity(problems, precision, schedule=None):

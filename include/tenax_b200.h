@@ -176,8 +176,9 @@ int tnx_heff_create_for(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, 
  * and keeps X1 only for the input slots that multi-term outputs read, which
  * the MPO kernel then forms; results equal the unfused schedule's bit for
  * bit.  fuse_mpo = 0: stage-1 GEMM, X1 in HBM, MPO kernel.  Other values:
- * TNX_ERR_VALUE.  An operator given no schedule runs routed when its
- * stage FLOPs (tnx_heff_flops) reach 5e9, unfused below.  Takes effect at the
+ * TNX_ERR_VALUE.  fuse_mpo = -1 (automatic, also the schedule of an
+ * operator given none): routed when its stage FLOPs (tnx_heff_flops) reach
+ * 5e9, unfused below.  Takes effect at the
  * next tnx_heff_set_operators; FP64 operators always run unfused.  tnx_heff_get_schedule reports the schedule
  * in effect; before tnx_heff_set_operators, the one the precision given to
  * tnx_heff_create_for would get (host planning only). */

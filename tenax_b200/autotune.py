@@ -47,11 +47,12 @@ def sector_histogram(problems) -> tuple:
 
 
 # the schedules a tuned entry chose among: entries tuned over another set are re-tuned
-SCHEDULE_SET = ("fused", "routed", "unfused")
+SCHEDULE_SET = ("fused", "routed", "auto", "unfused")
 
 
 def schedule_label(s: dict) -> str:
-    return {1: f"fused c={s['c_per_tile']}", 2: "routed"}.get(s["fuse_mpo"], "unfused")
+    return {1: f"fused c={s['c_per_tile']}", 2: "routed", -1: "auto (routed from 5e9 FLOPs)"}.get(s["fuse_mpo"],
+                                                                                                "unfused")
 
 
 def cache_key(problems, precision: str) -> str:
@@ -63,7 +64,8 @@ def cache_key(problems, precision: str) -> str:
 
 def candidates(problems, precision: str) -> list:
     """The fused kernel at the largest c extent that fits, at half of it and
-    at 1, the routed stage-1 epilogue, and the three-kernel path."""
+    at 1, the routed stage-1 epilogue, routed or unfused per operator by its
+    size (-1), and the three-kernel path."""
     p = problems[0]
     probe = HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, precision,
                          schedule={"fuse_mpo": 1, "c_per_tile": 0})
@@ -73,6 +75,7 @@ def candidates(problems, precision: str) -> list:
         for c in sorted({cc, max(1, cc // 2), 1}, reverse=True):
             out.append({"fuse_mpo": 1, "c_per_tile": c})
     out.append({"fuse_mpo": 2, "c_per_tile": 0})
+    out.append({"fuse_mpo": -1, "c_per_tile": 0})
     out.append({"fuse_mpo": 0, "c_per_tile": 0})
     return out
 
@@ -84,7 +87,7 @@ def time_schedule(problems, precision: str, schedule: dict, reps: int = 5, warmu
 
     ops = [HeffOperator(p.L, p.Wl, p.Wr, p.R, p.theta.indices, p.theta.keys, precision, schedule=schedule)
            for p in problems]
-    if len({o.schedule["fuse_mpo"] for o in ops}) != 1:
+    if len({o.schedule["fuse_mpo"] for o in ops}) != 1 and schedule["fuse_mpo"] != -1:
         return float("inf")  # the structure does not take this schedule everywhere
     xs = [embed_in_keys(p.theta, o.keys).data for p, o in zip(problems, ops)]
     ys = [o.out_like() for o in ops]

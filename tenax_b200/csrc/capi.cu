@@ -1181,7 +1181,7 @@ int tnx_heff_create_for(const tnx_tensor_desc* L, const tnx_tensor_desc* theta, 
 int tnx_heff_set_schedule(tnx_heff* h, const tnx_heff_schedule* sched) {
   if (!h || !sched) return set_err(TNX_ERR_VALUE, "null argument");
   if (sched->c_per_tile < 0 || sched->c_per_tile > 32) return set_err(TNX_ERR_VALUE, "c_per_tile must be in [0, 32]");
-  if (sched->fuse_mpo < 0 || sched->fuse_mpo > 2) return set_err(TNX_ERR_VALUE, "fuse_mpo must be 0, 1 or 2");
+  if (sched->fuse_mpo < -1 || sched->fuse_mpo > 2) return set_err(TNX_ERR_VALUE, "fuse_mpo must be -1, 0, 1 or 2");
   h->sched_fuse = sched->fuse_mpo;
   h->sched_cc = sched->c_per_tile;
   return TNX_OK;
