@@ -259,8 +259,9 @@ def run_ours(args):
     # schedule of the mixed stages 1-3: tuned on these problems (autotune.py)
     # unless given on the command line
     tuning = None
-    if args.unfused or args.routed or args.c_per_tile or args.no_tune:
-        schedule = {"fuse_mpo": 0 if args.unfused else (2 if args.routed else 1), "c_per_tile": args.c_per_tile}
+    if args.unfused or args.routed or args.auto or args.c_per_tile or args.no_tune:
+        kind = 0 if args.unfused else 2 if args.routed else -1 if args.auto else 1
+        schedule = {"fuse_mpo": kind, "c_per_tile": args.c_per_tile}
     else:
         from tenax_b200 import autotune
 
@@ -1062,6 +1063,8 @@ def main():
                     help="mixed stages 1-3 as stage-1 GEMM + X1 in HBM + MPO kernel instead of the fused kernel")
     ap.add_argument("--routed", action="store_true",
                     help="mixed stages 1-3 with the routed stage-1 epilogue, without tuning")
+    ap.add_argument("--auto", action="store_true",
+                    help="mixed stages 1-3 routed or unfused per problem by its size, without tuning")
     ap.add_argument("--c-per-tile", type=int, default=0, help="fused kernel: c values per tile (0 = largest that fits)")
     ap.add_argument("--no-tune", action="store_true", help="fused schedule without tuning it")
     ap.add_argument("--mode", default="partition", choices=["partition", "replicas"],
