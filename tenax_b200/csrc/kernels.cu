@@ -296,8 +296,11 @@ __global__ void __launch_bounds__(256) pack_rows_kernel(const uint64_t* __restri
   const int4 ch = chunks[blockIdx.x];  // (segment, first row, first K chunk, -)
   const DevRowPackSeg s = segs[ch.x];
   const int r = ch.y + static_cast<int>(threadIdx.x);
-  if (r >= s.rows) return;
-  const double* src = reinterpret_cast<const double*>(src_tab[s.src_slot]) + s.src_off + r;
+  // BF16 / TF32 CTAs all reach the shared-memory exchange below: a row past
+  // the segment loads zeros and is not stored
+  if (MODE == IMG_F64 && r >= s.rows) return;
+  const int rr = r < s.rows ? r : s.rows - 1;
+  const double* src = reinterpret_cast<const double*>(src_tab[s.src_slot]) + s.src_off + rr;
   uint8_t* img = reinterpret_cast<uint8_t*>(s.img_addr);
   const int nkc = (s.kval + kMpoVec - 1) / kMpoVec;
   ValT v[kChunks][kMpoVec];
@@ -306,11 +309,59 @@ __global__ void __launch_bounds__(256) pack_rows_kernel(const uint64_t* __restri
 #pragma unroll
     for (int u = 0; u < kMpoVec; ++u) {
       const int a = (ch.z + j) * kMpoVec + u;
-      v[j][u] = a < s.kval ? static_cast<ValT>(src[static_cast<int64_t>(a) * s.kstride] * s.scale) : ValT(0);
+      v[j][u] = (a < s.kval && r < s.rows) ? static_cast<ValT>(src[static_cast<int64_t>(a) * s.kstride] * s.scale)
+                                           : ValT(0);
     }
+  if constexpr (MODE == IMG_F64) {
 #pragma unroll
-  for (int j = 0; j < kChunks; ++j)
-    if (ch.z + j < nkc) img_store_chunk<MODE>(img, s.lo_off, s.nKt, s.row0 + r, s.k0 + (ch.z + j) * kMpoVec, v[j]);
+    for (int j = 0; j < kChunks; ++j)
+      if (ch.z + j < nkc) img_store_chunk<MODE>(img, s.lo_off, s.nKt, s.row0 + r, s.k0 + (ch.z + j) * kMpoVec, v[j]);
+  } else {
+    // BF16 / TF32: each row's 4 chunks in their image form go through shared
+    // memory, so that the four lanes of a quad then write one row's 64 bytes
+    // (of each plane) and a store instruction fills whole sectors of 8 rows
+    __shared__ uint4 sh[256 * 9];  // per row: 4 chunks x (hi or first unit, lo or second unit), pitch 9
+#pragma unroll
+    for (int j = 0; j < kChunks; ++j) {
+      uint32_t a[4], b[4];
+      if constexpr (MODE == IMG_BF16) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const __nv_bfloat162 h = __floats2bfloat162_rn(v[j][2 * u], v[j][2 * u + 1]);
+          const __nv_bfloat162 l =
+              __floats2bfloat162_rn(v[j][2 * u] - __low2float(h), v[j][2 * u + 1] - __high2float(h));
+          a[u] = *reinterpret_cast<const uint32_t*>(&h);
+          b[u] = *reinterpret_cast<const uint32_t*>(&l);
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(a[u]) : "f"(v[j][u]));
+          asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(b[u]) : "f"(v[j][4 + u]));
+        }
+      }
+      sh[threadIdx.x * 9 + 2 * j] = make_uint4(a[0], a[1], a[2], a[3]);
+      sh[threadIdx.x * 9 + 2 * j + 1] = make_uint4(b[0], b[1], b[2], b[3]);
+    }
+    __syncthreads();
+    const int j = threadIdx.x & 3;  // this thread's chunk
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int rl = (threadIdx.x >> 2) + 64 * i;  // row within the CTA's 256
+      if (ch.y + rl >= s.rows || ch.z + j >= nkc) continue;
+      const int64_t row = s.row0 + ch.y + rl;
+      const int64_t k = s.k0 + (ch.z + j) * kMpoVec;
+      const uint4 x0 = sh[rl * 9 + 2 * j], x1 = sh[rl * 9 + 2 * j + 1];
+      if constexpr (MODE == IMG_BF16) {
+        const int64_t off = img_byte_offset(MODE, 0, s.nKt, row, k);
+        *reinterpret_cast<uint4*>(img + off) = x0;
+        *reinterpret_cast<uint4*>(img + s.lo_off + off) = x1;
+      } else {
+        *reinterpret_cast<uint4*>(img + img_byte_offset(MODE, 0, s.nKt, row, k)) = x0;
+        *reinterpret_cast<uint4*>(img + img_byte_offset(MODE, 0, s.nKt, row, k + 4)) = x1;
+      }
+    }
+  }
 }
 
 void launch_pack_rows(const uint64_t* src_tab, const DevRowPackSeg* segs, const int4* chunks, int n_chunks, int mode,
