@@ -1751,10 +1751,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
                     r.rstride = os.rows_per_c;
                     r.k0 = os.k0 + os.k_add;
                     r.w = static_cast<float>(ow.second);
-                    // a power-of-two weight rescales the row's image form exactly
-                    int ex = 0;
-                    const double mant = std::frexp(std::fabs(ow.second), &ex);
-                    r.kind = static_cast<uint8_t>((mant == 0.5 && ex >= -20 && ex <= 21) ? 2 : 0);
+                    r.kind = 0;
                     e.routes.push_back(r);
                   }
                   if (h->rl.in_kept[pi][sl]) {

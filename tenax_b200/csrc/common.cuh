@@ -133,13 +133,13 @@ struct DevGroup {
 };
 
 // One destination of the routed stage-1 rows of one (row class, column class)
-// pair: kinds 0 and 2 write w * row into the stage-4 operand image at image
-// row row0 + c * rstride, K k0 + d (8 d per aligned unit, the image's own
-// precision split; kind 2: w is a power of two, applied to the split form,
-// which gives the same bits); kind 1 writes w * row in FP32 at
+// pair: kind 0 writes w * row (rounded to FP32, as the MPO kernel computes a
+// single-term output) into the stage-4 operand image at image row
+// row0 + c * rstride, K k0 + d (8 d per aligned unit, the image's own
+// precision split); kind 1 writes w * row in FP32 at
 // addr + (c * rstride + d) * 4.  32 bytes: two 16-byte asynchronous copies.
 struct DevRoute {
-  uint64_t addr;     // kinds 0, 2: image tile 0; kind 1: element (c = 0, d = 0)
+  uint64_t addr;     // kind 0: image tile 0; kind 1: element (c = 0, d = 0)
   int32_t row0, rstride, k0;
   float w;
   uint16_t nKt;
@@ -150,7 +150,7 @@ static_assert(sizeof(DevRoute) == 32, "route records are two 16-byte units");
 
 // The routed epilogue's tables (see DevGroup and DevRoute).
 struct DevRouteTabs {
-  int64_t lo_off;    // byte offset of the low-part stage-4 image (kinds 0, 2)
+  int64_t lo_off;    // byte offset of the low-part stage-4 image (kind 0)
   const DevRoute* routes;
   const int2* win;   // per (tile, lane quarter, 32-column chunk): (first route, count)
   const int2* rows;  // (row class, c) per group row; class -1: no destinations

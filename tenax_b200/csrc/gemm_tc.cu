@@ -74,88 +74,6 @@ struct TileIter {
 constexpr int kStagePitch = 33;  // fp32 words per staged row (+1 breaks bank conflicts)
 constexpr int kEpiStageBytes = EPI_WARPS * 32 * kStagePitch * 4;
 
-// 8 values in their image form: BF16 -> four hi and four lo bf16x2 words
-// (split as the packing kernels split); TF32 -> two units of four TF32 words
-// (hi[0..3] then lo[0..3] hold the eight values).
-template <bool TF32>
-static __device__ __forceinline__ void img_units(const float (&v)[kMpoVec], uint32_t (&hi)[4], uint32_t (&lo)[4]) {
-  if constexpr (TF32) {
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi[u]) : "f"(v[u]));
-      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo[u]) : "f"(v[4 + u]));
-    }
-  } else {
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * u], v[2 * u + 1]);
-      const __nv_bfloat162 l = __floats2bfloat162_rn(v[2 * u] - __low2float(h), v[2 * u + 1] - __high2float(h));
-      hi[u] = *reinterpret_cast<const uint32_t*>(&h);
-      lo[u] = *reinterpret_cast<const uint32_t*>(&l);
-    }
-  }
-}
-
-// Image units from img_units scaled by a power of two w (exact: the image
-// form of w * v), stored at K k (a multiple of 8) of the row at `img`.
-template <bool TF32>
-static __device__ __forceinline__ void img_store_units(uint8_t* img, int64_t lo_off, int key, int k,
-                                                       const uint32_t (&hi)[4], const uint32_t (&lo)[4], float w) {
-  if constexpr (TF32) {
-    const int j = (k >> 2) & 7;
-    uint8_t* t = img + static_cast<int64_t>(k >> 5) * TILE_BYTES;
-    uint32_t a[4], b[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      a[u] = __float_as_uint(__uint_as_float(hi[u]) * w);
-      b[u] = __float_as_uint(__uint_as_float(lo[u]) * w);
-    }
-    *reinterpret_cast<uint4*>(t + ((j ^ key) << 4)) = make_uint4(a[0], a[1], a[2], a[3]);
-    *reinterpret_cast<uint4*>(t + (((j + 1) ^ key) << 4)) = make_uint4(b[0], b[1], b[2], b[3]);
-  } else {
-    const __nv_bfloat162 w2 = __float2bfloat162_rn(w);
-    uint32_t a[4], b[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const __nv_bfloat162 h = __hmul2(*reinterpret_cast<const __nv_bfloat162*>(&hi[u]), w2);
-      const __nv_bfloat162 l = __hmul2(*reinterpret_cast<const __nv_bfloat162*>(&lo[u]), w2);
-      a[u] = *reinterpret_cast<const uint32_t*>(&h);
-      b[u] = *reinterpret_cast<const uint32_t*>(&l);
-    }
-    uint8_t* t = img + static_cast<int64_t>(k >> 6) * TILE_BYTES + ((((k >> 3) & 7) ^ key) << 4);
-    *reinterpret_cast<uint4*>(t) = make_uint4(a[0], a[1], a[2], a[3]);
-    *reinterpret_cast<uint4*>(t + lo_off) = make_uint4(b[0], b[1], b[2], b[3]);
-  }
-}
-
-// route records of one 32-column chunk's window a warp's staging buffer holds
-// (two buffers of NCH windows); larger windows are read from global memory
-constexpr int kWin = 64;
-
-template <bool TF32, bool ROUTED>
-__host__ __device__ constexpr int gemm_tc_stages() {
-  return ROUTED ? (TF32 ? 4 : 2) : (TF32 ? 6 : 3);
-}
-// dynamic shared memory: operand ring, alignment slack, barriers, per
-// epilogue warp a 32 x 33 FP32 staging buffer and (routed) two route windows
-template <bool TF32, bool ROUTED>
-constexpr int gemm_tc_smem() {
-  return gemm_tc_stages<TF32, ROUTED>() * (TF32 ? 2 : 4) * TILE_BYTES + 1024 + 256 + kEpiStageBytes +
-         (ROUTED ? EPI_WARPS * 2 * (TBN / 32 / (EPI_WARPS / 4)) * kWin * static_cast<int>(sizeof(DevRoute)) : 0);
-}
-static_assert(gemm_tc_smem<false, false>() <= 232448 && gemm_tc_smem<false, true>() <= 232448 &&
-                  gemm_tc_smem<true, true>() <= 232448, "fits 227 KB of shared memory");
-
-// 16-byte asynchronous copy global -> shared (L2 only), its group commit and
-// the wait for every group but the most recent one
-static __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
-}
-static __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-static __device__ __forceinline__ void cp_async_wait_prior() {
-  asm volatile("cp.async.wait_group 1;" ::: "memory");
-}
-
 // Byte offset of the start of row `row` in an operand image of nKt K tiles
 // (16 KB tiles of 128 rows x 128 bytes, SWIZZLE_128B: the 16-byte unit j of
 // a row sits at unit j ^ (row & 7)).
