@@ -74,6 +74,34 @@ struct TileIter {
 constexpr int kStagePitch = 33;  // fp32 words per staged row (+1 breaks bank conflicts)
 constexpr int kEpiStageBytes = EPI_WARPS * 32 * kStagePitch * 4;
 
+// route records of one 32-column chunk's window a warp's staging buffer holds
+// (two buffers of NCH windows); larger windows are read from global memory
+constexpr int kWin = 64;
+
+template <bool TF32, bool ROUTED>
+__host__ __device__ constexpr int gemm_tc_stages() {
+  return ROUTED ? (TF32 ? 4 : 2) : (TF32 ? 6 : 3);
+}
+// dynamic shared memory: operand ring, alignment slack, barriers, per
+// epilogue warp a 32 x 33 FP32 staging buffer and (routed) two route windows
+template <bool TF32, bool ROUTED>
+constexpr int gemm_tc_smem() {
+  return gemm_tc_stages<TF32, ROUTED>() * (TF32 ? 2 : 4) * TILE_BYTES + 1024 + 256 + kEpiStageBytes +
+         (ROUTED ? EPI_WARPS * 2 * (TBN / 32 / (EPI_WARPS / 4)) * kWin * static_cast<int>(sizeof(DevRoute)) : 0);
+}
+static_assert(gemm_tc_smem<false, false>() <= 232448 && gemm_tc_smem<false, true>() <= 232448 &&
+                  gemm_tc_smem<true, true>() <= 232448, "fits 227 KB of shared memory");
+
+// 16-byte asynchronous copy global -> shared (L2 only), its group commit and
+// the wait for every group but the most recent one
+static __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
+}
+static __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+static __device__ __forceinline__ void cp_async_wait_prior() {
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+
 // Byte offset of the start of row `row` in an operand image of nKt K tiles
 // (16 KB tiles of 128 rows x 128 bytes, SWIZZLE_128B: the 16-byte unit j of
 // a row sits at unit j ^ (row & 7)).
