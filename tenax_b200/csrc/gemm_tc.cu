@@ -152,6 +152,10 @@ __global__ void __launch_bounds__(THREADS, 1)
   constexpr int NT = TF32 ? 2 : 4;          // operand tiles per stage
   constexpr int STAGES = gemm_tc_stages<TF32, ROUTED>();  // 192 KB of operand ring (128 KB routed)
   constexpr int KSUB = 4;                   // MMAs per 128-byte K slab (32 B each)
+  // TMEM accumulators: the routed instance runs 4 (all 512 columns), so the
+  // MMAs run up to three tiles ahead of its longer epilogue
+  constexpr int NACC = ROUTED ? 4 : ::tnx::NACC;
+  constexpr int TMEM_COLS = NACC * TBN;
   if (skip && *skip) return;
 
   extern __shared__ uint8_t smem_raw[];
