@@ -1547,7 +1547,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
         const int id = static_cast<int>(trs.size());
         trs.push_back(rs);
         const int nkc = (rs.kval + kMpoKAlign - 1) / kMpoKAlign, cpt = pack_rows_chunks_per_thread();
-        for (int r0 = 0; r0 < rs.rows; r0 += 256)
+        for (int r0 = 0; r0 < rs.rows; r0 += pack_rows_per_cta())
           for (int kc = 0; kc < nkc; kc += cpt) trc.push_back(make_int4(id, r0, kc, 0));
       }
       if (fz) {
@@ -1571,7 +1571,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
           const int id = static_cast<int>(fth.size());
           fth.push_back(rs);
           const int nkc = (rs.kval + kMpoKAlign - 1) / kMpoKAlign, cpt = pack_rows_chunks_per_thread();
-          for (int r0 = 0; r0 < rs.rows; r0 += 256)
+          for (int r0 = 0; r0 < rs.rows; r0 += pack_rows_per_cta())
             for (int kc = 0; kc < nkc; kc += cpt) fthc.push_back(make_int4(id, r0, kc, 0));
         }
       }

@@ -285,8 +285,11 @@ __global__ void __launch_bounds__(kMpoThreads) mpo_apply_point_kernel(
 // row pack: k-major blocks with contiguous rows (theta of the H_eff stage 1)
 // -> operand image, 8 consecutive k per thread and store (see DevRowPackSeg)
 // ---------------------------------------------------------------------------
+// rows per CTA: small theta slices (a few rows of d) leave fewer threads idle than 256
+constexpr int kPackRows = 128;
+
 template <int MODE>
-__global__ void __launch_bounds__(256) pack_rows_kernel(const uint64_t* __restrict__ src_tab,
+__global__ void __launch_bounds__(kPackRows) pack_rows_kernel(const uint64_t* __restrict__ src_tab,
                                                         const DevRowPackSeg* __restrict__ segs,
                                                         const int4* __restrict__ chunks,
                                                         const int32_t* __restrict__ skip) {
@@ -320,7 +323,7 @@ __global__ void __launch_bounds__(256) pack_rows_kernel(const uint64_t* __restri
     // BF16 / TF32: each row's 4 chunks in their image form go through shared
     // memory, so that the four lanes of a quad then write one row's 64 bytes
     // (of each plane) and a store instruction fills whole sectors of 8 rows
-    __shared__ uint4 sh[256 * 9];  // per row: 4 chunks x (hi or first unit, lo or second unit), pitch 9
+    __shared__ uint4 sh[kPackRows * 9];  // per row: 4 chunks x (hi or first unit, lo or second unit), pitch 9
 #pragma unroll
     for (int j = 0; j < kChunks; ++j) {
       uint32_t a[4], b[4];
@@ -347,7 +350,7 @@ __global__ void __launch_bounds__(256) pack_rows_kernel(const uint64_t* __restri
     const int j = threadIdx.x & 3;  // this thread's chunk
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const int rl = (threadIdx.x >> 2) + 64 * i;  // row within the CTA's 256
+      const int rl = (threadIdx.x >> 2) + (kPackRows / 4) * i;  // row within the CTA's kPackRows
       if (ch.y + rl >= s.rows || ch.z + j >= nkc) continue;
       const int64_t row = s.row0 + ch.y + rl;
       const int64_t k = s.k0 + (ch.z + j) * kMpoVec;
@@ -368,11 +371,11 @@ void launch_pack_rows(const uint64_t* src_tab, const DevRowPackSeg* segs, const 
                       const int32_t* skip, cudaStream_t st) {
   if (n_chunks <= 0) return;
   if (mode == IMG_F64)
-    pack_rows_kernel<IMG_F64><<<n_chunks, 256, 0, st>>>(src_tab, segs, chunks, skip);
+    pack_rows_kernel<IMG_F64><<<n_chunks, kPackRows, 0, st>>>(src_tab, segs, chunks, skip);
   else if (mode == IMG_BF16)
-    pack_rows_kernel<IMG_BF16><<<n_chunks, 256, 0, st>>>(src_tab, segs, chunks, skip);
+    pack_rows_kernel<IMG_BF16><<<n_chunks, kPackRows, 0, st>>>(src_tab, segs, chunks, skip);
   else
-    pack_rows_kernel<IMG_TF32><<<n_chunks, 256, 0, st>>>(src_tab, segs, chunks, skip);
+    pack_rows_kernel<IMG_TF32><<<n_chunks, kPackRows, 0, st>>>(src_tab, segs, chunks, skip);
 }
 
 void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevMpoSlot* islots,
@@ -394,6 +397,8 @@ void launch_mpo_apply(bool x1_f32, int mode, const DevMpoPair* pairs, const DevM
 }
 
 int mpo_points_per_cta() { return kMpoThreads; }
+int pack_rows_per_cta() { return kPackRows; }
+
 int pack_rows_chunks_per_thread() { return 4; }
 int mpo_d_per_thread(int mode) { return mode == IMG_F64 ? 1 : kMpoVec; }
 

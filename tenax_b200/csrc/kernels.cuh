@@ -10,11 +10,12 @@ namespace tnx {
 
 void launch_pack(const uint64_t* src_tab, const DevPackSeg* segs, const DevChunk* chunks, int n_chunks, int mode,
                  const int32_t* skip, cudaStream_t st);
-// chunks: (segment, first row, first 8-wide K chunk, -): 256 rows x pack_rows_chunks_per_thread()
+// chunks: (segment, first row, first 8-wide K chunk, -): pack_rows_per_cta() rows x pack_rows_chunks_per_thread()
 // K chunks each; K blocks of the image start at multiples of 8
 void launch_pack_rows(const uint64_t* src_tab, const DevRowPackSeg* segs, const int4* chunks, int n_chunks, int mode,
                       const int32_t* skip, cudaStream_t st);
 int pack_rows_chunks_per_thread();
+int pack_rows_per_cta();  // rows of one chunk
 // chunks: seg = pointer-table slot, [start, start+count) elements set to 0
 void launch_zero_ranges(const uint64_t* out_tab, const DevChunk* chunks, int n_chunks, const int32_t* skip,
                         cudaStream_t st);
