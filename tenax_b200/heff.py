@@ -170,7 +170,12 @@ class HeffOperator:
 
 
 class HeffBatch:
-    """Independent H_eff problems applied together: one launch per stage."""
+    """Independent H_eff problems applied together: one launch per stage.
+
+    Operators on the routed and the unfused schedule share a batch (one
+    stage-1 launch holds both kinds of groups, the MPO tables are per
+    problem); operators on the fused schedule cannot be mixed with the
+    others (ValueError)."""
 
     def __init__(self, ops, skip_flag: torch.Tensor | None = None):
         self.ops = list(ops)
