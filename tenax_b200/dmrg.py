@@ -11,7 +11,7 @@ SVD (linalg.py:75-333) with cuSOLVER per charge sector.
 from __future__ import annotations
 
 import time
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 from typing import NamedTuple
 
 import numpy as np
@@ -64,6 +64,12 @@ class DMRGConfig:
     svd_streams: int = 8
     # run each Krylov loop of a fused H_eff as one captured CUDA graph
     cuda_graph: bool = False
+    # schedule of the mixed-precision H_eff stages 1-3 (HeffOperator's
+    # ``schedule``).  A sweep builds one operator per site and applies it a
+    # few dozen times, so the three-kernel schedule, whose tables are the
+    # cheapest to build on the host, is the default; None takes the
+    # operator's automatic choice (routed from 5e9 stage FLOPs on).
+    heff_schedule: dict | None = field(default_factory=lambda: {"fuse_mpo": 0, "c_per_tile": 0})
 
 
 NOISE_REL = {"fp64": 0.0, "bf16x3": 1e-5, "tf32": 2e-3}
@@ -545,7 +551,8 @@ def two_site_update(site_l, site_r, L, Wl, Wr, R, config, stats: list | None = N
         else:
             theta = _pad(theta, False)
     t1 = _tick(phases, "theta", t0)
-    op = HeffOperator(L, Wl, Wr, R, theta.indices, theta.keys, config.precision)
+    op = HeffOperator(L, Wl, Wr, R, theta.indices, theta.keys, config.precision,
+                      schedule=None if config.precision == "fp64" else config.heff_schedule)
     fp64 = {}
 
     def make_fp64():
