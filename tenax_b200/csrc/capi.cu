@@ -1877,6 +1877,10 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
             r.cc = static_cast<uint8_t>(o[3] & 255);
             // every (c, d) of the entry lands inside the X3 image or the kept X1 slots
             const int64_t last = static_cast<int64_t>(e.mc - 1) * r.rstride;
+            // the epilogue forms row indices and tile indices in 32 bits
+            if (r.row0 + last + e.md_pad >= (int64_t{1} << 31) ||
+                cdiv(r.row0 + last + 1, 128) * static_cast<int64_t>(r.nKt) >= (int64_t{1} << 32))
+              return set_err(TNX_ERR_UNSUPPORTED, "a routed destination exceeds 32-bit row indexing");
             if (r.kind != 1) {
               const uint64_t end = r.addr + static_cast<uint64_t>(cdiv(r.row0 + last + 1, 128) * r.nKt) * ig.tile_bytes;
               if (r.addr < x3_base || end > x3_base + static_cast<uint64_t>(x3_tiles) * ig.tile_bytes ||

@@ -102,39 +102,67 @@ static __device__ __forceinline__ void cp_async_wait_prior() {
   asm volatile("cp.async.wait_group 1;" ::: "memory");
 }
 
-// Byte offset of the start of row `row` in an operand image of nKt K tiles
-// (16 KB tiles of 128 rows x 128 bytes, SWIZZLE_128B: the 16-byte unit j of
-// a row sits at unit j ^ (row & 7)).
-static __device__ __forceinline__ int64_t img_row_base(int nKt, int64_t row) {
-  return (row >> 7) * static_cast<int64_t>(nKt) * TILE_BYTES + (row & 127) * 128;
+// Packed FP32 pairs (sm_100a f32x2): one instruction rounds both lanes of the
+// pair exactly as the scalar .rn operation rounds each of them.
+static __device__ __forceinline__ uint64_t f2_pack(uint32_t lo, uint32_t hi) {
+  uint64_t d;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "r"(lo), "r"(hi));
+  return d;
+}
+static __device__ __forceinline__ void f2_unpack(uint64_t a, uint32_t& lo, uint32_t& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=r"(lo), "=r"(hi) : "l"(a));
+}
+static __device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+static __device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
 }
 
-// 8 consecutive K (k a multiple of 8) of one image row whose start is `img`
-// and swizzle key `key`: a 16-byte unit of the hi and of the lo BF16 images
-// (split as the packing kernels split), or two units of TF32.
+// The routed epilogue's store of 8 consecutive K (k a multiple of 8) of image
+// row `irow` of the stage-4 image at `img` (16 KB tiles of 128 rows x 128
+// bytes, nKt K tiles per 128-row band, SWIZZLE_128B: the 16-byte unit j of a
+// row sits at unit j ^ (row & 7)), from 4 packed FP32 pairs: split BF16 hi and lo units (split as the
+// packing kernels split), or two TF32 units.  Tile index and in-tile offset
+// are formed in 32 bits (the host checks that the route's rows and tiles fit).
 template <bool TF32>
-static __device__ __forceinline__ void img_row_chunk(uint8_t* img, int64_t lo_off, int key, int k,
-                                                     const float (&v)[kMpoVec]) {
+static __device__ __forceinline__ void route_store(uint8_t* img, int64_t lo_off, int irow, int nKt, int k,
+                                                   const uint64_t (&x)[4]) {
+  static_assert(TILE_BYTES == (1 << 14) && TBM == 128, "tile offsets are formed by shifts");
   if constexpr (TF32) {
+    const uint32_t tile = static_cast<uint32_t>(irow >> 7) * static_cast<uint32_t>(nKt) + static_cast<uint32_t>(k >> 5);
+    uint8_t* row = img + ((static_cast<uint64_t>(tile) << 14) | (static_cast<uint32_t>(irow & 127) << 7));
     const int j = (k >> 2) & 7;
-    uint8_t* t = img + static_cast<int64_t>(k >> 5) * TILE_BYTES;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      uint32_t w[4];
+      uint32_t f[4], w[4];
+      f2_unpack(x[2 * h], f[0], f[1]);
+      f2_unpack(x[2 * h + 1], f[2], f[3]);
 #pragma unroll
-      for (int u = 0; u < 4; ++u) asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(w[u]) : "f"(v[4 * h + u]));
-      *reinterpret_cast<uint4*>(t + (((j + h) ^ key) << 4)) = make_uint4(w[0], w[1], w[2], w[3]);
+      for (int u = 0; u < 4; ++u) asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(w[u]) : "f"(__uint_as_float(f[u])));
+      *reinterpret_cast<uint4*>(row + ((static_cast<uint32_t>((j + h) ^ irow) & 7u) << 4)) =
+          make_uint4(w[0], w[1], w[2], w[3]);
     }
   } else {
+    const uint32_t tile = static_cast<uint32_t>(irow >> 7) * static_cast<uint32_t>(nKt) + static_cast<uint32_t>(k >> 6);
+    const uint32_t low = (static_cast<uint32_t>(irow & 127) << 7) | ((static_cast<uint32_t>((k >> 3) ^ irow) & 7u) << 4);
+    uint8_t* t = img + ((static_cast<uint64_t>(tile) << 14) | low);
     uint32_t hi[4], lo[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * u], v[2 * u + 1]);
-      const __nv_bfloat162 l = __floats2bfloat162_rn(v[2 * u] - __low2float(h), v[2 * u + 1] - __high2float(h));
+      uint32_t a, b;
+      f2_unpack(x[u], a, b);
+      const __nv_bfloat162 h = __floats2bfloat162_rn(__uint_as_float(a), __uint_as_float(b));
       hi[u] = *reinterpret_cast<const uint32_t*>(&h);
+      // x - hi, both lanes in one instruction (hi's BF16 halves widened exactly)
+      f2_unpack(f2_sub(x[u], f2_pack(hi[u] << 16, hi[u] & 0xffff0000u)), a, b);
+      const __nv_bfloat162 l = __floats2bfloat162_rn(__uint_as_float(a), __uint_as_float(b));
       lo[u] = *reinterpret_cast<const uint32_t*>(&l);
     }
-    uint8_t* t = img + static_cast<int64_t>(k >> 6) * TILE_BYTES + ((((k >> 3) & 7) ^ key) << 4);
     *reinterpret_cast<uint4*>(t) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
     *reinterpret_cast<uint4*>(t + lo_off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
   }
@@ -425,18 +453,27 @@ __global__ void __launch_bounds__(THREADS, 1)
           for (int j = 0; j < NCH; ++j) {
             const int c0 = 32 * (e / 4) + 32 * (EPI_WARPS / 4) * j;
             if (tl.nt * TBN + c0 >= g.N || tw[j].y == 0) continue;  // warp-uniform: nothing to write
+            // the chunk in shared memory as 32 rows of 8 16-byte units, unit c
+            // of row r at r * 8 + (c ^ (r & 7)): the row-per-lane writes and
+            // the quad-per-row reads are both free of bank conflicts
+            uint4* s4 = reinterpret_cast<uint4*>(stg);
             {
               uint32_t v[32];
               tmem_ld32(tbase + c0, v);
 #pragma unroll
-              for (int t = 0; t < 32; ++t) stg[lane * kStagePitch + t] = __uint_as_float(v[t]);
+              for (int c = 0; c < 8; ++c)
+                s4[lane * 8 + (c ^ (lane & 7))] = make_uint4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
             }
             __syncwarp();
-            float xv[4][kMpoVec];
+            uint64_t xv[4][kMpoVec / 2];  // rows lane / 4 + 8 i: the unit's 8 columns as packed pairs
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-              for (int t = 0; t < kMpoVec; ++t) xv[i][t] = stg[((lane >> 2) + 8 * i) * kStagePitch + 8 * (lane & 3) + t];
+              for (int h = 0; h < 2; ++h) {
+                const uint4 u = s4[((lane >> 2) + 8 * i) * 8 + ((2 * (lane & 3) + h) ^ ((lane >> 2) & 7))];
+                xv[i][2 * h] = f2_pack(u.x, u.y);
+                xv[i][2 * h + 1] = f2_pack(u.z, u.w);
+              }
             __syncwarp();  // the staging buffer is free for the next chunk
             const int ccl = cu[j].x, dl = cu[j].y;  // this lane's unit: column class, d
             DevRoute* wr = wbuf + (par * NCH + j) * kWin;
@@ -451,20 +488,25 @@ __global__ void __launch_bounds__(THREADS, 1)
               }
               const DevRoute R = wr[r % kWin];
               if (R.cc != ccl) continue;
+              const uint32_t wb = __float_as_uint(R.w);
+              const uint64_t w2 = f2_pack(wb, wb);
 #pragma unroll
               for (int i = 0; i < 4; ++i) {
                 if (R.rc != rcl[i]) continue;
-                float x[kMpoVec];
+                uint64_t x[kMpoVec / 2];
 #pragma unroll
-                for (int t = 0; t < kMpoVec; ++t) x[t] = xv[i][t] * R.w;
-                const int64_t irow = static_cast<int64_t>(R.row0) + static_cast<int64_t>(crow[i]) * R.rstride;
+                for (int u = 0; u < kMpoVec / 2; ++u) x[u] = f2_mul(xv[i][u], w2);
+                // rows and offsets fit 32 bits (checked when the routes are built)
+                const int rrel = crow[i] * R.rstride;
                 if (R.kind == 1) {
-                  float4* dst = reinterpret_cast<float4*>(reinterpret_cast<float*>(R.addr) + irow - R.row0 + dl);
-                  dst[0] = make_float4(x[0], x[1], x[2], x[3]);
-                  dst[1] = make_float4(x[4], x[5], x[6], x[7]);
+                  uint32_t f[8];
+#pragma unroll
+                  for (int u = 0; u < 4; ++u) f2_unpack(x[u], f[2 * u], f[2 * u + 1]);
+                  uint4* dst = reinterpret_cast<uint4*>(reinterpret_cast<float*>(R.addr) + (rrel + dl));
+                  dst[0] = make_uint4(f[0], f[1], f[2], f[3]);
+                  dst[1] = make_uint4(f[4], f[5], f[6], f[7]);
                 } else {
-                  img_row_chunk<TF32>(reinterpret_cast<uint8_t*>(R.addr) + img_row_base(R.nKt, irow), rt.lo_off,
-                                      static_cast<int>(irow & 7), R.k0 + dl, x);
+                  route_store<TF32>(reinterpret_cast<uint8_t*>(R.addr), rt.lo_off, R.row0 + rrel, R.nKt, R.k0 + dl, x);
                 }
               }
             }
