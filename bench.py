@@ -251,6 +251,18 @@ def run_ours(args):
             batch.apply(xs, ys)
             torch.cuda.synchronize()
             res["e2e_max_abs_diff_vs_device"] = float((host_out[(args.steps - 1) % 2] - y_all.cpu()).abs().max())
+        # every problem of the batched apply against its operator applied alone
+        batch.apply(xs, ys)
+        torch.cuda.synchronize()
+        n_eq, worst = 0, 0.0
+        for o, x, y in zip(ops, xs, ys):
+            y1 = o.apply(x)
+            torch.cuda.synchronize()
+            o.release_scratch()
+            n_eq += int(torch.equal(y1, y))
+            worst = max(worst, float(torch.linalg.norm(y1 - y)) / max(float(torch.linalg.norm(y1)), 1e-300))
+            del y1
+        res["batch_vs_single"] = {"problems": len(ops), "bitwise_equal": n_eq, "max_rel_diff": worst}
         del batch, ops, x_all, y_all, xs, ys
         torch.cuda.empty_cache()
         return res
@@ -337,6 +349,11 @@ def run_ours(args):
         }
         if world == 1:
             out["parity"] = bench_parity(problems, args.precision, rmx["schedule"])
+        # the timed batch's outputs against each operator applied alone (this rank's problems)
+        out.setdefault("parity", {})["batch_vs_single"] = {"fp64": r64["batch_vs_single"],
+                                                           args.precision: rmx["batch_vs_single"]}
+        out["parity"]["ok"] = bool(out["parity"].get("ok", True) and all(
+            v["bitwise_equal"] == v["problems"] for v in out["parity"]["batch_vs_single"].values()))
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(chi_counts, seed=args.seed)
         if world == 1 and not args.no_dmrg:

@@ -412,6 +412,28 @@ __global__ void __launch_bounds__(THREADS, 1)
       it.prefetch();
       const DevTile tl = it.tl;
       const DevGroup g = it.g;
+      // Routed launches advance the window and class pipeline on every tile,
+      // whichever kind of group it belongs to: this tile's classes and
+      // windows were requested a tile ago; request the next tile's.
+      int2 ri = make_int2(-1, 0), cu[NCH], tw[NCH];
+      const int cur_par = par;
+      if constexpr (routed_launch) {
+        ri = ri_n;
+#pragma unroll
+        for (int j = 0; j < NCH; ++j) {
+          cu[j] = cu_n[j];
+          tw[j] = tw0[j];
+        }
+        copy_windows(tw1, par ^ 1);
+        if (it.t + step < n_tiles) classes_of(it.t + step, it.g1, it.tl1);
+#pragma unroll
+        for (int j = 0; j < NCH; ++j) {
+          tw0[j] = tw1[j];
+          tw1[j] = tw2[j];
+          tw2[j] = win_of(it.t + 3 * step, j);
+        }
+        par ^= 1;
+      }
       if constexpr (sizeof(OutT) == 4) {
         if (g.routed && routed_launch) {
           // Routed rows (b, c): the lane quarter's 32 rows, 32-column chunks.
@@ -421,28 +443,11 @@ __global__ void __launch_bounds__(THREADS, 1)
           // store instruction fills whole 32-byte sectors of 8 rows.  A row's
           // row class and a unit's column class select the routes of the
           // tile's window that apply.
-          const int2 ri = ri_n;
-          int2 cu[NCH], tw[NCH];
-#pragma unroll
-          for (int j = 0; j < NCH; ++j) {
-            cu[j] = cu_n[j];
-            tw[j] = tw0[j];
-          }
           int rcl[4], crow[4];
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             rcl[i] = __shfl_sync(0xffffffffu, ri.x, (lane >> 2) + 8 * i);
             crow[i] = __shfl_sync(0xffffffffu, ri.y, (lane >> 2) + 8 * i);
-          }
-          // the next tile: its windows into the other buffer, its classes,
-          // and the window bounds one tile further
-          copy_windows(tw1, par ^ 1);
-          if (it.t + step < n_tiles) classes_of(it.t + step, it.g1, it.tl1);
-#pragma unroll
-          for (int j = 0; j < NCH; ++j) {
-            tw0[j] = tw1[j];
-            tw1[j] = tw2[j];
-            tw2[j] = win_of(it.t + 3 * step, j);
           }
           cp_async_wait_prior();  // this tile's windows have landed
           __syncwarp();
@@ -476,7 +481,7 @@ __global__ void __launch_bounds__(THREADS, 1)
               }
             __syncwarp();  // the staging buffer is free for the next chunk
             const int ccl = cu[j].x, dl = cu[j].y;  // this lane's unit: column class, d
-            DevRoute* wr = wbuf + (par * NCH + j) * kWin;
+            DevRoute* wr = wbuf + (cur_par * NCH + j) * kWin;
             const bool in_smem = tw[j].y <= kWin;  // warp-uniform
 #pragma unroll 1
             for (int r = 0; r < tw[j].y; ++r) {
@@ -511,8 +516,7 @@ __global__ void __launch_bounds__(THREADS, 1)
               }
             }
           }
-          __syncwarp();  // this window buffer is rewritten two tiles later
-          par ^= 1;
+          __syncwarp();  // this window buffer is rewritten by the next tile
           tc_fence_before();
           mbar_arrive(&tempty[acc]);
           if (++acc == NACC) {

@@ -162,6 +162,11 @@ class HeffOperator:
         """The fused kernels' device-side timeout flag (0 on the general path)."""
         return self._batch.device_error() if self._batch is not None else 0
 
+    def release_scratch(self) -> None:
+        """Free the device buffers ``apply`` keeps between calls (its one-operator
+        batch: images and intermediates); the next ``apply`` rebuilds them."""
+        self._batch = None
+
     def __del__(self):
         if getattr(self, "handle", None) is not None and _capi.LIB is not None:
             self._batch = None

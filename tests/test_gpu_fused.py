@@ -186,6 +186,37 @@ def test_routed_and_unfused_share_a_batch():
         torch.testing.assert_close(a, b, rtol=0, atol=0)
 
 
+@pytest.mark.parametrize("precision", ["bf16x3", "tf32"])
+def test_routed_and_unfused_interleaved_tiles(precision):
+    """A mixed batch with thousands of stage-1 tiles, so that every CTA of the
+    persistent launch runs many tiles and routed tiles follow unfused ones
+    (the window and class pipeline must advance on both kinds): bit for bit
+    the single applies, and the automatic schedule gives the same bits."""
+    Wl, Wr = W.cylinder_bulk_w()
+    gen = np.random.default_rng(23)
+    probs = [W.make_heff_problem(c, c, Wl, Wr, gen) for c in (1024, 512, 1024, 384)]
+    scheds = (ROUTED, UNFUSED, ROUTED, UNFUSED)
+    ops = [_op(p, precision, s) for p, s in zip(probs, scheds)]
+    xs = [embed_in_keys(p.theta, o.keys).data for p, o in zip(probs, ops)]
+    singles = [o.apply(x) for o, x in zip(ops, xs)]
+    torch.cuda.synchronize()
+    # the automatic schedule routes the two chi = 1024 operators and runs the others unfused
+    auto = [_op(p, precision, None) for p in probs]
+    assert [o.schedule["fuse_mpo"] for o in auto] == [2, 0, 2, 0]
+    for batch in (tb.HeffBatch(ops), tb.HeffBatch(auto)):
+        outs = [torch.full_like(a, float("nan")) for a in singles]
+        # a first apply on other inputs leaves other values in every intermediate,
+        # so a tile whose stores were skipped cannot pass on stale data
+        batch.apply([-3.0 * x for x in xs], outs)
+        for y in outs:
+            y.fill_(float("nan"))
+        batch.apply(xs, outs)
+        torch.cuda.synchronize()
+        assert batch.device_error() == 0
+        for a, b in zip(singles, outs):
+            torch.testing.assert_close(b, a, rtol=0, atol=0)
+
+
 @pytest.mark.parametrize("pair", [(FUSED, UNFUSED), (ROUTED, FUSED)])
 def test_mixed_schedules_cannot_share_a_batch(pair):
     p = _problem("tiny_sectors")
