@@ -319,7 +319,8 @@ def run_ours(args):
     traffic = None
     tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tp):
-        key = (f"{args.precision}_fused1" if fused and dom == 1 else f"{args.precision}_routed1" if routed and dom == 1
+        sched1 = "auto1" if rmx["schedule"]["fuse_mpo"] == -1 else "routed1"
+        key = (f"{args.precision}_fused1" if fused and dom == 1 else f"{args.precision}_{sched1}" if routed and dom == 1
                else f"{args.precision}_stage{dom}")
         traffic = json.load(open(tp)).get(key)
     if rank == 0:
