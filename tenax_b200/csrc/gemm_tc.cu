@@ -40,7 +40,6 @@ constexpr int THREADS = 64 + 32 * EPI_WARPS;
 #endif
 constexpr int NACC = TNX_TMEM_ACC;
 static_assert(NACC == 2 || NACC == 4, "TMEM accumulators: 2 or 4 (512 columns)");
-constexpr int TMEM_COLS = NACC * TBN;
 // The persistent loop over a CTA's tiles with the descriptors of the next
 // tiles in flight: the group record of tile t+1 and the tile record of t+2
 // are requested while tile t is processed, so no role waits on the
