@@ -227,6 +227,10 @@ int tnx_heff_batch_apply_stage(tnx_heff_batch* b, int32_t stage, void* stream);
 int tnx_heff_stage_flops(const tnx_heff* h, double* flops3);
 /* Number of kernel launches one apply issues (launch accounting). */
 int tnx_heff_batch_launches(const tnx_heff_batch* b, int32_t* n_launches);
+/* Routed stage-1 tables (introspection, no reference counterpart): the number
+ * of route records and the largest window of records one epilogue warp scans
+ * for one 32-column chunk of a tile.  Both 0 when no operator is routed. */
+int tnx_heff_batch_route_stats(const tnx_heff_batch* b, int64_t* n_routes, int32_t* max_window);
 /* Device error flag of the tcgen05 GEMM (non-zero: a bounded wait gave up). */
 int tnx_heff_batch_error(tnx_heff_batch* b, int32_t* err);
 /* Optional device int32 flag: when non-zero, every kernel of an apply returns

@@ -91,6 +91,7 @@ def _load():
         "tnx_heff_batch_apply_host": (C.c_int, [P, P, P, i32, P]),
         "tnx_heff_batch_size": (C.c_int, [P, P, P]),
         "tnx_heff_batch_launches": (C.c_int, [P, P]),
+        "tnx_heff_batch_route_stats": (C.c_int, [P, P, P]),
         "tnx_heff_batch_apply_stage": (C.c_int, [P, i32, P]),
         "tnx_heff_stage_flops": (C.c_int, [P, P]),
         "tnx_heff_batch_error": (C.c_int, [P, P]),
@@ -130,7 +131,7 @@ EXPORTED = [
     "tnx_heff_closed", "tnx_heff_set_schedule", "tnx_heff_get_schedule", "tnx_heff_out_keys", "tnx_heff_flops", "tnx_heff_set_operators", "tnx_heff_destroy",
     "tnx_heff_batch_create", "tnx_heff_batch_apply", "tnx_heff_batch_apply_host", "tnx_heff_batch_size",
     "tnx_heff_batch_apply_stage", "tnx_heff_stage_flops",
-    "tnx_heff_batch_launches", "tnx_heff_batch_error",
+    "tnx_heff_batch_launches", "tnx_heff_batch_route_stats", "tnx_heff_batch_error",
     "tnx_heff_batch_set_skip_flag", "tnx_heff_batch_destroy", "tnx_reduce_scratch_len", "tnx_dot", "tnx_nrm2", "tnx_wait_flag",
     "tnx_svd_batch",
     "tnx_lanczos_step", "tnx_combine", "tnx_scale", "tnx_fuse_plan_create", "tnx_fuse_plan_output",

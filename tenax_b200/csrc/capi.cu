@@ -1386,6 +1386,8 @@ struct tnx_heff_batch {
   // a range of routes) and X1 of the input slots multi-term outputs read
   bool routed = false;
   DevMem routes, route_win, route_rows, route_cols;
+  int64_t n_routes = 0;
+  int32_t route_win_max = 0;  // records in the largest (tile, lane quarter, chunk) window
   const int32_t* skip = nullptr;
   int n_launches = 0;
   std::vector<uint64_t> last_src, last_out;
@@ -1936,7 +1938,10 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
                 }
               }
             }
-            if (hi > lo) TW[t * 16 + q * 4 + ch] = make_int2(lo, hi - lo);
+            if (hi > lo) {
+              TW[t * 16 + q * 4 + ch] = make_int2(lo, hi - lo);
+              b->route_win_max = std::max(b->route_win_max, hi - lo);
+            }
           }
       }
       upload(b->route_win, TW);
@@ -2008,6 +2013,7 @@ int tnx_heff_batch_create(tnx_heff* const* hs, int32_t n, int32_t precision, tnx
       b->n_thp_row_chunks = static_cast<int>(fthc.size());
     }
     if (rt) {
+      b->n_routes = static_cast<int64_t>(RT.size());
       upload(b->routes, RT);
       upload(b->route_rows, RI);
       upload(b->route_cols, CI);
@@ -2036,6 +2042,13 @@ int tnx_heff_batch_set_skip_flag(tnx_heff_batch* b, const int32_t* flag) {
 
 int tnx_heff_batch_launches(const tnx_heff_batch* b, int32_t* n_launches) {
   *n_launches = b->n_launches;
+  return TNX_OK;
+}
+
+int tnx_heff_batch_route_stats(const tnx_heff_batch* b, int64_t* n_routes, int32_t* max_window) {
+  if (!b || !n_routes || !max_window) return set_err(TNX_ERR_VALUE, "null argument");
+  *n_routes = b->n_routes;
+  *max_window = b->route_win_max;
   return TNX_OK;
 }
 

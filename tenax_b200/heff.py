@@ -214,6 +214,14 @@ class HeffBatch:
         op = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
         _capi.check(_capi.LIB.tnx_heff_batch_apply(self.handle, tp, op, torch.cuda.current_stream().cuda_stream))
 
+    def route_stats(self) -> tuple:
+        """(route records, largest window of records one epilogue warp scans
+        for one 32-column chunk of a tile) of the routed stage-1 launch; (0, 0)
+        when no operator is routed."""
+        n, w = C.c_int64(), C.c_int32()
+        _capi.check(_capi.LIB.tnx_heff_batch_route_stats(self.handle, C.byref(n), C.byref(w)))
+        return n.value, w.value
+
     def capture(self, thetas, outs) -> "torch.cuda.CUDAGraph":
         """A CUDA graph of one apply with these buffers: the batch's pointer
         tables are bound by an eager apply first, so the captured apply

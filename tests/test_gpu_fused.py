@@ -107,6 +107,19 @@ def test_routed_matches_unfused_bitwise(case, precision):
     assert _rel({k: v for k, v in got.items() if k in ref}, ref) < TOL[precision]
 
 
+def test_routed_long_windows_are_exercised():
+    """Tiny sectors put many row and column classes under one warp's chunk,
+    so some windows exceed the 64 records a shared-memory window buffer holds
+    and the epilogue reads them in pieces; the bitwise routed-vs-unfused test
+    on this structure therefore covers that path.  Wide sectors keep every
+    window in the buffer."""
+    small = tb.HeffBatch([_op(_problem("tiny_sectors"), "bf16x3", ROUTED)])
+    n, w = small.route_stats()
+    assert n > 0 and w > 64, (n, w)
+    unf = tb.HeffBatch([_op(_problem("tiny_sectors"), "bf16x3", UNFUSED)])
+    assert unf.route_stats() == (0, 0)
+
+
 def test_routed_batch_equals_individual():
     """Three problems of different chi in one routed batch: bit for bit the
     single-problem applies."""
