@@ -193,7 +193,13 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint64_t* tfull = empty + STAGES;
   uint64_t* tempty = tfull + NACC;
   uint64_t* drain = tempty + NACC;
-  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(drain + 1);
+  // split BF16: each stage lands in two halves, the hi planes of A and B on
+  // full[s] and the lo planes on full2[s], so the hi x hi products start
+  // while the lo planes are still in flight
+  uint64_t* full2 = drain + 1;
+  uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(full2 + (TF32 ? 0 : STAGES));
+  static_assert((2 * STAGES + 2 * NACC + 1 + (TF32 ? 0 : STAGES)) * 8 + 8 <= 256,
+                "barriers, TMEM address and abort flag fit the 256 bytes before the epilogue staging");
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
   // epilogue staging: one 32 x 33 fp32 buffer per epilogue warp, after 256 B of barriers
   float* epi_stage = reinterpret_cast<float*>(smem + STAGES * NT * TILE_BYTES + 256);
@@ -202,6 +208,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 1);
+      if (!TF32) mbar_init(&full2[s], 1);
       mbar_init(&empty[s], 1);
     }
     for (int a = 0; a < NACC; ++a) {
@@ -243,15 +250,19 @@ __global__ void __launch_bounds__(THREADS, 1)
             break;
           }
           uint8_t* st = smem + s * NT * TILE_BYTES;
-          mbar_expect_tx(&full[s], NT * TILE_BYTES);
           const int64_t ko = static_cast<int64_t>(kt) * TILE_BYTES;
-          bulk_g2s(st, ga + ko, TILE_BYTES, &full[s]);
           if (TF32) {
+            mbar_expect_tx(&full[s], NT * TILE_BYTES);
+            bulk_g2s(st, ga + ko, TILE_BYTES, &full[s]);
             bulk_g2s(st + TILE_BYTES, gb + ko, TILE_BYTES, &full[s]);
           } else {
-            bulk_g2s(st + TILE_BYTES, ga + g.a_lo + ko, TILE_BYTES, &full[s]);
+            // stage layout [A hi][A lo][B hi][B lo]; hi planes first
+            mbar_expect_tx(&full[s], 2 * TILE_BYTES);
+            bulk_g2s(st, ga + ko, TILE_BYTES, &full[s]);
             bulk_g2s(st + 2 * TILE_BYTES, gb + ko, TILE_BYTES, &full[s]);
-            bulk_g2s(st + 3 * TILE_BYTES, gb + g.b_lo + ko, TILE_BYTES, &full[s]);
+            mbar_expect_tx(&full2[s], 2 * TILE_BYTES);
+            bulk_g2s(st + TILE_BYTES, ga + g.a_lo + ko, TILE_BYTES, &full2[s]);
+            bulk_g2s(st + 3 * TILE_BYTES, gb + g.b_lo + ko, TILE_BYTES, &full2[s]);
           }
           last_par[s] = static_cast<int>(ph);
           if (++s == STAGES) {
@@ -266,6 +277,10 @@ __global__ void __launch_bounds__(THREADS, 1)
           if (last_par[i] < 0) continue;
           uint64_t t0 = gtimer();
           while (!mbar_try_wait(&full[i], static_cast<uint32_t>(last_par[i])) && gtimer() - t0 < kTimeoutNs) {
+          }
+          if (TF32) continue;
+          t0 = gtimer();
+          while (!mbar_try_wait(&full2[i], static_cast<uint32_t>(last_par[i])) && gtimer() - t0 < kTimeoutNs) {
           }
         }
       }
@@ -318,10 +333,21 @@ __global__ void __launch_bounds__(THREADS, 1)
             const uint64_t dal = sw128_desc(sa + TILE_BYTES);
             const uint64_t db = sw128_desc(sa + 2 * TILE_BYTES);
             const uint64_t dbl = sw128_desc(sa + 3 * TILE_BYTES);
+            // hi x hi on the hi planes, then hi x lo and lo x hi once the lo planes land
 #pragma unroll
             for (int kk = 0; kk < KSUB; ++kk) {
               if (kk >= nk) break;
               mma_issue<TF32>(d_tmem, da + 2 * kk, db + 2 * kk, idesc, (kt | kk) ? 1u : 0u);
+            }
+            issued = true;  // an abort below still waits for these MMAs before TMEM is freed
+            if (!wait_or_abort(&full2[s], ph, abort_flag, err_flag)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+#pragma unroll
+            for (int kk = 0; kk < KSUB; ++kk) {
+              if (kk >= nk) break;
               mma_issue<TF32>(d_tmem, da + 2 * kk, dbl + 2 * kk, idesc, 1u);
               mma_issue<TF32>(d_tmem, dal + 2 * kk, db + 2 * kk, idesc, 1u);
             }

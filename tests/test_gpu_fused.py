@@ -5,8 +5,10 @@ against the oracle and against the unfused three-kernel path (stage-1 GEMM,
 X1 in HBM, MPO kernel) on the same inputs.
 
 Tolerances (relative Frobenius error against the oracle): split-BF16x3 2e-5,
-TF32 5e-3; fused against unfused: 1e-6 (BF16x3) and 1e-4 (TF32), since the
-two paths sum the same FP32 products in different orders.  Routed against
+TF32 5e-3; fused against unfused: 2e-6 (BF16x3) and 1e-4 (TF32), since the
+two paths sum the same FP32 products in different orders (the three-kernel
+stage 1 adds a K slab's hi x hi products before its cross products, the
+fused kernel interleaves them; measured up to 1.05e-6 on the 320-wide chain).  Routed against
 unfused: bit for bit (the same operand images, the same MMA K order per
 point, the same FP32 arithmetic for every output slot).
 """
@@ -27,7 +29,7 @@ from tenax_b200 import workloads as W  # noqa: E402
 from tenax_b200.tensor import SymmetricTensor, embed_in_keys  # noqa: E402
 
 TOL = {"bf16x3": 2e-5, "tf32": 5e-3}
-PATH_TOL = {"bf16x3": 1e-6, "tf32": 1e-4}
+PATH_TOL = {"bf16x3": 2e-6, "tf32": 1e-4}
 FUSED = {"fuse_mpo": 1, "c_per_tile": 0}
 UNFUSED = {"fuse_mpo": 0, "c_per_tile": 0}
 ROUTED = {"fuse_mpo": 2, "c_per_tile": 0}
