@@ -109,3 +109,15 @@ def test_sector_histogram_key():
                               Wl=types.SimpleNamespace(indices=(types.SimpleNamespace(charges=np.zeros(26)),)))
     hist, dws = sector_histogram([p])
     assert dict(hist) == {2: 1, 8: 1, 3: 1, 0: 1, 6: 1} and dws == (26,)
+
+
+def test_dram_view_of_the_dominant_kernel():
+    """roofline.dram: measured DRAM bytes per launch over the stage time,
+    against the HBM copy bandwidth; absent without a traffic figure."""
+    b = _bench()
+    v = b._dram_view(7374000000, 2.264, {"hbm_gbs": 6650.0}, "fallback")
+    assert v["unit"] == "GB/s" and v["peak"] == 6650.0
+    assert abs(v["achieved"] - 7374000000 / 2.264e-3 / 1e9) < 0.1
+    assert abs(v["frac"] - v["achieved"] / 6650.0) < 1e-4
+    assert b._dram_view(None, 2.264, {"hbm_gbs": 6650.0}, "fallback") is None
+    assert b._dram_view(7374000000, 2.264, {}, "measured") is None
