@@ -11,9 +11,9 @@ d sector padded to 128, its columns ``c_per_tile`` c values per MPO input
 block; the routed epilogue writes each X1 row once per single-term output
 that reads it.  The tuner times each candidate schedule on the actual
 problems, keeps the fastest, and caches it under a key made of the device
-name, the precision and a histogram of the bond sector sizes (power-of-two
-buckets) with the MPO bond dimension, so later batches with the same sector
-profile skip the timing.
+name, the precision, a histogram of the bond sector sizes (power-of-two
+buckets) with the MPO bond dimension, and a hash of the kernel library, so
+later batches with the same sector profile on the same build skip the timing.
 """
 
 from __future__ import annotations
@@ -55,11 +55,28 @@ def schedule_label(s: dict) -> str:
                                                                                                 "unfused")
 
 
+_LIBRARY_ID = None
+
+
+def library_id() -> str:
+    """Content hash of the loaded CUDA library: schedules tuned on another
+    build of the kernels are timed again."""
+    global _LIBRARY_ID
+    if _LIBRARY_ID is None:
+        import hashlib
+
+        from tenax_b200 import _capi
+
+        with open(_capi.LIB._name, "rb") as f:
+            _LIBRARY_ID = hashlib.sha256(f.read()).hexdigest()[:16]
+    return _LIBRARY_ID
+
+
 def cache_key(problems, precision: str) -> str:
     name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
     hist, dws = sector_histogram(problems)
     return json.dumps({"device": name, "precision": precision, "dw": dws, "sectors": hist,
-                       "schedules": list(SCHEDULE_SET)}, sort_keys=True)
+                       "schedules": list(SCHEDULE_SET), "library": library_id()}, sort_keys=True)
 
 
 def candidates(problems, precision: str) -> list:

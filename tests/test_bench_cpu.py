@@ -121,3 +121,21 @@ def test_dram_view_of_the_dominant_kernel():
     assert abs(v["frac"] - v["achieved"] / 6650.0) < 1e-4
     assert b._dram_view(None, 2.264, {"hbm_gbs": 6650.0}, "fallback") is None
     assert b._dram_view(7374000000, 2.264, {}, "measured") is None
+
+
+def test_autotune_key_names_the_library_build():
+    """A schedule tuned on one build of the kernels is not reused by another:
+    the cache key carries a hash of the loaded library."""
+    import json
+    import types
+
+    import numpy as np
+
+    from tenax_b200 import autotune
+
+    leg = types.SimpleNamespace(charges=np.repeat(np.arange(3), [4, 9, 2]))
+    p = types.SimpleNamespace(theta=types.SimpleNamespace(indices=(leg, None, None, leg)),
+                              Wl=types.SimpleNamespace(indices=(types.SimpleNamespace(charges=np.zeros(5)),)))
+    key = json.loads(autotune.cache_key([p], "bf16x3"))
+    assert len(key["library"]) == 16 and key["library"] == autotune.library_id()
+    assert key["schedules"] == list(autotune.SCHEDULE_SET) and key["dw"] == [5]
